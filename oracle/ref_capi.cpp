@@ -1,0 +1,92 @@
+// ORACLE (reference build) -- test infrastructure only.
+// Flat C entry points over the REFERENCE solver's own functions (src/grid.cpp,
+// src/collision.cpp, src/import.cpp, src/export.cpp compiled unmodified from the
+// reference tree by oracle/Makefile, against the project's Eigen-subset shim in
+// place of Eigen3, which is not installed on this image).  Used by the tests to
+// pin the oracle restatement and by bench.py's reference arm as the CPU baseline.
+// Particles travel as 26-double records in the reference's struct Particle order.
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "snow/collision.hpp"
+#include "snow/debug.hpp"
+#include "snow/export.hpp"
+#include "snow/grid.hpp"
+#include "snow/import.hpp"
+#include "snow/particle.hpp"
+
+static_assert(sizeof(Particle) == 208, "reference Particle must be 26 packed doubles");
+
+namespace {
+std::vector<Particle> to_vec(const double* rec, int64_t n) {
+  std::vector<Particle> v;
+  v.reserve((std::size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    v.emplace_back(Eigen::Vector3d::Zero(), Eigen::Vector3d::Zero(), 0.0, 0.0);
+    std::memcpy(static_cast<void*>(&v.back()), rec + 26 * i, sizeof(Particle));
+  }
+  return v;
+}
+void from_vec(const std::vector<Particle>& v, double* rec) {
+  for (std::size_t i = 0; i < v.size(); ++i)
+    std::memcpy(rec + 26 * i, static_cast<const void*>(&v[i]), sizeof(Particle));
+}
+std::vector<CollisionBody> planes(const double* q, int n) {
+  std::vector<CollisionBody> b;
+  for (int i = 0; i < n; ++i, q += 7)
+    b.push_back(make_plane({q[0], q[1], q[2]}, {q[3], q[4], q[5]}, q[6]));
+  return b;
+}
+thread_local std::string g_err;
+}  // namespace
+
+extern "C" {
+
+void ref_setup(double* rec, int64_t n, double dx) {
+  auto v = to_vec(rec, n);
+  setup(v, dx);
+  from_vec(v, rec);
+}
+
+// params: gravity[3], dt, dx, mu0, lambda0, xi, theta_c, theta_s, alpha
+void ref_step(double* rec, int64_t n, const double* p, const double* plane_data, int n_planes,
+              int steps, double* stage_ms) {
+  auto v = to_vec(rec, n);
+  auto bodies = planes(plane_data, n_planes);
+  std::vector<ParticleStencil> stencils(v.size());
+  StepTimings t;
+  for (int s = 0; s < steps; ++s)
+    step(v, bodies, stencils, Eigen::Vector3d{p[0], p[1], p[2]}, p[3], p[4], p[5], p[6], p[7],
+         p[8], p[9], p[10], t);
+  if (stage_ms) {
+    const double ms[10] = {t.stencil, t.p2g, t.forces_constitutive, t.forces_accumulative,
+                           t.grid_velocity, t.grid_collisions, t.stress_update, t.g2p,
+                           t.particle_collisions, t.position_update};
+    std::memcpy(stage_ms, ms, sizeof ms);
+  }
+  from_vec(v, rec);
+}
+
+// Two calls: with out == nullptr returns the particle count, else fills `out`
+// (capacity records).  Returns -1 and keeps the exception text on error.
+int64_t ref_import(const char* groups, const char* particles, double* out, int64_t capacity) {
+  try {
+    auto v = import_particles(groups, particles);
+    if (out) {
+      if ((int64_t)v.size() > capacity) return -2;
+      from_vec(v, out);
+    }
+    return (int64_t)v.size();
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+const char* ref_last_error(void) { return g_err.c_str(); }
+
+void ref_export(const double* rec, int64_t n, int frame) { export_particles(to_vec(rec, n), frame); }
+
+}  // extern "C"
