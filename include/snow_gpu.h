@@ -1,0 +1,189 @@
+/*
+ * snow_gpu.h -- C ABI of the B200 explicit-MPM snow step.
+ *
+ * This is the boundary between the C++20 drop-in API (the headers under include/snow/, the
+ * reference solver's own function signatures) and the sm_100a CUDA kernels.
+ * Only plain C types cross it: pointers, sizes, doubles and small structs.
+ * Every entry point returns 0 on success or a negative SNOW_E* code; the text
+ * of the last error on the calling thread is available from
+ * snow_gpu_last_error().  A `stream` argument is a cudaStream_t (NULL = the
+ * legacy default stream); calls are stream-ordered and, unless stated
+ * otherwise, return once their work has completed.
+ *
+ * Particles cross the boundary as records of 26 doubles (208 bytes) in the
+ * order of the reference's struct Particle (include/snow/particle.hpp:5-28 in
+ * the reference tree): x_p[3], v_p[3], m_p, V_p0, F_P[9], F_E[9], the 3x3
+ * matrices column-major as in Eigen::Matrix3d.
+ *
+ * Reference interfaces replaced (reference tree paths):
+ *   snow_gpu_setup            setup(std::vector<Particle>&, double)          include/snow/grid.hpp:96, src/grid.cpp:340
+ *   snow_gpu_step             step(particles, colliders, stencils, gravity, dt, dx, mu_0,
+ *                             lambda_0, xi, theta_c, theta_s, alpha, timings)  include/snow/grid.hpp:97, src/grid.cpp:359
+ *   snow_gpu_make_plane       make_plane(point, normal, friction)             include/snow/collision.hpp:14, src/collision.cpp:5
+ *   snow_step_timings         struct StepTimings                              include/snow/debug.hpp:3-15
+ *   snow_gpu_stage_*          the per-stage functions of include/snow/grid.hpp:75-95
+ *                             (P2G, calculate_volume, force_calculation,
+ *                             grid_velocity, grid_collisions, stress_update,
+ *                             G2P, particle_collisions, position_update)
+ *   snow_gpu_batch_*          no reference counterpart: many independent scenes
+ *                             advanced by one launch per stage
+ */
+#ifndef SNOW_GPU_H
+#define SNOW_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SNOW_GPU_ABI_VERSION 1
+#define SNOW_RECORD_DOUBLES 26
+
+enum {
+  SNOW_OK = 0,
+  SNOW_E_ARG = -1,        /* invalid argument */
+  SNOW_E_CUDA = -2,       /* CUDA runtime error (no device, out of memory, ...) */
+  SNOW_E_CAPACITY = -3,   /* grid block / hash capacity exceeded during a step */
+  SNOW_E_NONFINITE = -4,  /* a particle position became NaN or infinite */
+  SNOW_E_KEYRANGE = -5,   /* scene extent too large for the 32-bit block keys */
+  SNOW_E_STATE = -6       /* call out of order (e.g. unknown scene id) */
+};
+
+/* Precision of a batch. */
+enum {
+  SNOW_FP64 = 0,  /* every quantity in double: the drop-in path */
+  SNOW_MIXED = 1  /* x, v, m, V_p0, F_E, grid and transfers in float; F_P, its
+                     determinant and the hardening exponential in double */
+};
+
+/* Collider kinds. */
+enum { SNOW_COLLIDER_PLANE = 0 };
+
+/* A collider (CollisionBody, include/snow/collision.hpp:6-12).  A plane is
+ * the half-space phi(x) = normal . (x - point) <= 0 with unit `normal`; the
+ * collider moves with constant `velocity` (zero for make_plane). */
+typedef struct snow_collider {
+  int32_t kind;
+  int32_t reserved;
+  double point[3];
+  double normal[3];
+  double velocity[3];
+  double friction;
+  double param[2];
+} snow_collider;
+
+/* Arguments 4-12 of step() (src/grid.cpp:359). */
+typedef struct snow_step_params {
+  double gravity[3];
+  double time_step;
+  double grid_spacing;
+  double mu_0;
+  double lambda_0;
+  double hardening_coefficient;
+  double max_compression;
+  double max_stretch;
+  double alpha;
+} snow_step_params;
+
+/* StepTimings (include/snow/debug.hpp:3-15), milliseconds, accumulated.
+ * The fused kernels report their time under the first stage they contain:
+ * stencil = key/sort/block build, p2g = P2G + constitutive + force scatter,
+ * grid_velocity = grid update + collisions, stress_update = elastoplastic
+ * update + G2P + particle collisions + advection; the other fields stay 0. */
+typedef struct snow_step_timings {
+  double stencil, p2g, forces_constitutive, forces_accumulative, grid_velocity, grid_collisions,
+      stress_update, g2p, particle_collisions, position_update;
+} snow_step_timings;
+
+typedef struct snow_gpu_batch snow_gpu_batch;
+
+/* ---- process ---------------------------------------------------------- */
+int snow_gpu_init(int device);
+const char* snow_gpu_last_error(void);
+int snow_gpu_abi_version(void);
+
+/* make_plane (src/collision.cpp:5-27): unit normal = normal / |normal|
+ * (a zero normal is kept as is), zero velocity. */
+int snow_gpu_make_plane(const double point[3], const double normal[3], double friction,
+                        snow_collider* out);
+
+/* ---- batches of scenes -------------------------------------------------- */
+int snow_gpu_batch_create(snow_gpu_batch** out, int precision);
+int snow_gpu_batch_destroy(snow_gpu_batch* batch);
+
+/* Adds a scene: uploads n particle records (host memory), its step
+ * parameters and colliders.  The scene id is written to *scene_id. */
+int snow_gpu_batch_add_scene(snow_gpu_batch* batch, const double* records, int64_t n,
+                             const snow_step_params* params, const snow_collider* colliders,
+                             int n_colliders, int32_t* scene_id, void* stream);
+int snow_gpu_batch_remove_scene(snow_gpu_batch* batch, int32_t scene_id);
+int snow_gpu_batch_set_params(snow_gpu_batch* batch, int32_t scene_id,
+                              const snow_step_params* params, const snow_collider* colliders,
+                              int n_colliders);
+/* Replaces the particle state of a scene (same particle count). */
+int snow_gpu_batch_upload(snow_gpu_batch* batch, int32_t scene_id, const double* records,
+                          int64_t n, void* stream);
+/* Copies a scene's particles back in their original order. */
+int snow_gpu_batch_download(snow_gpu_batch* batch, int32_t scene_id, double* records, int64_t n,
+                            void* stream);
+/* setup() for one scene: V_p0 = m_p / (sum_i m_i w_ip / dx^3) from a mass-only P2G. */
+int snow_gpu_batch_setup(snow_gpu_batch* batch, int32_t scene_id, double grid_spacing,
+                         void* stream);
+/* Advances every scene of the batch by n_steps explicit steps (one launch per
+ * stage for all scenes; replayed from a CUDA graph when timings == NULL).
+ * Returns after the steps complete and reports overflow/NaN status. */
+int snow_gpu_batch_step(snow_gpu_batch* batch, int n_steps, snow_step_timings* timings,
+                        void* stream);
+int snow_gpu_batch_scene_count(snow_gpu_batch* batch);
+int64_t snow_gpu_batch_particles(snow_gpu_batch* batch);
+/* Device bytes held by the batch (particles, sort, grid). */
+int64_t snow_gpu_batch_device_bytes(snow_gpu_batch* batch);
+/* Last status word (bit set of overflow / NaN conditions) and the grid blocks
+ * used by the last step. */
+int snow_gpu_batch_status(snow_gpu_batch* batch, uint32_t* status, int64_t* blocks_used,
+                          int64_t* blocks_capacity);
+/* Use (1) or bypass (0) CUDA-graph replay for timing-free steps. */
+int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable);
+
+/* ---- one scene: setup() / step() of the reference ------------------------ */
+/* setup() on host records: records[i].V_p0 is overwritten. */
+int snow_gpu_setup(double* records, int64_t n, double grid_spacing);
+/* n_steps of step() on host records, in place (upload, steps, download). */
+int snow_gpu_step(double* records, int64_t n, const snow_step_params* params,
+                  const snow_collider* colliders, int n_colliders, int n_steps,
+                  snow_step_timings* timings);
+
+/* ---- single stages (the reference's per-stage functions) ----------------
+ * Grids cross as node lists: ijk[n][3] (int32) and fields[n][10] (double) =
+ * mass, momentum[3], velocity[3], force[3].  Stage entry points run the same
+ * device code as the fused step.  The *_p2g and *_force entries return the
+ * contributions of the particles on an empty grid: every node of the grid
+ * blocks the particles' stencils touch (capacity cap_nodes; the count is
+ * written to *n_nodes). */
+int snow_gpu_stage_p2g(const double* records, int64_t n, double grid_spacing, int32_t* ijk,
+                       double* fields, int64_t cap_nodes, int64_t* n_nodes);
+int snow_gpu_stage_force(const double* records, int64_t n, double grid_spacing, double mu_0,
+                         double lambda_0, double hardening_coefficient, int32_t* ijk,
+                         double* fields, int64_t cap_nodes, int64_t* n_nodes);
+int snow_gpu_stage_grid_velocity(double* fields, int64_t n_nodes, const double gravity[3],
+                                 double time_step);
+int snow_gpu_stage_grid_collisions(const int32_t* ijk, double* fields, int64_t n_nodes,
+                                   const snow_collider* colliders, int n_colliders,
+                                   double grid_spacing);
+/* calculate_volume / stress_update / G2P of particles against a given grid. */
+int snow_gpu_stage_volume(const int32_t* ijk, const double* fields, int64_t n_nodes,
+                          double* records, int64_t n, double grid_spacing);
+int snow_gpu_stage_stress_update(const int32_t* ijk, const double* fields, int64_t n_nodes,
+                                 double* records, int64_t n, double grid_spacing,
+                                 double time_step, double max_compression, double max_stretch);
+int snow_gpu_stage_g2p(const int32_t* ijk, const double* fields, int64_t n_nodes,
+                       double* records, int64_t n, double grid_spacing, double alpha);
+int snow_gpu_stage_particle_collisions(double* records, int64_t n,
+                                       const snow_collider* colliders, int n_colliders);
+int snow_gpu_stage_position_update(double* records, int64_t n, double time_step);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SNOW_GPU_H */

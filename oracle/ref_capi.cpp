@@ -5,6 +5,9 @@
 // place of Eigen3, which is not installed on this image).  Used by the tests to
 // pin the oracle restatement and by bench.py's reference arm as the CPU baseline.
 // Particles travel as 26-double records in the reference's struct Particle order.
+// Step calls report the ten StepTimings stages and, in slot 10, the wall time
+// of the step loop (milliseconds).
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -58,10 +61,13 @@ void ref_step(double* rec, int64_t n, const double* p, const double* plane_data,
   auto bodies = planes(plane_data, n_planes);
   std::vector<ParticleStencil> stencils(v.size());
   StepTimings t;
+  const auto t0 = std::chrono::steady_clock::now();
   for (int s = 0; s < steps; ++s)
     step(v, bodies, stencils, Eigen::Vector3d{p[0], p[1], p[2]}, p[3], p[4], p[5], p[6], p[7],
          p[8], p[9], p[10], t);
+  const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (stage_ms) {
+    stage_ms[10] = wall;
     const double ms[10] = {t.stencil, t.p2g, t.forces_constitutive, t.forces_accumulative,
                            t.grid_velocity, t.grid_collisions, t.stress_update, t.g2p,
                            t.particle_collisions, t.position_update};

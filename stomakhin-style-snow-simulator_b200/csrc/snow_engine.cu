@@ -1,0 +1,811 @@
+// Host side of the B200 snow step: batches of scenes, device buffers, CUDA
+// graphs, the particle record <-> structure-of-arrays conversion and the C ABI
+// declared in include/snow_gpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "snow_batch.cuh"
+#include "snow_engine.hpp"
+#include "snow_gpu.h"
+
+namespace snow {
+
+int radix_tiles(int64_t n);
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error(SNOW_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+template <typename T>
+T* dalloc(size_t count) {
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  check_cuda(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+  return static_cast<T*>(p);
+}
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+// ------------------------------------------------- record <-> SoA conversion
+template <typename R>
+__global__ void k_records_to_planes(const double* rec, int64_t n, R* r, double* fp, int32_t* id,
+                                    int64_t st) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* p = rec + 26 * i;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k * st + i] = (R)p[k];          // x, v, m, V_p0
+#pragma unroll
+  for (int k = 0; k < 9; ++k) fp[k * st + i] = p[8 + k];        // F_P
+#pragma unroll
+  for (int k = 0; k < 9; ++k) r[(PFE + k) * st + i] = (R)p[17 + k];  // F_E
+  id[i] = (int32_t)i;
+}
+
+template <typename R>
+__global__ void k_planes_to_records(double* rec, int64_t n, const R* r, const double* fp,
+                                    const int32_t* id, int64_t st) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* p = rec + 26 * (int64_t)id[i];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) p[k] = (double)r[k * st + i];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) p[8 + k] = fp[k * st + i];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) p[17 + k] = (double)r[(PFE + k) * st + i];
+}
+
+int64_t pad32(int64_t n) { return (n + 31) / 32 * 32; }
+
+}  // namespace
+
+// ---------------------------------------------------------------- Batch impl
+Batch::Batch(int precision) : prec_(precision) {
+  if (precision != SNOW_FP64 && precision != SNOW_MIXED) throw Error(SNOW_E_ARG, "unknown precision");
+  rsize_ = precision == SNOW_FP64 ? sizeof(double) : sizeof(float);
+  d_ctr_ = dalloc<Counters>(1);
+  check_cuda(cudaMemset(d_ctr_, 0, sizeof(Counters)), "cudaMemset");
+  check_cuda(cudaMallocHost((void**)&h_ctr_, sizeof(Counters)), "cudaMallocHost");
+  std::memset(h_ctr_, 0, sizeof(Counters));
+  check_cuda(cudaStreamCreate(&own_stream_), "cudaStreamCreate");
+}
+
+Batch::~Batch() {
+  drop_graph();
+  for (auto& s : scenes_) free_scene(*s);
+  dfree(d_scenes_);
+  dfree(d_coll_);
+  dfree(d_ctr_);
+  if (h_ctr_) cudaFreeHost(h_ctr_);
+  free_particle_buffers();
+  free_grid();
+  dfree(staging_);
+  dfree(d_tmp_scene_);
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+void Batch::free_scene(Scene& s) {
+  for (int k = 0; k < 2; ++k) {
+    dfree(s.r[k]);
+    dfree(s.fp[k]);
+    dfree(s.id[k]);
+  }
+}
+
+void Batch::free_particle_buffers() {
+  for (int k = 0; k < 2; ++k) {
+    dfree(keys_[k]);
+    dfree(vals_[k]);
+  }
+  dfree(hist_);
+  dfree(digit_total_);
+  cap_p_ = 0;
+}
+
+void Batch::free_grid() {
+  dfree(hkeys_);
+  dfree(hvals_);
+  dfree(blk_);
+  dfree(blk_key_);
+  dfree(pblk_start_);
+  dfree(pblk_end_);
+  dfree(acc_);
+  dfree(vel_);
+  cap_blocks_ = 0;
+  hcap_ = 0;
+}
+
+void Batch::drop_graph() {
+  if (gexec_) cudaGraphExecDestroy(gexec_);
+  gexec_ = nullptr;
+}
+
+Scene* Batch::find(int32_t id) {
+  for (auto& s : scenes_)
+    if (s->sid == id) return s.get();
+  throw Error(SNOW_E_STATE, "unknown scene id " + std::to_string(id));
+}
+
+void Batch::ensure_staging(int64_t n) {
+  if (n <= staging_cap_) return;
+  dfree(staging_);
+  staging_ = dalloc<double>((size_t)std::max<int64_t>(n, 1) * 26);
+  staging_cap_ = n;
+}
+
+static void validate_params(const snow_step_params* p) {
+  if (!p) throw Error(SNOW_E_ARG, "params is NULL");
+  if (!(p->grid_spacing > 0.0) || !std::isfinite(p->grid_spacing))
+    throw Error(SNOW_E_ARG, "grid_spacing must be positive and finite");
+  if (!std::isfinite(p->time_step)) throw Error(SNOW_E_ARG, "time_step must be finite");
+}
+
+int32_t Batch::add_scene(const double* records, int64_t n, const snow_step_params* params,
+                         const snow_collider* colliders, int n_colliders, cudaStream_t s) {
+  if (n < 0 || (n > 0 && !records)) throw Error(SNOW_E_ARG, "bad particle array");
+  if (n > INT32_MAX) throw Error(SNOW_E_ARG, "at most 2^31-1 particles per scene");
+  validate_params(params);
+  auto sc = std::make_unique<Scene>();
+  sc->sid = next_id_++;
+  sc->n = n;
+  sc->stride = pad32(std::max<int64_t>(n, 1));
+  for (int k = 0; k < 2; ++k) {
+    sc->r[k] = dalloc<unsigned char>((size_t)sc->stride * kRealPlanes * rsize_);
+    sc->fp[k] = dalloc<double>((size_t)sc->stride * kFPPlanes);
+    sc->id[k] = dalloc<int32_t>((size_t)sc->stride);
+  }
+  sc->params = *params;
+  set_colliders(*sc, colliders, n_colliders);
+  Scene* raw = sc.get();
+  scenes_.push_back(std::move(sc));
+  dirty_ = true;
+  upload(raw->sid, records, n, s);
+  return raw->sid;
+}
+
+void Batch::set_colliders(Scene& sc, const snow_collider* c, int n) {
+  if (n < 0 || (n > 0 && !c)) throw Error(SNOW_E_ARG, "bad collider array");
+  sc.colliders.clear();
+  for (int i = 0; i < n; ++i) {
+    if (c[i].kind != SNOW_COLLIDER_PLANE)
+      throw Error(SNOW_E_ARG, "unsupported collider kind " + std::to_string(c[i].kind));
+    Collider d{};
+    d.kind = c[i].kind;
+    for (int a = 0; a < 3; ++a) {
+      d.point[a] = c[i].point[a];
+      d.normal[a] = c[i].normal[a];
+      d.velocity[a] = c[i].velocity[a];
+    }
+    d.friction = c[i].friction;
+    d.param[0] = c[i].param[0];
+    d.param[1] = c[i].param[1];
+    sc.colliders.push_back(d);
+  }
+}
+
+void Batch::remove_scene(int32_t id) {
+  for (size_t k = 0; k < scenes_.size(); ++k)
+    if (scenes_[k]->sid == id) {
+      cudaDeviceSynchronize();
+      free_scene(*scenes_[k]);
+      scenes_.erase(scenes_.begin() + k);
+      dirty_ = true;
+      return;
+    }
+  throw Error(SNOW_E_STATE, "unknown scene id " + std::to_string(id));
+}
+
+void Batch::set_params(int32_t id, const snow_step_params* params, const snow_collider* c, int n) {
+  validate_params(params);
+  Scene* sc = find(id);
+  sc->params = *params;
+  set_colliders(*sc, c, n);
+  params_dirty_ = true;
+}
+
+void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s) {
+  Scene* sc = find(id);
+  if (n != sc->n) throw Error(SNOW_E_ARG, "upload: particle count differs from the scene's");
+  if (n == 0) return;
+  ensure_staging(n);
+  check_cuda(cudaMemcpyAsync(staging_, records, (size_t)n * 26 * sizeof(double),
+                             cudaMemcpyHostToDevice, s),
+             "upload copy");
+  const unsigned g = (unsigned)((n + 255) / 256);
+  if (prec_ == SNOW_FP64)
+    k_records_to_planes<double><<<g, 256, 0, s>>>(staging_, n, (double*)sc->r[sc->cur],
+                                                   sc->fp[sc->cur], sc->id[sc->cur], sc->stride);
+  else
+    k_records_to_planes<float><<<g, 256, 0, s>>>(staging_, n, (float*)sc->r[sc->cur],
+                                                  sc->fp[sc->cur], sc->id[sc->cur], sc->stride);
+  check_cuda(cudaGetLastError(), "upload kernel");
+  boxes_dirty_ = true;
+}
+
+void Batch::download(int32_t id, double* records, int64_t n, cudaStream_t s) {
+  Scene* sc = find(id);
+  if (n != sc->n) throw Error(SNOW_E_ARG, "download: particle count differs from the scene's");
+  if (n == 0) return;
+  ensure_staging(n);
+  const unsigned g = (unsigned)((n + 255) / 256);
+  if (prec_ == SNOW_FP64)
+    k_planes_to_records<double><<<g, 256, 0, s>>>(staging_, n, (const double*)sc->r[sc->cur],
+                                                   sc->fp[sc->cur], sc->id[sc->cur], sc->stride);
+  else
+    k_planes_to_records<float><<<g, 256, 0, s>>>(staging_, n, (const float*)sc->r[sc->cur],
+                                                  sc->fp[sc->cur], sc->id[sc->cur], sc->stride);
+  check_cuda(cudaGetLastError(), "download kernel");
+  check_cuda(cudaMemcpyAsync(records, staging_, (size_t)n * 26 * sizeof(double),
+                             cudaMemcpyDeviceToHost, s),
+             "download copy");
+  check_cuda(cudaStreamSynchronize(s), "download sync");
+}
+
+SceneDev Batch::scene_dev(const Scene& sc, int64_t begin) const {
+  SceneDev d{};
+  for (int k = 0; k < 2; ++k) {
+    d.r[k] = sc.r[k];
+    d.fp[k] = sc.fp[k];
+    d.id[k] = sc.id[k];
+  }
+  d.stride = sc.stride;
+  d.n = sc.n;
+  d.begin = begin;
+  d.cur = sc.cur;
+  d.active = 1;
+  const snow_step_params& p = sc.params;
+  d.dx = p.grid_spacing;
+  d.dt = p.time_step;
+  for (int a = 0; a < 3; ++a) d.g[a] = p.gravity[a];
+  d.mu0 = p.mu_0;
+  d.lambda0 = p.lambda_0;
+  d.xi = p.hardening_coefficient;
+  d.theta_c = p.max_compression;
+  d.theta_s = p.max_stretch;
+  d.alpha = p.alpha;
+  for (int a = 0; a < 3; ++a) {
+    d.nb_lo[a] = INT_MAX;
+    d.nb_hi[a] = INT_MIN;
+  }
+  return d;
+}
+
+void Batch::ensure_particle_buffers(int64_t total) {
+  if (total <= cap_p_) return;
+  free_particle_buffers();
+  const int64_t cap = std::max<int64_t>(total, 1024);
+  for (int k = 0; k < 2; ++k) {
+    keys_[k] = dalloc<uint32_t>((size_t)cap);
+    vals_[k] = dalloc<uint32_t>((size_t)cap);
+  }
+  ntiles_cap_ = radix_tiles(cap);
+  hist_ = dalloc<uint32_t>((size_t)ntiles_cap_ * 256);
+  digit_total_ = dalloc<uint32_t>(256);
+  cap_p_ = cap;
+}
+
+void Batch::ensure_grid(int64_t blocks) {
+  if (blocks <= cap_blocks_) return;
+  free_grid();
+  const int64_t cap = std::max<int64_t>(blocks, 256);
+  cap_blocks_ = (int32_t)cap;
+  uint32_t h = 1;
+  while (h < 2 * (uint64_t)cap) h <<= 1;
+  hcap_ = h;
+  hkeys_ = dalloc<uint32_t>(h);
+  hvals_ = dalloc<int32_t>(h);
+  blk_ = dalloc<int4>((size_t)cap);
+  blk_key_ = dalloc<uint32_t>((size_t)cap);
+  pblk_start_ = dalloc<int32_t>((size_t)cap);
+  pblk_end_ = dalloc<int32_t>((size_t)cap);
+  acc_ = dalloc<unsigned char>((size_t)cap * 64 * kAccCh * rsize_);
+  vel_ = dalloc<unsigned char>((size_t)cap * 64 * kVelCh * rsize_);
+  check_cuda(cudaMemset(acc_, 0, (size_t)cap * 64 * kAccCh * rsize_), "cudaMemset");
+  check_cuda(cudaMemset(vel_, 0, (size_t)cap * 64 * kVelCh * rsize_), "cudaMemset");
+}
+
+BatchDev Batch::dev(SceneDev* scenes, int num_scenes, int64_t total) const {
+  BatchDev b{};
+  b.scenes = scenes;
+  b.num_scenes = num_scenes;
+  b.total = total;
+  b.colliders = d_coll_;
+  for (int k = 0; k < 2; ++k) {
+    b.keys[k] = keys_[k];
+    b.vals[k] = vals_[k];
+  }
+  b.hist = hist_;
+  b.digit_total = digit_total_;
+  b.ntiles = radix_tiles(std::max<int64_t>(total, 1));
+  b.hkeys = hkeys_;
+  b.hvals = hvals_;
+  b.hmask = hcap_ - 1;
+  b.cap_blocks = cap_blocks_;
+  b.blk = blk_;
+  b.blk_key = blk_key_;
+  b.pblk_start = pblk_start_;
+  b.pblk_end = pblk_end_;
+  b.acc = acc_;
+  b.vel = vel_;
+  b.ctr = d_ctr_;
+  return b;
+}
+
+// Uploads the scene table and colliders, measures the scenes' block boxes and
+// sizes the grid for them (twice the box volume, so the scenes can move).
+void Batch::rebuild(cudaStream_t s) {
+  drop_graph();
+  total_ = 0;
+  std::vector<SceneDev> table;
+  std::vector<Collider> coll;
+  for (auto& sc : scenes_) {
+    SceneDev d = scene_dev(*sc, total_);
+    d.coll_begin = (int32_t)coll.size();
+    d.coll_count = (int32_t)sc->colliders.size();
+    coll.insert(coll.end(), sc->colliders.begin(), sc->colliders.end());
+    table.push_back(d);
+    total_ += sc->n;
+  }
+  if ((int)table.size() > d_scenes_cap_) {
+    dfree(d_scenes_);
+    d_scenes_cap_ = std::max<int>(16, (int)table.size() * 2);
+    d_scenes_ = dalloc<SceneDev>(d_scenes_cap_);
+  }
+  if ((int)coll.size() > d_coll_cap_ || !d_coll_) {
+    dfree(d_coll_);
+    d_coll_cap_ = std::max<int>(16, (int)coll.size() * 2);
+    d_coll_ = dalloc<Collider>(d_coll_cap_);
+  }
+  if (!table.empty())
+    check_cuda(cudaMemcpyAsync(d_scenes_, table.data(), table.size() * sizeof(SceneDev),
+                               cudaMemcpyHostToDevice, s),
+               "scene table");
+  if (!coll.empty())
+    check_cuda(cudaMemcpyAsync(d_coll_, coll.data(), coll.size() * sizeof(Collider),
+                               cudaMemcpyHostToDevice, s),
+               "colliders");
+  ensure_particle_buffers(total_);
+  const BatchDev b = dev(d_scenes_, (int)table.size(), total_);
+  if (prec_ == SNOW_FP64)
+    StepLaunch<double>::bbox_init(b, s);
+  else
+    StepLaunch<float>::bbox_init(b, s);
+  check_cuda(cudaGetLastError(), "bbox");
+  // size the grid from the measured boxes
+  check_cuda(cudaMemcpyAsync(table.data(), d_scenes_, table.size() * sizeof(SceneDev),
+                             cudaMemcpyDeviceToHost, s),
+             "scene table readback");
+  check_cuda(cudaStreamSynchronize(s), "sync");
+  int64_t vol = 0;
+  for (const SceneDev& d : table) {
+    if (d.nb_lo[0] > d.nb_hi[0]) continue;
+    int64_t v = 1;
+    for (int a = 0; a < 3; ++a) v *= (int64_t)(d.nb_hi[a] - d.nb_lo[a] + 4);
+    vol += v;
+  }
+  ensure_grid(std::min<int64_t>(2 * vol + 1024, std::max<int64_t>(8 * total_ + 64, 1024)));
+  num_dev_scenes_ = (int)table.size();
+  dirty_ = false;
+  boxes_dirty_ = false;
+  params_dirty_ = false;
+}
+
+// Re-uploads parameters only (scene table entries keep their device-side state).
+void Batch::refresh_params(cudaStream_t s) {
+  std::vector<SceneDev> table(num_dev_scenes_);
+  check_cuda(cudaMemcpyAsync(table.data(), d_scenes_, table.size() * sizeof(SceneDev),
+                             cudaMemcpyDeviceToHost, s),
+             "scene table readback");
+  check_cuda(cudaStreamSynchronize(s), "sync");
+  std::vector<Collider> coll;
+  for (size_t k = 0; k < scenes_.size(); ++k) {
+    const Scene& sc = *scenes_[k];
+    SceneDev fresh = scene_dev(sc, table[k].begin);
+    SceneDev& d = table[k];
+    d.dx = fresh.dx;
+    d.dt = fresh.dt;
+    for (int a = 0; a < 3; ++a) d.g[a] = fresh.g[a];
+    d.mu0 = fresh.mu0;
+    d.lambda0 = fresh.lambda0;
+    d.xi = fresh.xi;
+    d.theta_c = fresh.theta_c;
+    d.theta_s = fresh.theta_s;
+    d.alpha = fresh.alpha;
+    d.coll_begin = (int32_t)coll.size();
+    d.coll_count = (int32_t)sc.colliders.size();
+    coll.insert(coll.end(), sc.colliders.begin(), sc.colliders.end());
+  }
+  if ((int)coll.size() > d_coll_cap_) {
+    // the collider array moves: captured graphs hold the old pointer
+    drop_graph();
+    dfree(d_coll_);
+    d_coll_cap_ = std::max<int>(16, (int)coll.size() * 2);
+    d_coll_ = dalloc<Collider>(d_coll_cap_);
+  }
+  check_cuda(cudaMemcpyAsync(d_scenes_, table.data(), table.size() * sizeof(SceneDev),
+                             cudaMemcpyHostToDevice, s),
+             "scene table");
+  if (!coll.empty())
+    check_cuda(cudaMemcpyAsync(d_coll_, coll.data(), coll.size() * sizeof(Collider),
+                               cudaMemcpyHostToDevice, s),
+               "colliders");
+  params_dirty_ = false;
+}
+
+template <typename R>
+void Batch::launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev) {
+  auto mark = [&](int k) {
+    if (ev) cudaEventRecord(ev[k], s);
+  };
+  mark(0);
+  StepLaunch<R>::keyspace(b, s, false);
+  StepLaunch<R>::keys(b, s);
+  radix_sort(b, s);
+  StepLaunch<R>::blocks(b, s);
+  mark(1);
+  StepLaunch<R>::p2g(b, P2G_FULL, s);
+  mark(2);
+  StepLaunch<R>::grid_update(b, s);
+  mark(3);
+  StepLaunch<R>::g2p(b, G2P_FULL, s);
+  StepLaunch<R>::finish(b, s);
+  mark(4);
+}
+
+void Batch::prepare(cudaStream_t s) {
+  if (dirty_ || boxes_dirty_)
+    rebuild(s);
+  else if (params_dirty_)
+    refresh_params(s);
+}
+
+void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
+  if (n_steps < 0) throw Error(SNOW_E_ARG, "negative step count");
+  if (n_steps == 0 || scenes_.empty()) return;
+  // The legacy NULL stream cannot be captured into a graph: run on the batch's
+  // own (blocking) stream instead, which orders itself with NULL-stream work.
+  if (!s) s = own_stream_;
+  prepare(s);
+  const BatchDev b = dev(d_scenes_, num_dev_scenes_, total_);
+  auto one = [&](cudaEvent_t* ev) {
+    if (prec_ == SNOW_FP64)
+      launch_step<double>(b, s, ev);
+    else
+      launch_step<float>(b, s, ev);
+  };
+  if (timings) {
+    cudaEvent_t ev[5];
+    for (auto& e : ev) check_cuda(cudaEventCreate(&e), "event");
+    for (int k = 0; k < n_steps; ++k) {
+      one(ev);
+      check_cuda(cudaEventSynchronize(ev[4]), "step");
+      float ms[4];
+      for (int q = 0; q < 4; ++q) cudaEventElapsedTime(&ms[q], ev[q], ev[q + 1]);
+      timings->stencil += ms[0];
+      timings->p2g += ms[1];
+      timings->grid_velocity += ms[2];
+      timings->stress_update += ms[3];
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+  } else if (use_graphs_) {
+    int k = 0;
+    if (!gexec_) {
+      // first step eagerly (initialises per-kernel launch settings), then capture
+      one(nullptr);
+      check_cuda(cudaGetLastError(), "step launch");
+      ++k;
+      if (k < n_steps) {
+        cudaGraph_t g;
+        check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+        one(nullptr);
+        check_cuda(cudaStreamEndCapture(s, &g), "capture end");
+        check_cuda(cudaGraphInstantiate(&gexec_, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+      }
+    }
+    for (; k < n_steps; ++k) check_cuda(cudaGraphLaunch(gexec_, s), "graph launch");
+  } else {
+    for (int k = 0; k < n_steps; ++k) one(nullptr);
+  }
+  check_cuda(cudaGetLastError(), "step launch");
+  for (auto& sc : scenes_) sc->cur ^= (n_steps & 1);
+  check_cuda(cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, s), "status");
+  check_cuda(cudaStreamSynchronize(s), "step");
+  last_status_ = h_ctr_->status;
+  last_blocks_ = (int64_t)h_ctr_->n_pblocks + h_ctr_->n_halo;
+  check_status();
+  // Keep 2x headroom: grow the grid before the next call if the last step came close.
+  if (last_blocks_ * 2 > cap_blocks_) dirty_ = true;
+}
+
+void Batch::check_status() {
+  const uint32_t st = last_status_;
+  if (!st) return;
+  cudaMemset(&d_ctr_->status, 0, sizeof(uint32_t));
+  if (st & (ST_BLOCK_OVERFLOW | ST_HASH_FULL))
+    throw Error(SNOW_E_CAPACITY, "grid block capacity exceeded (" + std::to_string(cap_blocks_) +
+                                     " blocks); the step result is not valid");
+  if (st & ST_NONFINITE) throw Error(SNOW_E_NONFINITE, "a particle position became NaN or infinite");
+  if (st & ST_KEY_OVERFLOW)
+    throw Error(SNOW_E_KEYRANGE, "scene extent exceeds the 32-bit block key range");
+  if (st & (ST_OUT_OF_BOX | ST_LOOKUP_MISS))
+    throw Error(SNOW_E_STATE, "internal grid inconsistency (status " + std::to_string(st) + ")");
+}
+
+// setup() for one scene: a private one-scene view over the batch's buffers.
+void Batch::setup(int32_t id, double dx, cudaStream_t s) {
+  if (!(dx > 0.0)) throw Error(SNOW_E_ARG, "grid_spacing must be positive");
+  Scene* sc = find(id);
+  if (sc->n == 0) return;
+  if (dirty_ || boxes_dirty_) rebuild(s);
+  drop_graph();  // the one-scene view reuses the step buffers
+  if (!d_tmp_scene_) d_tmp_scene_ = dalloc<SceneDev>(1);
+  SceneDev d = scene_dev(*sc, 0);
+  d.dx = dx;
+  check_cuda(cudaMemcpyAsync(d_tmp_scene_, &d, sizeof d, cudaMemcpyHostToDevice, s), "tmp scene");
+  ensure_particle_buffers(sc->n);
+  {
+    // measure this scene's block box at the setup spacing and size the grid for it
+    const BatchDev b0 = dev(d_tmp_scene_, 1, sc->n);
+    if (prec_ == SNOW_FP64)
+      StepLaunch<double>::bbox_init(b0, s);
+    else
+      StepLaunch<float>::bbox_init(b0, s);
+    check_cuda(cudaMemcpyAsync(&d, d_tmp_scene_, sizeof d, cudaMemcpyDeviceToHost, s), "box");
+    check_cuda(cudaStreamSynchronize(s), "sync");
+    int64_t vol = 1;
+    for (int a = 0; a < 3; ++a) vol *= (int64_t)(d.nb_hi[a] - d.nb_lo[a] + 4);
+    ensure_grid(std::min<int64_t>(vol + 1024, 8 * sc->n + 1024));
+  }
+  const BatchDev b = dev(d_tmp_scene_, 1, sc->n);
+  auto run = [&](auto tag) {
+    using R = decltype(tag);
+    StepLaunch<R>::keyspace(b, s, true);
+    StepLaunch<R>::keys(b, s);
+    radix_sort(b, s);
+    StepLaunch<R>::blocks(b, s);
+    StepLaunch<R>::p2g(b, P2G_MASS, s);
+    StepLaunch<R>::g2p(b, G2P_VOLUME, s);
+    StepLaunch<R>::zero_grid(b, s);
+  };
+  if (prec_ == SNOW_FP64)
+    run(double{});
+  else
+    run(float{});
+  check_cuda(cudaGetLastError(), "setup launch");
+  check_cuda(cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, s), "status");
+  check_cuda(cudaStreamSynchronize(s), "setup");
+  last_status_ = h_ctr_->status;
+  check_status();
+  boxes_dirty_ = true;  // the batch's own scene table must be re-measured
+}
+
+int64_t Batch::device_bytes() const {
+  int64_t b = 0;
+  for (auto& sc : scenes_) b += 2 * sc->stride * (kRealPlanes * (int64_t)rsize_ + kFPPlanes * 8 + 4);
+  b += cap_p_ * 16 + (int64_t)ntiles_cap_ * 256 * 4;
+  b += (int64_t)cap_blocks_ * (64 * (kAccCh + kVelCh) * (int64_t)rsize_ + 16 + 12) + (int64_t)hcap_ * 8;
+  b += staging_cap_ * 208;
+  return b;
+}
+
+}  // namespace snow
+
+// =================================================================== C ABI
+using snow::Batch;
+using snow::Error;
+
+struct snow_gpu_batch {
+  std::unique_ptr<Batch> impl;
+};
+
+namespace {
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return SNOW_OK;
+  } catch (const Error& e) {
+    return snow::set_error(e.code, e.what());
+  } catch (const std::exception& e) {
+    return snow::set_error(SNOW_E_ARG, e.what());
+  }
+}
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+
+int snow_gpu_abi_version(void) { return SNOW_GPU_ABI_VERSION; }
+const char* snow_gpu_last_error(void) { return snow::g_last_error.c_str(); }
+
+int snow_gpu_init(int device) {
+  return guarded([&] {
+    int n = 0;
+    snow::check_cuda(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+    if (device < 0 || device >= n) throw Error(SNOW_E_ARG, "no CUDA device " + std::to_string(device));
+    snow::check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    snow::check_cuda(cudaFree(nullptr), "context");
+  });
+}
+
+int snow_gpu_make_plane(const double point[3], const double normal[3], double friction,
+                        snow_collider* out) {
+  if (!point || !normal || !out) return snow::set_error(SNOW_E_ARG, "NULL argument");
+  std::memset(out, 0, sizeof *out);
+  out->kind = SNOW_COLLIDER_PLANE;
+  const double len = std::sqrt(normal[0] * normal[0] + normal[1] * normal[1] + normal[2] * normal[2]);
+  for (int a = 0; a < 3; ++a) {
+    out->point[a] = point[a];
+    out->normal[a] = len > 0.0 ? normal[a] / len : normal[a];
+  }
+  out->friction = friction;
+  return SNOW_OK;
+}
+
+int snow_gpu_batch_create(snow_gpu_batch** out, int precision) {
+  return guarded([&] {
+    if (!out) throw Error(SNOW_E_ARG, "out is NULL");
+    auto* b = new snow_gpu_batch;
+    try {
+      b->impl = std::make_unique<Batch>(precision);
+    } catch (...) {
+      delete b;
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int snow_gpu_batch_destroy(snow_gpu_batch* batch) {
+  return guarded([&] {
+    if (!batch) return;
+    cudaDeviceSynchronize();
+    delete batch;
+  });
+}
+
+#define SNOW_BATCH_OR_FAIL \
+  if (!batch || !batch->impl) throw Error(SNOW_E_ARG, "batch is NULL")
+
+int snow_gpu_batch_add_scene(snow_gpu_batch* batch, const double* records, int64_t n,
+                             const snow_step_params* params, const snow_collider* colliders,
+                             int n_colliders, int32_t* scene_id, void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    const int32_t id = batch->impl->add_scene(records, n, params, colliders, n_colliders, as_stream(stream));
+    if (scene_id) *scene_id = id;
+  });
+}
+int snow_gpu_batch_remove_scene(snow_gpu_batch* batch, int32_t scene_id) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->remove_scene(scene_id);
+  });
+}
+int snow_gpu_batch_set_params(snow_gpu_batch* batch, int32_t scene_id, const snow_step_params* params,
+                              const snow_collider* colliders, int n_colliders) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->set_params(scene_id, params, colliders, n_colliders);
+  });
+}
+int snow_gpu_batch_upload(snow_gpu_batch* batch, int32_t scene_id, const double* records, int64_t n,
+                          void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->upload(scene_id, records, n, as_stream(stream));
+  });
+}
+int snow_gpu_batch_download(snow_gpu_batch* batch, int32_t scene_id, double* records, int64_t n,
+                            void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->download(scene_id, records, n, as_stream(stream));
+  });
+}
+int snow_gpu_batch_setup(snow_gpu_batch* batch, int32_t scene_id, double grid_spacing, void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->setup(scene_id, grid_spacing, as_stream(stream));
+  });
+}
+int snow_gpu_batch_step(snow_gpu_batch* batch, int n_steps, snow_step_timings* timings, void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->step(n_steps, timings, as_stream(stream));
+  });
+}
+int snow_gpu_batch_scene_count(snow_gpu_batch* batch) {
+  return batch && batch->impl ? batch->impl->scene_count() : SNOW_E_ARG;
+}
+int64_t snow_gpu_batch_particles(snow_gpu_batch* batch) {
+  return batch && batch->impl ? batch->impl->particles() : SNOW_E_ARG;
+}
+int64_t snow_gpu_batch_device_bytes(snow_gpu_batch* batch) {
+  return batch && batch->impl ? batch->impl->device_bytes() : SNOW_E_ARG;
+}
+int snow_gpu_batch_status(snow_gpu_batch* batch, uint32_t* status, int64_t* used, int64_t* cap) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    if (status) *status = batch->impl->last_status();
+    if (used) *used = batch->impl->last_blocks();
+    if (cap) *cap = batch->impl->capacity_blocks();
+  });
+}
+int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->set_graphs(enable != 0);
+  });
+}
+
+// One-scene convenience entry points on host records (the literal drop-in:
+// upload, run, download on every call).
+static std::mutex g_single_mu;
+static std::unique_ptr<Batch> g_single;
+
+static Batch& single_batch() {
+  if (!g_single) g_single = std::make_unique<Batch>(SNOW_FP64);
+  return *g_single;
+}
+
+int snow_gpu_setup(double* records, int64_t n, double grid_spacing) {
+  std::lock_guard<std::mutex> lk(g_single_mu);
+  return guarded([&] {
+    if (n < 0 || (n > 0 && !records)) throw Error(SNOW_E_ARG, "bad particle array");
+    if (n == 0) return;
+    Batch& b = single_batch();
+    b.clear();
+    snow_step_params p{};
+    p.grid_spacing = grid_spacing;
+    const int32_t id = b.add_scene(records, n, &p, nullptr, 0, nullptr);
+    b.setup(id, grid_spacing, nullptr);
+    b.download(id, records, n, nullptr);
+  });
+}
+
+int snow_gpu_step(double* records, int64_t n, const snow_step_params* params,
+                  const snow_collider* colliders, int n_colliders, int n_steps,
+                  snow_step_timings* timings) {
+  std::lock_guard<std::mutex> lk(g_single_mu);
+  return guarded([&] {
+    if (n < 0 || (n > 0 && !records)) throw Error(SNOW_E_ARG, "bad particle array");
+    if (n == 0 || n_steps == 0) return;
+    Batch& b = single_batch();
+    int32_t id;
+    if (b.scene_count() == 1 && b.particles() == n) {
+      id = b.first_id();
+      b.set_params(id, params, colliders, n_colliders);
+      b.upload(id, records, n, nullptr);
+    } else {
+      b.clear();
+      id = b.add_scene(records, n, params, colliders, n_colliders, nullptr);
+    }
+    b.step(n_steps, timings, nullptr);
+    b.download(id, records, n, nullptr);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,148 @@
+// Host-side batch engine (C++ view of include/snow_gpu.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "snow_batch.cuh"
+#include "snow_gpu.h"
+
+namespace snow {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+int set_error(int code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+
+// One scene: its particle planes (two buffers), parameters and colliders.
+struct Scene {
+  int32_t sid = 0;  // handle returned to the caller
+  int64_t n = 0;
+  int64_t stride = 0;
+  int cur = 0;
+  void* r[2] = {nullptr, nullptr};
+  double* fp[2] = {nullptr, nullptr};
+  int32_t* id[2] = {nullptr, nullptr};
+  snow_step_params params{};
+  std::vector<Collider> colliders;
+};
+
+class Batch {
+ public:
+  explicit Batch(int precision);
+  ~Batch();
+  Batch(const Batch&) = delete;
+  Batch& operator=(const Batch&) = delete;
+
+  int32_t add_scene(const double* records, int64_t n, const snow_step_params* params,
+                    const snow_collider* colliders, int n_colliders, cudaStream_t s);
+  void remove_scene(int32_t id);
+  void set_params(int32_t id, const snow_step_params* params, const snow_collider* c, int n);
+  void upload(int32_t id, const double* records, int64_t n, cudaStream_t s);
+  void download(int32_t id, double* records, int64_t n, cudaStream_t s);
+  void setup(int32_t id, double dx, cudaStream_t s);
+  void step(int n_steps, snow_step_timings* timings, cudaStream_t s);
+
+  int scene_count() const { return (int)scenes_.size(); }
+  int64_t particles() const {
+    int64_t t = 0;
+    for (auto& s : scenes_) t += s->n;
+    return t;
+  }
+  int32_t first_id() const { return scenes_.empty() ? -1 : scenes_.front()->sid; }
+  void clear() {
+    while (!scenes_.empty()) remove_scene(scenes_.back()->sid);
+  }
+  uint32_t last_status() const { return last_status_; }
+  int64_t last_blocks() const { return last_blocks_; }
+  int64_t capacity_blocks() const { return cap_blocks_; }
+  void set_graphs(bool on) {
+    use_graphs_ = on;
+    drop_graph();
+  }
+  int64_t device_bytes() const;
+  int precision() const { return prec_; }
+  Scene* find(int32_t id);
+
+  // Buffers for the single-stage entry points.
+  BatchDev dev(SceneDev* scenes, int num_scenes, int64_t total) const;
+  SceneDev* device_scenes() const { return d_scenes_; }
+  int device_scene_count() const { return num_dev_scenes_; }
+  void prepare(cudaStream_t s);
+  int64_t total() const { return total_; }
+  void check_status();
+  Counters* host_counters() { return h_ctr_; }
+  Counters* device_counters() { return d_ctr_; }
+  void set_last_status(uint32_t st) { last_status_ = st; }
+
+ private:
+  void free_scene(Scene& s);
+  void free_particle_buffers();
+  void free_grid();
+  void drop_graph();
+  void ensure_staging(int64_t n);
+  void ensure_particle_buffers(int64_t total);
+  void ensure_grid(int64_t blocks);
+  void set_colliders(Scene& sc, const snow_collider* c, int n);
+  SceneDev scene_dev(const Scene& sc, int64_t begin) const;
+  void rebuild(cudaStream_t s);
+  void refresh_params(cudaStream_t s);
+  template <typename R>
+  void launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev);
+
+  int prec_;
+  size_t rsize_;
+  std::vector<std::unique_ptr<Scene>> scenes_;
+  int32_t next_id_ = 0;
+  bool dirty_ = true, boxes_dirty_ = true, params_dirty_ = false;
+  bool use_graphs_ = true;
+  int64_t total_ = 0;
+  int num_dev_scenes_ = 0;
+
+  SceneDev* d_scenes_ = nullptr;
+  int d_scenes_cap_ = 0;
+  SceneDev* d_tmp_scene_ = nullptr;
+  Collider* d_coll_ = nullptr;
+  int d_coll_cap_ = 0;
+  Counters* d_ctr_ = nullptr;
+  Counters* h_ctr_ = nullptr;
+
+  uint32_t* keys_[2] = {nullptr, nullptr};
+  uint32_t* vals_[2] = {nullptr, nullptr};
+  uint32_t* hist_ = nullptr;
+  uint32_t* digit_total_ = nullptr;
+  int64_t cap_p_ = 0;
+  int ntiles_cap_ = 0;
+
+  uint32_t* hkeys_ = nullptr;
+  int32_t* hvals_ = nullptr;
+  uint32_t hcap_ = 0;
+  int32_t cap_blocks_ = 0;
+  int4* blk_ = nullptr;
+  uint32_t* blk_key_ = nullptr;
+  int32_t* pblk_start_ = nullptr;
+  int32_t* pblk_end_ = nullptr;
+  void* acc_ = nullptr;
+  void* vel_ = nullptr;
+
+  double* staging_ = nullptr;
+  int64_t staging_cap_ = 0;
+
+  cudaGraphExec_t gexec_ = nullptr;
+  cudaStream_t own_stream_ = nullptr;
+  uint32_t last_status_ = 0;
+  int64_t last_blocks_ = 0;
+
+ public:
+  void ensure_grid_public(int64_t blocks) { ensure_grid(blocks); }
+  void ensure_particle_buffers_public(int64_t total) { ensure_particle_buffers(total); }
+};
+
+}  // namespace snow

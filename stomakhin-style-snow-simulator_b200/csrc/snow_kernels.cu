@@ -1,0 +1,859 @@
+// The explicit MPM snow step as fused sm_100a kernels over a batch of scenes.
+//
+//   keyspace     (1 block)  per-scene key boxes and key bases, sort bit count,
+//                            counter resets
+//   keys         (1/particle) block key + cell of every particle
+//   radix_sort   (radix_sort.cu) stable sort of (key, particle) pairs
+//   blocks_a     (1/particle) one grid block per run of equal block keys,
+//                            inserted into the block hash table
+//   blocks_b     (8/block)   the +{0,1}^3 neighbour blocks the stencils reach
+//   p2g          (persistent, 1 CTA per particle block)
+//                            stencil weights, hardening, stress, and the
+//                            scatter of mass, momentum and force into a shared
+//                            8x8x8-node tile; one global atomic per touched node
+//                            per block when the tile is flushed
+//   grid_update  (1/node)    v = p/m + dt (f/m + g), collisions at the node,
+//                            the FLIP increment, accumulators re-zeroed
+//   g2p          (persistent, 1 CTA per particle block)
+//                            gather of grad v, PIC and FLIP terms from a shared
+//                            tile; elastoplastic update; PIC/FLIP blend; particle
+//                            collisions; advection; block-sorted write-back and
+//                            the bounding box for the next step
+//   finish       (1 block)   swap the particle buffers
+//
+// Reference stages (src/grid.cpp:359-450): stencil = keys/sort/blocks,
+// P2G + force_constitutive + force_grid_accumulation = p2g, grid_velocity +
+// grid_collisions = grid_update, stress_update + G2P + particle_collisions +
+// position_update = g2p.
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdio>
+
+#include "snow_batch.cuh"
+
+namespace snow {
+
+int radix_tiles(int64_t n);
+
+namespace {
+
+constexpr int kTileN = 544;  // 8 x 8 x 8 node tile, z stride padded to 68
+SNOW_HD int tile_index(int x, int y, int z) { return x + 8 * y + 68 * z; }
+
+__device__ __forceinline__ const uint32_t* sorted_keys(const BatchDev& b) {
+  const uint32_t passes = (b.ctr->sort_bits + 7) / 8;
+  return b.keys[passes & 1];
+}
+__device__ __forceinline__ const uint32_t* sorted_vals(const BatchDev& b) {
+  const uint32_t passes = (b.ctr->sort_bits + 7) / 8;
+  return b.vals[passes & 1];
+}
+__device__ __forceinline__ void flag(const BatchDev& b, uint32_t bit) { atomicOr(&b.ctr->status, bit); }
+
+// Block coordinate of the particle at x (floor division of the stencil base by 4).
+template <typename R>
+__device__ __forceinline__ int block_coord(R x, R dx, int& cell) {
+  const int base = stencil_base(x / dx);
+  cell = base & 3;
+  return base >> 2;
+}
+
+template <typename R>
+struct PlaneView {
+  const R* r;
+  const double* fp;
+  const int32_t* id;
+  int64_t st;
+  __device__ R at(int plane, int64_t i) const { return r[plane * st + i]; }
+};
+
+// ------------------------------------------------------------------ bbox init
+template <typename R>
+__global__ void k_bbox_init(const BatchDev b) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < b.total;
+  int s = 0;
+  int c[3] = {INT_MAX, INT_MAX, INT_MAX};
+  int hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  if (valid) {
+    s = scene_of(b, t);
+    const SceneDev& sc = b.scenes[s];
+    const R* r = (const R*)sc.r[sc.cur];
+    const int64_t i = t - sc.begin;
+    for (int a = 0; a < 3; ++a) {
+      const R x = r[(PX + a) * sc.stride + i];
+      if (!isfinite((double)x)) {
+        flag(b, ST_NONFINITE);
+        continue;
+      }
+      int cell;
+      c[a] = hi[a] = block_coord(x, (R)sc.dx, cell);
+    }
+  }
+  if (!valid) return;
+  SceneDev& sc = b.scenes[s];
+  for (int a = 0; a < 3; ++a) {
+    if (c[a] != INT_MAX) atomicMin(&sc.nb_lo[a], c[a]);
+    if (hi[a] != INT_MIN) atomicMax(&sc.nb_hi[a], hi[a]);
+  }
+}
+
+// ------------------------------------------------------------------ keyspace
+__global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
+  __shared__ unsigned long long s_carry;
+  __shared__ unsigned long long s_warp[8];
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < b.num_scenes; base += 256) {
+    const int s = base + threadIdx.x;
+    unsigned long long cnt = 0;
+    if (s < b.num_scenes) {
+      SceneDev& sc = b.scenes[s];
+      bool empty = false;
+      for (int a = 0; a < 3; ++a) {
+        const int lo = sc.nb_lo[a], hi = sc.nb_hi[a];
+        if (lo > hi) empty = true;
+        sc.lo[a] = lo;
+        sc.dim[a] = empty ? 0 : (hi - lo + 2);  // +1 block of margin for the neighbours
+      }
+      if (empty) {
+        for (int a = 0; a < 3; ++a) sc.dim[a] = 0;
+      }
+      cnt = (unsigned long long)sc.dim[0] * sc.dim[1] * sc.dim[2];
+      for (int a = 0; a < 3; ++a) {
+        sc.nb_lo[a] = INT_MAX;
+        sc.nb_hi[a] = INT_MIN;
+      }
+    }
+    // inclusive scan of cnt over the block
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long x = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    unsigned long long before = 0;
+    for (int w = 0; w < warp; ++w) before += s_warp[w];
+    const unsigned long long incl = s_carry + before + x;
+    if (s < b.num_scenes) {
+      SceneDev& sc = b.scenes[s];
+      const unsigned long long kb = incl - cnt;
+      sc.key_base = (uint32_t)(kb > 0xFFFFFFFFull ? 0xFFFFFFFFull : kb);
+      sc.key_count = (uint32_t)(cnt > 0xFFFFFFFFull ? 0xFFFFFFFFull : cnt);
+    }
+    __syncthreads();
+    if (threadIdx.x == 255) s_carry = incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const unsigned long long total = s_carry;
+    uint32_t bits = 6;
+    if (total > (1ull << 26)) {
+      atomicOr(&b.ctr->status, ST_KEY_OVERFLOW);
+      bits = 32;
+    } else {
+      uint32_t kb = 0;
+      while ((1ull << kb) < total) ++kb;
+      bits += kb;
+    }
+    Counters* c = b.ctr;
+    c->sort_bits = bits;
+    c->n_pblocks = 0;
+    c->n_halo = 0;
+    c->work_p2g = c->work_grid = c->work_g2p = c->work_aux = 0;
+  }
+}
+
+// ---------------------------------------------------------------------- keys
+template <typename R>
+__global__ void __launch_bounds__(256) k_keys(const BatchDev b) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.total) return;
+  const int s = scene_of(b, t);
+  const SceneDev& sc = b.scenes[s];
+  const R* r = (const R*)sc.r[sc.cur];
+  const int64_t i = t - sc.begin;
+  const R dx = (R)sc.dx;
+  int blk[3], cell[3];
+  bool ok = true;
+  for (int a = 0; a < 3; ++a) {
+    const R x = r[(PX + a) * sc.stride + i];
+    if (!isfinite((double)x)) {
+      ok = false;
+      blk[a] = sc.lo[a];
+      cell[a] = 0;
+      continue;
+    }
+    blk[a] = block_coord(x, dx, cell[a]);
+    if (blk[a] < sc.lo[a] || blk[a] > sc.lo[a] + sc.dim[a] - 2) {
+      ok = false;
+      blk[a] = sc.lo[a];
+    }
+  }
+  if (!ok) flag(b, ST_OUT_OF_BOX);
+  const uint32_t bk = block_key(sc, blk[0], blk[1], blk[2]);
+  b.keys[0][t] = (bk << 6) | (uint32_t)(cell[0] + 4 * cell[1] + 16 * cell[2]);
+  b.vals[0][t] = (uint32_t)i;
+}
+
+// -------------------------------------------------------------------- blocks
+__device__ __forceinline__ bool hash_insert_new(const BatchDev& b, uint32_t key, uint32_t& slot_out,
+                                                bool& created) {
+  uint32_t slot = hash32(key) & b.hmask;
+  for (uint32_t probe = 0; probe <= b.hmask; ++probe) {
+    const uint32_t prev = atomicCAS(&b.hkeys[slot], kEmptyKey, key);
+    if (prev == kEmptyKey || prev == key) {
+      slot_out = slot;
+      created = prev == kEmptyKey;
+      return true;
+    }
+    slot = (slot + 1) & b.hmask;
+  }
+  flag(b, ST_HASH_FULL);
+  return false;
+}
+
+__device__ __forceinline__ int4 decode_block(const SceneDev& sc, uint32_t bk, int s) {
+  uint32_t local = bk - sc.key_base;
+  const int bx = sc.lo[0] + (int)(local % (uint32_t)sc.dim[0]);
+  local /= (uint32_t)sc.dim[0];
+  const int by = sc.lo[1] + (int)(local % (uint32_t)sc.dim[1]);
+  const int bz = sc.lo[2] + (int)(local / (uint32_t)sc.dim[1]);
+  return make_int4(bx, by, bz, s);
+}
+
+__global__ void __launch_bounds__(256) k_blocks_a(const BatchDev b) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.total) return;
+  const uint32_t* K = sorted_keys(b);
+  const uint32_t bk = K[t] >> 6;
+  if (t > 0 && (K[t - 1] >> 6) == bk) return;
+  const uint32_t pb = atomicAdd(&b.ctr->n_pblocks, 1u);
+  if ((int64_t)pb >= b.cap_blocks) {
+    flag(b, ST_BLOCK_OVERFLOW);
+    return;
+  }
+  const int s = scene_of(b, t);
+  b.pblk_start[pb] = (int32_t)t;
+  b.blk_key[pb] = bk;
+  b.blk[pb] = decode_block(b.scenes[s], bk, s);
+  uint32_t slot;
+  bool created;
+  if (hash_insert_new(b, bk, slot, created)) b.hvals[slot] = (int32_t)pb;
+}
+
+__global__ void __launch_bounds__(256) k_blocks_b(const BatchDev b) {
+  const uint32_t npb = min(b.ctr->n_pblocks, (uint32_t)b.cap_blocks);
+  const uint32_t* K = sorted_keys(b);
+  const int64_t work = (int64_t)npb * 8;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < work;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t pb = (uint32_t)(e >> 3);
+    const int d = (int)(e & 7);
+    const int4 bc = b.blk[pb];
+    if (d == 0) {
+      // end of the particle run of this block: first key above (bk << 6) | 63
+      const uint32_t lim = (b.blk_key[pb] << 6) | 63u;
+      int64_t lo = b.pblk_start[pb], hi = b.total;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (K[mid] <= lim) lo = mid + 1; else hi = mid;
+      }
+      b.pblk_end[pb] = (int32_t)lo;
+      continue;
+    }
+    const SceneDev& sc = b.scenes[bc.w];
+    const int nx = bc.x + (d & 1), ny = bc.y + ((d >> 1) & 1), nz = bc.z + (d >> 2);
+    const uint32_t nk = block_key(sc, nx, ny, nz);
+    uint32_t slot;
+    bool created;
+    if (!hash_insert_new(b, nk, slot, created) || !created) continue;
+    const uint32_t id = npb + atomicAdd(&b.ctr->n_halo, 1u);
+    if ((int64_t)id >= b.cap_blocks) {
+      flag(b, ST_BLOCK_OVERFLOW);
+      b.hvals[slot] = -1;
+      continue;
+    }
+    b.hvals[slot] = (int32_t)id;
+    b.blk[id] = make_int4(nx, ny, nz, bc.w);
+    b.blk_key[id] = nk;
+  }
+}
+
+// Number of grid blocks this step.
+__device__ __forceinline__ uint32_t num_blocks(const BatchDev& b) {
+  return min(b.ctr->n_pblocks + b.ctr->n_halo, (uint32_t)b.cap_blocks);
+}
+__device__ __forceinline__ uint32_t num_pblocks(const BatchDev& b) {
+  return min(b.ctr->n_pblocks, (uint32_t)b.cap_blocks);
+}
+
+// Shared per-block header for the particle-block kernels.
+struct BlockHeader {
+  int32_t blk, start, end, scene;
+  int32_t bx, by, bz;
+  int32_t nbr[8];
+};
+
+// Claims the next particle block for this CTA; returns false when none is left.
+template <bool kNeedNbr>
+__device__ __forceinline__ bool claim_block(const BatchDev& b, uint32_t* counter, BlockHeader& h) {
+  __syncthreads();
+  if (threadIdx.x == 0) h.blk = (int32_t)atomicAdd(counter, 1u);
+  __syncthreads();
+  const uint32_t npb = num_pblocks(b);
+  if ((uint32_t)h.blk >= npb) return false;
+  if (threadIdx.x == 0) {
+    const int4 bc = b.blk[h.blk];
+    h.start = b.pblk_start[h.blk];
+    h.end = b.pblk_end[h.blk];
+    h.scene = bc.w;
+    h.bx = bc.x;
+    h.by = bc.y;
+    h.bz = bc.z;
+  }
+  __syncthreads();
+  if (kNeedNbr && threadIdx.x < 8) {
+    const int d = threadIdx.x;
+    const SceneDev& sc = b.scenes[h.scene];
+    const uint32_t nk = block_key(sc, h.bx + (d & 1), h.by + ((d >> 1) & 1), h.bz + (d >> 2));
+    const int32_t id = hash_find(b, nk);
+    if (id < 0) flag(b, ST_LOOKUP_MISS);
+    h.nbr[d] = id;
+  }
+  __syncthreads();
+  return true;
+}
+
+// Tile position of local node `node` (0..63) of neighbour d; false if outside
+// the 7x7x7 region a particle block's stencils can reach.
+__device__ __forceinline__ bool tile_of(int d, int node, int& t) {
+  const int x = 4 * (d & 1) + (node & 3);
+  const int y = 4 * ((d >> 1) & 1) + ((node >> 2) & 3);
+  const int z = 4 * (d >> 2) + (node >> 4);
+  t = tile_index(x, y, z);
+  return x <= 6 && y <= 6 && z <= 6;
+}
+
+// -------------------------------------------------------------------- P2G
+template <typename R, int MODE>
+struct P2GChannels {
+  static constexpr int n = MODE == P2G_MASS ? 1 : (MODE == P2G_MASS_MOMENTUM ? 4 : 7);
+};
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
+  constexpr int NCH = P2GChannels<R, MODE>::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][kTileN]
+  __shared__ BlockHeader h;
+  __shared__ int32_t s_stride;
+  R* acc = (R*)b.acc;
+  const int64_t plane = (int64_t)b.cap_blocks * 64;
+
+  while (claim_block<true>(b, &b.ctr->work_p2g, h)) {
+    for (int e = threadIdx.x; e < NCH * kTileN; e += blockDim.x) tile[e] = R(0);
+    const int n = h.end - h.start;
+    if (threadIdx.x == 0) {
+      // Spread consecutive threads over different cells: thread k takes the
+      // (k * S mod n)-th particle of the cell-sorted run, S odd, coprime with n,
+      // about the mean particles per cell.
+      int S = n / 64;
+      S |= 1;
+      auto gcd = [](int a, int c) {
+        while (c) {
+          const int t = a % c;
+          a = c;
+          c = t;
+        }
+        return a;
+      };
+      while (n > 0 && gcd(S, n) != 1) S += 2;
+      s_stride = S;
+    }
+    __syncthreads();
+    const SceneDev& sc = b.scenes[h.scene];
+    const R dx = (R)sc.dx;
+    const PlaneView<R> pv{(const R*)sc.r[sc.cur], sc.fp[sc.cur], sc.id[sc.cur], sc.stride};
+    const uint32_t* vals = sorted_vals(b);
+    const int S = s_stride;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int j = h.start + (int)(((int64_t)k * S) % n);
+      const int64_t i = vals[j];
+      const R x0 = pv.at(PX, i), x1 = pv.at(PX + 1, i), x2 = pv.at(PX + 2, i);
+      const AxisWeights<R> wx = axis_weights(x0, dx), wy = axis_weights(x1, dx), wz = axis_weights(x2, dx);
+      const int tx = wx.base - 4 * h.bx, ty = wy.base - 4 * h.by, tz = wz.base - 4 * h.bz;
+      if ((unsigned)tx > 3u || (unsigned)ty > 3u || (unsigned)tz > 3u) {
+        flag(b, ST_OUT_OF_BOX);  // non-finite or mis-sorted particle: never index the tile with it
+        continue;
+      }
+      const R m = pv.at(PM, i);
+      R mv[3] = {R(0), R(0), R(0)};
+      if constexpr (MODE == P2G_FULL || MODE == P2G_MASS_MOMENTUM) {
+        mv[0] = m * pv.at(PV, i);
+        mv[1] = m * pv.at(PV + 1, i);
+        mv[2] = m * pv.at(PV + 2, i);
+      }
+      Sym3<R> M{};
+      if constexpr (MODE == P2G_FULL || MODE == P2G_FORCE) {
+        M3<R> FE;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) FE.a[e] = pv.at(PFE + e, i);
+        M3<double> FP;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) FP.a[e] = pv.fp[e * pv.st + i];
+        const double hard = exp(sc.xi * (1.0 - det3(FP)));
+        M = force_matrix<R>(FE, pv.at(PVOL, i), (R)sc.mu0, (R)sc.lambda0, (R)hard);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const R A = wx.w[a] * wy.w[c];
+          const R Bx = wx.dw[a] * wy.w[c];
+          const R By = wx.w[a] * wy.dw[c];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int t = tile_index(tx + a, ty + c, tz + e);
+            const R w = A * wz.w[e];
+            if constexpr (MODE != P2G_FORCE) atomicAdd(&tile[t], w * m);
+            if constexpr (MODE == P2G_FULL || MODE == P2G_MASS_MOMENTUM) {
+              atomicAdd(&tile[kTileN + t], w * mv[0]);
+              atomicAdd(&tile[2 * kTileN + t], w * mv[1]);
+              atomicAdd(&tile[3 * kTileN + t], w * mv[2]);
+            }
+            if constexpr (MODE == P2G_FULL || MODE == P2G_FORCE) {
+              const R gx = Bx * wz.w[e], gy = By * wz.w[e], gz = A * wz.dw[e];
+              constexpr int f0 = MODE == P2G_FULL ? 4 : 4;
+              atomicAdd(&tile[f0 * kTileN + t], M.xx * gx + M.xy * gy + M.xz * gz);
+              atomicAdd(&tile[(f0 + 1) * kTileN + t], M.xy * gx + M.yy * gy + M.yz * gz);
+              atomicAdd(&tile[(f0 + 2) * kTileN + t], M.xz * gx + M.yz * gy + M.zz * gz);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // Flush: one global atomic per touched node and channel.
+    for (int e = threadIdx.x; e < 8 * 64; e += blockDim.x) {
+      const int d = e >> 6, node = e & 63;
+      int t;
+      if (!tile_of(d, node, t)) continue;
+      const int32_t nb = h.nbr[d];
+      if (nb < 0) continue;
+      const int64_t g = (int64_t)nb * 64 + node;
+      if constexpr (MODE == P2G_FORCE) {
+#pragma unroll
+        for (int ch = 4; ch < 7; ++ch) {
+          const R v = tile[ch * kTileN + t];
+          if (v != R(0)) atomicAdd(&acc[ch * plane + g], v);
+        }
+      } else {
+        bool any = false;
+#pragma unroll
+        for (int ch = 0; ch < NCH; ++ch) any |= tile[ch * kTileN + t] != R(0);
+        if (!any) continue;
+#pragma unroll
+        for (int ch = 0; ch < NCH; ++ch) atomicAdd(&acc[ch * plane + g], tile[ch * kTileN + t]);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------- grid update
+template <typename R>
+__global__ void __launch_bounds__(256) k_grid_update(const BatchDev b) {
+  R* acc = (R*)b.acc;
+  R* vel = (R*)b.vel;
+  const int64_t plane = (int64_t)b.cap_blocks * 64;
+  const int64_t work = (int64_t)num_blocks(b) * 64;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < work;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t blk = e >> 6;
+    const int node = (int)(e & 63);
+    const int4 bc = b.blk[blk];
+    const SceneDev& sc = b.scenes[bc.w];
+    const R m = acc[e];
+    R v[3] = {R(0), R(0), R(0)}, pm[3] = {R(0), R(0), R(0)};
+    {
+      const R p[3] = {acc[plane + e], acc[2 * plane + e], acc[3 * plane + e]};
+      const R f[3] = {acc[4 * plane + e], acc[5 * plane + e], acc[6 * plane + e]};
+      const R g[3] = {(R)sc.g[0], (R)sc.g[1], (R)sc.g[2]};
+      node_velocity(m, p, f, g, (R)sc.dt, v, pm);
+    }
+    const R dx = (R)sc.dx;
+    const R px = dx * (R)(4 * bc.x + (node & 3));
+    const R py = dx * (R)(4 * bc.y + ((node >> 2) & 3));
+    const R pz = dx * (R)(4 * bc.z + (node >> 4));
+    for (int c = 0; c < sc.coll_count; ++c) collide(b.colliders[sc.coll_begin + c], px, py, pz, v[0], v[1], v[2]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      vel[a * plane + e] = v[a];
+      vel[(3 + a) * plane + e] = m > R(0) ? v[a] - pm[a] : R(0);
+    }
+#pragma unroll
+    for (int ch = 0; ch < kAccCh; ++ch) acc[ch * plane + e] = R(0);
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_zero_grid(const BatchDev b) {
+  R* acc = (R*)b.acc;
+  const int64_t plane = (int64_t)b.cap_blocks * 64;
+  const int64_t work = (int64_t)num_blocks(b) * 64;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < work;
+       e += (int64_t)gridDim.x * blockDim.x)
+    for (int ch = 0; ch < kAccCh; ++ch) acc[ch * plane + e] = R(0);
+}
+
+// --------------------------------------------------------------------- G2P
+template <int MODE>
+struct G2PChannels {
+  static constexpr int n = MODE == G2P_VOLUME ? 1 : (MODE == G2P_STRESS ? 3 : 6);
+};
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(256) k_g2p(const BatchDev b) {
+  constexpr int NCH = G2PChannels<MODE>::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][kTileN]
+  __shared__ BlockHeader h;
+  const R* vel = (const R*)b.vel;
+  const R* acc = (const R*)b.acc;
+  const int64_t plane = (int64_t)b.cap_blocks * 64;
+  int bmin[3] = {INT_MAX, INT_MAX, INT_MAX}, bmax[3] = {INT_MIN, INT_MIN, INT_MIN};
+  int last_scene = -1;
+
+  while (claim_block<true>(b, &b.ctr->work_g2p, h)) {
+    // Stage the 7x7x7 nodes this block's stencils read.
+    for (int e = threadIdx.x; e < 8 * 64; e += blockDim.x) {
+      const int d = e >> 6, node = e & 63;
+      int t;
+      if (!tile_of(d, node, t)) continue;
+      const int32_t nb = h.nbr[d];
+      const int64_t g = (int64_t)(nb < 0 ? 0 : nb) * 64 + node;
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        R v;
+        if constexpr (MODE == G2P_VOLUME) v = acc[g];
+        else v = vel[ch * plane + g];
+        tile[ch * kTileN + t] = nb < 0 ? R(0) : v;
+      }
+    }
+    __syncthreads();
+    const int s = h.scene;
+    if (MODE == G2P_FULL && s != last_scene) {
+      // flush the bounding box of the previous scene
+      if (last_scene >= 0) {
+        SceneDev& ps = b.scenes[last_scene];
+        for (int a = 0; a < 3; ++a) {
+          int lo = bmin[a], hi = bmax[a];
+          for (int o = 16; o; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+          }
+          if ((threadIdx.x & 31) == 0) {
+            if (lo < *(volatile int*)&ps.nb_lo[a]) atomicMin(&ps.nb_lo[a], lo);
+            if (hi > *(volatile int*)&ps.nb_hi[a]) atomicMax(&ps.nb_hi[a], hi);
+          }
+          bmin[a] = INT_MAX;
+          bmax[a] = INT_MIN;
+        }
+      }
+      last_scene = s;
+    }
+    const SceneDev& sc = b.scenes[s];
+    const R dx = (R)sc.dx;
+    const int cur = sc.cur;
+    const PlaneView<R> pv{(const R*)sc.r[cur], sc.fp[cur], sc.id[cur], sc.stride};
+    const uint32_t* vals = sorted_vals(b);
+    const int n = h.end - h.start;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int j = h.start + k;
+      const int64_t i = vals[j];
+      R x[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) x[a] = pv.at(PX + a, i);
+      const AxisWeights<R> wx = axis_weights(x[0], dx), wy = axis_weights(x[1], dx), wz = axis_weights(x[2], dx);
+      const int tx = wx.base - 4 * h.bx, ty = wy.base - 4 * h.by, tz = wz.base - 4 * h.bz;
+      if ((unsigned)tx > 3u || (unsigned)ty > 3u || (unsigned)tz > 3u) {
+        flag(b, ST_OUT_OF_BOX);  // non-finite or mis-sorted particle: never index the tile with it
+        continue;
+      }
+
+      if constexpr (MODE == G2P_VOLUME) {
+        // calculate_volume (grid.cpp:138-160)
+        const double dx3 = pow((double)sc.dx, 3.0);
+        R density = R(0);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const R w = wx.w[a] * wy.w[c] * wz.w[e];
+              density += (tile[tile_index(tx + a, ty + c, tz + e)] * w) / (R)dx3;
+            }
+        R* rw = (R*)sc.r[cur];
+        rw[PVOL * sc.stride + i] = pv.at(PM, i) / density;
+        continue;
+      } else {
+        R gv[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};  // column-major
+        R vpic[3] = {R(0), R(0), R(0)}, dflip[3] = {R(0), R(0), R(0)};
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const R A = wx.w[a] * wy.w[c];
+            const R Bx = wx.dw[a] * wy.w[c];
+            const R By = wx.w[a] * wy.dw[c];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int t = tile_index(tx + a, ty + c, tz + e);
+              const R v0 = tile[t], v1 = tile[kTileN + t], v2 = tile[2 * kTileN + t];
+              if constexpr (MODE == G2P_FULL || MODE == G2P_STRESS) {
+                const R g0 = Bx * wz.w[e], g1 = By * wz.w[e], g2 = A * wz.dw[e];
+                gv[0] += v0 * g0; gv[1] += v1 * g0; gv[2] += v2 * g0;
+                gv[3] += v0 * g1; gv[4] += v1 * g1; gv[5] += v2 * g1;
+                gv[6] += v0 * g2; gv[7] += v1 * g2; gv[8] += v2 * g2;
+              }
+              if constexpr (MODE == G2P_FULL || MODE == G2P_VELOCITY) {
+                const R w = A * wz.w[e];
+                vpic[0] += w * v0;
+                vpic[1] += w * v1;
+                vpic[2] += w * v2;
+                dflip[0] += w * tile[3 * kTileN + t];
+                dflip[1] += w * tile[4 * kTileN + t];
+                dflip[2] += w * tile[5 * kTileN + t];
+              }
+            }
+          }
+        }
+        const R dt = (R)sc.dt;
+        M3<R> FEn;
+        M3<double> FPn;
+        if constexpr (MODE == G2P_FULL || MODE == G2P_STRESS) {
+          // stress_update (grid.cpp:277-285)
+          M3<R> FE, L;
+#pragma unroll
+          for (int e = 0; e < 9; ++e) {
+            FE.a[e] = pv.at(PFE + e, i);
+            L.a[e] = dt * gv[e];
+          }
+          L.a[0] += R(1);
+          L.a[4] += R(1);
+          L.a[8] += R(1);
+          FEn = mat_mul(L, FE);
+          Sym3<R> Dinv;
+          bool clamped;
+          plastic_projection(FEn, R(1) - (R)sc.theta_c, R(1) + (R)sc.theta_s, Dinv, clamped);
+#pragma unroll
+          for (int e = 0; e < 9; ++e) FPn.a[e] = pv.fp[e * pv.st + i];
+          if (clamped) {
+            const double d[9] = {(double)Dinv.xx, (double)Dinv.xy, (double)Dinv.xz,
+                                 (double)Dinv.xy, (double)Dinv.yy, (double)Dinv.yz,
+                                 (double)Dinv.xz, (double)Dinv.yz, (double)Dinv.zz};
+            M3<double> Dm;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) Dm.a[e] = d[e];
+            FPn = mat_mul(Dm, FPn);
+          }
+        }
+        R vn[3];
+        if constexpr (MODE == G2P_FULL || MODE == G2P_VELOCITY) {
+          // G2P (grid.cpp:321-324)
+          const R alpha = (R)sc.alpha;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const R vflip = pv.at(PV + a, i) + dflip[a];
+            vn[a] = (R(1) - alpha) * vpic[a] + alpha * vflip;
+          }
+        }
+        if constexpr (MODE == G2P_STRESS) {
+          R* rw = (R*)sc.r[cur];
+          double* fw = sc.fp[cur];
+#pragma unroll
+          for (int e = 0; e < 9; ++e) {
+            rw[(PFE + e) * sc.stride + i] = FEn.a[e];
+            fw[e * sc.stride + i] = FPn.a[e];
+          }
+          continue;
+        }
+        if constexpr (MODE == G2P_VELOCITY) {
+          R* rw = (R*)sc.r[cur];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) rw[(PV + a) * sc.stride + i] = vn[a];
+          continue;
+        }
+        if constexpr (MODE == G2P_FULL) {
+          // particle_collisions (grid.cpp:327-333), position_update (grid.cpp:335-338)
+          for (int c = 0; c < sc.coll_count; ++c)
+            collide(b.colliders[sc.coll_begin + c], x[0], x[1], x[2], vn[0], vn[1], vn[2]);
+          R xn[3];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) xn[a] = x[a] + dt * vn[a];
+          const int64_t o = j - sc.begin;  // block-sorted slot in the other buffer
+          R* rw = (R*)sc.r[cur ^ 1];
+          double* fw = sc.fp[cur ^ 1];
+          const int64_t st = sc.stride;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            rw[(PX + a) * st + o] = xn[a];
+            rw[(PV + a) * st + o] = vn[a];
+          }
+          rw[PM * st + o] = pv.at(PM, i);
+          rw[PVOL * st + o] = pv.at(PVOL, i);
+#pragma unroll
+          for (int e = 0; e < 9; ++e) {
+            rw[(PFE + e) * st + o] = FEn.a[e];
+            fw[e * st + o] = FPn.a[e];
+          }
+          sc.id[cur ^ 1][o] = pv.id[i];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            if (isfinite((double)xn[a])) {
+              int cell;
+              const int bc = block_coord(xn[a], dx, cell);
+              bmin[a] = min(bmin[a], bc);
+              bmax[a] = max(bmax[a], bc);
+            } else {
+              flag(b, ST_NONFINITE);
+            }
+          }
+        }
+      }
+    }
+  }
+  if (MODE == G2P_FULL && last_scene >= 0) {
+    SceneDev& ps = b.scenes[last_scene];
+    for (int a = 0; a < 3; ++a) {
+      int lo = bmin[a], hi = bmax[a];
+      for (int o = 16; o; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      }
+      if ((threadIdx.x & 31) == 0) {
+        if (lo < *(volatile int*)&ps.nb_lo[a]) atomicMin(&ps.nb_lo[a], lo);
+        if (hi > *(volatile int*)&ps.nb_hi[a]) atomicMax(&ps.nb_hi[a], hi);
+      }
+    }
+  }
+}
+
+__global__ void k_finish(const BatchDev b) {
+  for (int s = threadIdx.x; s < b.num_scenes; s += blockDim.x) b.scenes[s].cur ^= 1;
+}
+
+// ------------------------------------------------------------ launch helpers
+template <typename K>
+int persistent_grid(K kernel, int threads, size_t smem) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  return per_sm * sm_count();
+}
+
+template <typename K>
+void set_smem(K kernel, size_t smem) {
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+}  // namespace
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+template <typename R>
+void StepLaunch<R>::bbox_init(const BatchDev& b, cudaStream_t s) {
+  if (b.total <= 0) return;
+  k_bbox_init<R><<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
+}
+template <typename R>
+void StepLaunch<R>::keyspace(const BatchDev& b, cudaStream_t s, bool) {
+  k_keyspace<<<1, 256, 0, s>>>(b);
+}
+template <typename R>
+void StepLaunch<R>::keys(const BatchDev& b, cudaStream_t s) {
+  if (b.total <= 0) return;
+  k_keys<R><<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
+}
+template <typename R>
+void StepLaunch<R>::blocks(const BatchDev& b, cudaStream_t s) {
+  if (b.total <= 0) return;
+  cudaMemsetAsync(b.hkeys, 0xFF, sizeof(uint32_t) * ((size_t)b.hmask + 1), s);
+  k_blocks_a<<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
+  k_blocks_b<<<2 * sm_count(), 256, 0, s>>>(b);
+}
+
+template <typename R, int MODE>
+static void launch_p2g(const BatchDev& b, cudaStream_t s) {
+  const size_t smem = sizeof(R) * P2GChannels<R, MODE>::n * kTileN;
+  static int grid = 0;
+  if (!grid) {
+    set_smem(k_p2g<R, MODE>, smem);
+    grid = persistent_grid(k_p2g<R, MODE>, 256, smem);
+  }
+  k_p2g<R, MODE><<<grid, 256, smem, s>>>(b);
+}
+template <typename R>
+void StepLaunch<R>::p2g(const BatchDev& b, int mode, cudaStream_t s) {
+  if (b.total <= 0) return;
+  switch (mode) {
+    case P2G_FULL: launch_p2g<R, P2G_FULL>(b, s); break;
+    case P2G_MASS: launch_p2g<R, P2G_MASS>(b, s); break;
+    case P2G_MASS_MOMENTUM: launch_p2g<R, P2G_MASS_MOMENTUM>(b, s); break;
+    case P2G_FORCE: launch_p2g<R, P2G_FORCE>(b, s); break;
+  }
+}
+template <typename R>
+void StepLaunch<R>::grid_update(const BatchDev& b, cudaStream_t s) {
+  if (b.total <= 0) return;
+  static int grid = 0;
+  if (!grid) grid = persistent_grid(k_grid_update<R>, 256, 0);
+  k_grid_update<R><<<grid, 256, 0, s>>>(b);
+}
+template <typename R>
+void StepLaunch<R>::zero_grid(const BatchDev& b, cudaStream_t s) {
+  if (b.total <= 0) return;
+  k_zero_grid<R><<<4 * sm_count(), 256, 0, s>>>(b);
+}
+template <typename R, int MODE>
+static void launch_g2p(const BatchDev& b, cudaStream_t s) {
+  const size_t smem = sizeof(R) * G2PChannels<MODE>::n * kTileN;
+  static int grid = 0;
+  if (!grid) {
+    set_smem(k_g2p<R, MODE>, smem);
+    grid = persistent_grid(k_g2p<R, MODE>, 256, smem);
+  }
+  k_g2p<R, MODE><<<grid, 256, smem, s>>>(b);
+}
+template <typename R>
+void StepLaunch<R>::g2p(const BatchDev& b, int mode, cudaStream_t s) {
+  if (b.total <= 0) return;
+  switch (mode) {
+    case G2P_FULL: launch_g2p<R, G2P_FULL>(b, s); break;
+    case G2P_VOLUME: launch_g2p<R, G2P_VOLUME>(b, s); break;
+    case G2P_STRESS: launch_g2p<R, G2P_STRESS>(b, s); break;
+    case G2P_VELOCITY: launch_g2p<R, G2P_VELOCITY>(b, s); break;
+  }
+}
+template <typename R>
+void StepLaunch<R>::finish(const BatchDev& b, cudaStream_t s) {
+  k_finish<<<1, 256, 0, s>>>(b);
+}
+
+template struct StepLaunch<double>;
+template struct StepLaunch<float>;
+
+}  // namespace snow

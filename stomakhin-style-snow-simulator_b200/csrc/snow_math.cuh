@@ -1,0 +1,316 @@
+// Per-particle and per-node arithmetic of the explicit MPM snow step, shared by
+// the fused kernels and the single-stage entry points (host + device).
+//
+// Formulas follow the reference solver src/grid.cpp line by line; where the GPU
+// form differs algebraically (never numerically beyond round-off) the comment
+// says how and why.
+#pragma once
+
+#include <cstdint>
+#include <cmath>
+
+#define SNOW_HD __host__ __device__ __forceinline__
+
+namespace snow {
+
+template <typename T>
+SNOW_HD T sgn(T x) {  // signum (grid.cpp:15-20)
+  return x > T(0) ? T(1) : (x < T(0) ? T(-1) : T(0));
+}
+
+// Cubic B-spline N(a, b) of |a - b| (grid.cpp:24-40).
+template <typename T>
+SNOW_HD T bspline(T a, T b) {
+  const T d = fabs(a - b);
+  if (d >= T(0) && d < T(1)) return T(0.5) * d * d * d - d * d + T(2.0 / 3.0);
+  if (d >= T(1) && d < T(2)) return T(-1.0 / 6.0) * d * d * d + d * d - T(2) * d + T(4.0 / 3.0);
+  return T(0);
+}
+
+// N_dash(node, x) = dN/dx (grid.cpp:42-58).
+template <typename T>
+SNOW_HD T bspline_slope(T node, T x) {
+  const T d = fabs(node - x);
+  if (d >= T(0) && d < T(1)) return (T(1.5) * d * d - T(2) * d) * sgn(x - node);
+  if (d >= T(1) && d < T(2)) return (T(-1.0 / 2.0) * d * d + T(2) * d - T(2)) * sgn(x - node);
+  return T(0);
+}
+
+// Lower stencil corner base = floor(x / dx) - 1 (grid.cpp:64-67).
+template <typename T>
+SNOW_HD int stencil_base(T gp) {
+  return static_cast<int>(floor(gp)) - 1;
+}
+
+// Weights and weight slopes of the 4 stencil nodes along one axis.
+// slope[i] = N_dash / dx, as build_stencil stores it (grid.cpp:80).
+template <typename T>
+struct AxisWeights {
+  T w[4];
+  T dw[4];
+  int base;
+};
+template <typename T>
+SNOW_HD AxisWeights<T> axis_weights(T x, T dx) {
+  AxisWeights<T> a;
+  const T gp = x / dx;
+  a.base = stencil_base(gp);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const T node = static_cast<T>(a.base + i);
+    a.w[i] = bspline(node, gp);
+    a.dw[i] = bspline_slope(node, gp) / dx;
+  }
+  return a;
+}
+
+// ----------------------------------------------------------------- 3x3 algebra
+// Matrices are column-major, m[c * 3 + r], like the reference's Eigen::Matrix3d.
+template <typename T>
+struct M3 {
+  T a[9];
+  SNOW_HD T& operator()(int r, int c) { return a[c * 3 + r]; }
+  SNOW_HD T operator()(int r, int c) const { return a[c * 3 + r]; }
+};
+
+template <typename T>
+SNOW_HD M3<T> mat_mul(const M3<T>& x, const M3<T>& y) {
+  M3<T> m;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) m(r, c) = x(r, 0) * y(0, c) + x(r, 1) * y(1, c) + x(r, 2) * y(2, c);
+  return m;
+}
+
+// Cofactor expansion along the first row.
+template <typename T>
+SNOW_HD T det3(const M3<T>& m) {
+  return m(0, 0) * (m(1, 1) * m(2, 2) - m(1, 2) * m(2, 1)) -
+         m(0, 1) * (m(1, 0) * m(2, 2) - m(1, 2) * m(2, 0)) +
+         m(0, 2) * (m(1, 0) * m(2, 1) - m(1, 1) * m(2, 0));
+}
+
+// Symmetric 3x3 as six scalars.
+template <typename T>
+struct Sym3 {
+  T xx, yy, zz, xy, xz, yz;
+};
+
+// Eigen-decomposition S = Q diag(lam) Q^T of a symmetric 3x3 by cyclic Jacobi
+// rotations (Golub & Van Loan, Matrix Computations, 4th ed., Alg. 8.5.2 with
+// the stable rotation of Alg. 8.5.1).  Converges quadratically; the sweep loop
+// stops when the off-diagonal mass falls below tol^2 of the diagonal mass.
+template <typename T>
+SNOW_HD void rotate_pq(T& app, T& aqq, T& apq, T& arp, T& arq, T q[9], int p, int qq) {
+  if (apq == T(0)) return;
+  const T theta = (aqq - app) / (T(2) * apq);
+  T t;
+  if (fabs(theta) > T(1e18))
+    t = T(0.5) / theta;
+  else
+    t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
+  const T c = T(1) / sqrt(t * t + T(1));
+  const T s = t * c;
+  app -= t * apq;
+  aqq += t * apq;
+  apq = T(0);
+  const T rp = arp, rq = arq;
+  arp = c * rp - s * rq;
+  arq = s * rp + c * rq;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const T vp = q[p * 3 + k], vq = q[qq * 3 + k];
+    q[p * 3 + k] = c * vp - s * vq;
+    q[qq * 3 + k] = s * vp + c * vq;
+  }
+}
+
+template <typename T>
+SNOW_HD void sym_eig3(Sym3<T> s, T lam[3], T q[9], T tol, int max_sweeps) {
+#pragma unroll
+  for (int i = 0; i < 9; ++i) q[i] = T(i % 4 == 0 ? 1 : 0);
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    const T off = s.xy * s.xy + s.xz * s.xz + s.yz * s.yz;
+    const T dia = s.xx * s.xx + s.yy * s.yy + s.zz * s.zz;
+    if (!(off > tol * tol * dia)) break;
+    rotate_pq(s.xx, s.yy, s.xy, s.xz, s.yz, q, 0, 1);  // (p,q)=(0,1), r=2
+    rotate_pq(s.xx, s.zz, s.xz, s.xy, s.yz, q, 0, 2);  // (0,2), r=1
+    rotate_pq(s.yy, s.zz, s.yz, s.xy, s.xz, q, 1, 2);  // (1,2), r=0
+  }
+  lam[0] = s.xx;
+  lam[1] = s.yy;
+  lam[2] = s.zz;
+}
+
+template <typename T>
+struct EigTol;
+template <>
+struct EigTol<double> {
+  static constexpr double tol = 1e-17;
+  static constexpr int sweeps = 12;
+};
+template <>
+struct EigTol<float> {
+  static constexpr float tol = 1e-8f;
+  static constexpr int sweeps = 8;
+};
+
+// Q diag(f) Q^T.
+template <typename T>
+SNOW_HD Sym3<T> spectral(const T q[9], const T f[3]) {
+  Sym3<T> r;
+  r.xx = q[0] * q[0] * f[0] + q[3] * q[3] * f[1] + q[6] * q[6] * f[2];
+  r.yy = q[1] * q[1] * f[0] + q[4] * q[4] * f[1] + q[7] * q[7] * f[2];
+  r.zz = q[2] * q[2] * f[0] + q[5] * q[5] * f[1] + q[8] * q[8] * f[2];
+  r.xy = q[0] * q[1] * f[0] + q[3] * q[4] * f[1] + q[6] * q[7] * f[2];
+  r.xz = q[0] * q[2] * f[0] + q[3] * q[5] * f[1] + q[6] * q[8] * f[2];
+  r.yz = q[1] * q[2] * f[0] + q[4] * q[5] * f[1] + q[7] * q[8] * f[2];
+  return r;
+}
+
+// --------------------------------------------------------- constitutive model
+// Force matrix of one particle, M = -V_p0 * P(F_E) * F_E^T (grid.cpp:174-176)
+// with the fixed-corotated stress P = 2 mu (F_E - R_E) + lambda (J-1) J F_E^-T
+// and exponential hardening mu = mu0 h, lambda = lambda0 h, h = exp(xi (1 - det F_P))
+// (grid.cpp:162-172).
+//
+// GPU form: P F^T = 2 mu (F F^T - R F^T) + lambda (J-1) J I, and R F^T = U S U^T
+// = sqrt(F F^T) for every SVD F = U S V^T with S >= 0 (R = U V^T, the reference's
+// polar factor from JacobiSVD).  So M needs only the symmetric square root of
+// B = F F^T (one 3x3 symmetric Jacobi eigensolve) and no inverse; M is symmetric.
+// `hardening` is exp(xi (1 - det F_P)) evaluated by the caller in double.
+template <typename T>
+SNOW_HD Sym3<T> force_matrix(const M3<T>& F, T V0, T mu0, T lambda0, T hardening) {
+  const T mu = mu0 * hardening;
+  const T lambda = lambda0 * hardening;
+  const T J = det3(F);
+  Sym3<T> B;
+  B.xx = F(0, 0) * F(0, 0) + F(0, 1) * F(0, 1) + F(0, 2) * F(0, 2);
+  B.yy = F(1, 0) * F(1, 0) + F(1, 1) * F(1, 1) + F(1, 2) * F(1, 2);
+  B.zz = F(2, 0) * F(2, 0) + F(2, 1) * F(2, 1) + F(2, 2) * F(2, 2);
+  B.xy = F(0, 0) * F(1, 0) + F(0, 1) * F(1, 1) + F(0, 2) * F(1, 2);
+  B.xz = F(0, 0) * F(2, 0) + F(0, 1) * F(2, 1) + F(0, 2) * F(2, 2);
+  B.yz = F(1, 0) * F(2, 0) + F(1, 1) * F(2, 1) + F(1, 2) * F(2, 2);
+  T lam[3], q[9];
+  sym_eig3(B, lam, q, EigTol<T>::tol, EigTol<T>::sweeps);
+  T sv[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) sv[i] = sqrt(lam[i] > T(0) ? lam[i] : T(0));
+  const Sym3<T> R = spectral(q, sv);  // R F^T = sqrt(F F^T)
+  const T two_mu = T(2) * mu;
+  const T vol = lambda * (J - T(1)) * J;
+  Sym3<T> M;
+  M.xx = -V0 * (two_mu * (B.xx - R.xx) + vol);
+  M.yy = -V0 * (two_mu * (B.yy - R.yy) + vol);
+  M.zz = -V0 * (two_mu * (B.zz - R.zz) + vol);
+  M.xy = -V0 * (two_mu * (B.xy - R.xy));
+  M.xz = -V0 * (two_mu * (B.xz - R.xz));
+  M.yz = -V0 * (two_mu * (B.yz - R.yz));
+  return M;
+}
+
+// Elastoplastic update (grid.cpp:277-285): trial F_E* = (I + dt grad v) F_E,
+// SVD F_E* = U S V^T, S clamped to [1 - theta_c, 1 + theta_s],
+// F_E <- U S_c V^T,  F_P <- F_E^-1 F_E* F_P.
+//
+// GPU form: with C = F_E*^T F_E* = V S^2 V^T (symmetric Jacobi eigensolve) and
+// D = V diag(s_c / s) V^T,  U S_c V^T = F_E* D  and  F_E^-1 F_E* = V diag(s / s_c) V^T
+// = D^-1, so F_E <- F_E* D and F_P <- D^-1 F_P: no U, no inverse.  Where no
+// singular value is clamped D = I and F_E* passes through unchanged.
+// Returns the trial F_E* in `FE` replaced by the projected F_E, and
+// D^-1 (symmetric) in `Dinv` for the caller to apply to F_P.
+template <typename T>
+SNOW_HD void plastic_projection(M3<T>& FE, T lo, T hi, Sym3<T>& Dinv, bool& clamped) {
+  Sym3<T> C;
+  C.xx = FE(0, 0) * FE(0, 0) + FE(1, 0) * FE(1, 0) + FE(2, 0) * FE(2, 0);
+  C.yy = FE(0, 1) * FE(0, 1) + FE(1, 1) * FE(1, 1) + FE(2, 1) * FE(2, 1);
+  C.zz = FE(0, 2) * FE(0, 2) + FE(1, 2) * FE(1, 2) + FE(2, 2) * FE(2, 2);
+  C.xy = FE(0, 0) * FE(0, 1) + FE(1, 0) * FE(1, 1) + FE(2, 0) * FE(2, 1);
+  C.xz = FE(0, 0) * FE(0, 2) + FE(1, 0) * FE(1, 2) + FE(2, 0) * FE(2, 2);
+  C.yz = FE(0, 1) * FE(0, 2) + FE(1, 1) * FE(1, 2) + FE(2, 1) * FE(2, 2);
+  T lam[3], q[9];
+  sym_eig3(C, lam, q, EigTol<T>::tol, EigTol<T>::sweeps);
+  T r[3], ri[3];
+  clamped = false;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const T s = sqrt(lam[i] > T(0) ? lam[i] : T(0));
+    const T sc = s < lo ? lo : (s > hi ? hi : s);  // std::clamp (grid.cpp:281-283)
+    if (sc != s) clamped = true;
+    r[i] = s > T(0) ? sc / s : T(1);
+    ri[i] = s > T(0) ? s / sc : T(1);
+  }
+  if (!clamped) {
+    Dinv = Sym3<T>{T(1), T(1), T(1), T(0), T(0), T(0)};
+    return;
+  }
+  const Sym3<T> D = spectral(q, r);
+  Dinv = spectral(q, ri);
+  M3<T> out;
+#pragma unroll
+  for (int rr = 0; rr < 3; ++rr) {
+    const T f0 = FE(rr, 0), f1 = FE(rr, 1), f2 = FE(rr, 2);
+    out(rr, 0) = f0 * D.xx + f1 * D.xy + f2 * D.xz;
+    out(rr, 1) = f0 * D.xy + f1 * D.yy + f2 * D.yz;
+    out(rr, 2) = f0 * D.xz + f1 * D.yz + f2 * D.zz;
+  }
+  FE = out;
+}
+
+// grid_velocity (grid.cpp:195-204): for a node with mass > 0,
+// v = p / m + dt (f / m + g); p / m is returned in `pm` for the FLIP increment.
+template <typename T>
+SNOW_HD bool node_velocity(T m, const T p[3], const T f[3], const T g[3], T dt, T v[3], T pm[3]) {
+  if (!(m > T(0))) return false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    pm[a] = p[a] / m;
+    v[a] = pm[a] + dt * ((f[a] / m) + g[a]);
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------ colliders
+// Collider record shared by host and device.  kind 0 = half-space bounded by a
+// plane (make_plane, src/collision.cpp:5-27: phi = n.(x - p), normal n).
+// `velocity` is the collider's rigid velocity (make_plane sets zero).
+struct Collider {
+  int32_t kind;
+  int32_t pad;
+  double point[3];
+  double normal[3];
+  double velocity[3];
+  double friction;
+  double param[2];  // reserved for other shapes
+};
+
+// collision_helper (grid.cpp:206-231): Coulomb friction, stick when
+// |v_t| <= -mu v_n, else slide.
+template <typename T>
+SNOW_HD void collide(const Collider& b, T x, T y, T z, T& vx, T& vy, T& vz) {
+  const T nx = T(b.normal[0]), ny = T(b.normal[1]), nz = T(b.normal[2]);
+  const T phi = nx * (x - T(b.point[0])) + ny * (y - T(b.point[1])) + nz * (z - T(b.point[2]));
+  if (!(phi <= T(0))) return;
+  const T cx = T(b.velocity[0]), cy = T(b.velocity[1]), cz = T(b.velocity[2]);
+  const T rx = vx - cx, ry = vy - cy, rz = vz - cz;
+  const T vn = rx * nx + ry * ny + rz * nz;
+  if (!(vn < T(0))) return;
+  const T tx = rx - vn * nx, ty = ry - vn * ny, tz = rz - vn * nz;
+  const T tn = sqrt(tx * tx + ty * ty + tz * tz);
+  const T mu = T(b.friction);
+  T ox, oy, oz;
+  if (tn <= T(-1) * mu * vn) {
+    ox = oy = oz = T(0);
+  } else {
+    const T k = mu * vn;
+    ox = tx + k * (tx / tn);
+    oy = ty + k * (ty / tn);
+    oz = tz + k * (tz / tn);
+  }
+  vx = ox + cx;
+  vy = oy + cy;
+  vz = oz + cz;
+}
+
+}  // namespace snow

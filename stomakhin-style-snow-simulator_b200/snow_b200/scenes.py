@@ -111,9 +111,15 @@ def _lattice_in(pred, lo, hi, h, jitter_frac, rng):
     return x + rng.uniform(-jitter_frac * h, jitter_frac * h, x.shape)
 
 
-def torus(center, R: float, r: float, n_target: int, rng, axis: int = 0) -> np.ndarray:
-    """Jittered lattice torus of about n_target particles; symmetry axis along `axis`."""
+def torus(center, R: float, r: float, n_target: int, rng, axis: int = 0, exact: bool = False):
+    """Jittered lattice torus of about n_target particles (exactly n_target with
+    `exact`: a slightly finer lattice, then a seeded subset in lattice order);
+    symmetry axis along `axis`."""
     h = (2 * math.pi ** 2 * R * r * r / n_target) ** (1 / 3)
+    if exact:
+        x, _ = torus(center, R, r, int(n_target * 1.03) + 64, rng, axis)
+        keep = np.sort(rng.choice(x.shape[0], n_target, replace=False))
+        return x[keep], h
     c = np.asarray(center)
     ext = R + r
     lo, hi = c - ext, c + ext
@@ -136,8 +142,8 @@ def tori_scene(n_per_torus: int = 325_000, steps: int = 500, seed: int = 1) -> S
     overlap at t = 0; spacing h = (2 pi^2 R r^2 / n)^(1/3) gives n per torus.
     """
     rng = np.random.default_rng(seed)
-    xa, h = torus((0.3, 0.5, 0.5), 0.15, 0.06, n_per_torus, rng)
-    xb, _ = torus((0.7, 0.5, 0.5), 0.15, 0.06, n_per_torus, rng)
+    xa, h = torus((0.3, 0.5, 0.5), 0.15, 0.06, n_per_torus, rng, exact=True)
+    xb, _ = torus((0.7, 0.5, 0.5), 0.15, 0.06, n_per_torus, rng, exact=True)
     m = 400.0 * h ** 3
     ra = records(xa, np.broadcast_to((8.0, 0.0, 0.0), xa.shape), m)
     rb = records(xb, np.broadcast_to((-8.0, 0.0, 0.0), xb.shape), m)

@@ -1,0 +1,147 @@
+"""ctypes access to the ORACLE (test infrastructure only).
+
+* ``oracle/liboracle.so``      the CPU restatement of the MPM step
+* ``oracle/_ref/libsnow_ref.so`` the reference's own sources compiled against
+  the project's Eigen-subset shim (present where it was built)
+
+Both take (n, 26) float64 particle records and the 11 step parameters of
+:meth:`snow_b200.scenes.Scene.params`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libsnow_ref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class _StepLib:
+    prefix = ""
+
+    def __init__(self, path: str):
+        self.L = ctypes.CDLL(path)
+        f = getattr(self.L, self.prefix + "_setup")
+        f.argtypes, f.restype = [_dp, ctypes.c_int64, ctypes.c_double], None
+        f = getattr(self.L, self.prefix + "_step")
+        f.argtypes = [_dp, ctypes.c_int64, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp]
+        f.restype = None
+
+    def setup(self, rec: np.ndarray, dx: float) -> np.ndarray:
+        out = np.ascontiguousarray(rec, dtype=np.float64).copy()
+        getattr(self.L, self.prefix + "_setup")(_p(out), out.shape[0], float(dx))
+        return out
+
+    def step(self, rec: np.ndarray, params, planes, steps: int = 1):
+        """Returns (new records, milliseconds[11]: ten stages, then the step loop's wall time)."""
+        out = np.ascontiguousarray(rec, dtype=np.float64).copy()
+        prm = np.ascontiguousarray(params, dtype=np.float64)
+        pl = np.ascontiguousarray(np.asarray(planes, dtype=np.float64).reshape(-1, 7))
+        ms = np.zeros(11)
+        getattr(self.L, self.prefix + "_step")(_p(out), out.shape[0], _p(prm), _p(pl), pl.shape[0],
+                                               int(steps), _p(ms))
+        return out, ms
+
+
+class Oracle(_StepLib):
+    prefix = "oracle"
+
+    def __init__(self, path: str = ORACLE_SO):
+        super().__init__(path)
+        L = self.L
+        L.oracle_N.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.oracle_N.restype = ctypes.c_double
+        L.oracle_N_dash.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.oracle_N_dash.restype = ctypes.c_double
+        L.oracle_grid_new.restype = ctypes.c_void_p
+        L.oracle_grid_free.argtypes = [ctypes.c_void_p]
+        L.oracle_grid_size.argtypes = [ctypes.c_void_p]
+        L.oracle_grid_size.restype = ctypes.c_int64
+        L.oracle_grid_export.argtypes = [ctypes.c_void_p, _ip, _dp]
+        L.oracle_grid_set.argtypes = [ctypes.c_void_p, _ip, _dp, ctypes.c_int64]
+        L.oracle_p2g.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_double]
+        L.oracle_calculate_volume.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_double]
+        L.oracle_force_calculation.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int64] + [ctypes.c_double] * 4
+        L.oracle_grid_velocity.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double]
+        L.oracle_grid_collisions.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_double]
+        L.oracle_stress_update.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int64] + [ctypes.c_double] * 4
+        L.oracle_g2p.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_double, ctypes.c_double]
+        L.oracle_particle_collisions.argtypes = [_dp, ctypes.c_int64, _dp, ctypes.c_int]
+        L.oracle_position_update.argtypes = [_dp, ctypes.c_int64, ctypes.c_double]
+        L.oracle_svd3.argtypes = [_dp, _dp, _dp, _dp]
+
+    def N(self, a, b):
+        return self.L.oracle_N(float(a), float(b))
+
+    def N_dash(self, a, b):
+        return self.L.oracle_N_dash(float(a), float(b))
+
+
+class OracleGrid:
+    """The oracle's std::unordered_map grid, as node lists (ijk, fields[10])."""
+
+    def __init__(self, oracle: Oracle):
+        self.o = oracle
+        self.h = ctypes.c_void_p(oracle.L.oracle_grid_new())
+
+    def __del__(self):
+        try:
+            self.o.L.oracle_grid_free(self.h)
+        except Exception:
+            pass
+
+    def set(self, ijk, fields):
+        ijk = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
+        f = np.ascontiguousarray(fields, dtype=np.float64).reshape(-1, 10)
+        self.o.L.oracle_grid_set(self.h, _p(ijk, _ip), _p(f), ijk.shape[0])
+        return self
+
+    def nodes(self):
+        n = self.o.L.oracle_grid_size(self.h)
+        ijk = np.zeros((n, 3), np.int32)
+        f = np.zeros((n, 10))
+        if n:
+            self.o.L.oracle_grid_export(self.h, _p(ijk, _ip), _p(f))
+        return ijk, f
+
+    def as_dict(self):
+        ijk, f = self.nodes()
+        return {tuple(int(v) for v in k): row for k, row in zip(ijk, f)}
+
+
+class Reference(_StepLib):
+    prefix = "ref"
+
+    def __init__(self, path: str = REF_SO):
+        super().__init__(path)
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def rel_err(a: np.ndarray, b: np.ndarray, floor: float = 1e-6) -> float:
+    """max_i ||a_i - b_i|| / max(||b_i||, floor) over rows."""
+    a = np.asarray(a).reshape(a.shape[0], -1)
+    b = np.asarray(b).reshape(b.shape[0], -1)
+    num = np.linalg.norm(a - b, axis=1)
+    den = np.maximum(np.linalg.norm(b, axis=1), floor)
+    return float(np.max(num / den)) if len(num) else 0.0
+
+
+QUANTITIES = {"x": slice(0, 3), "v": slice(3, 6), "F_P": slice(8, 17), "F_E": slice(17, 26)}
+
+
+def errors(a: np.ndarray, b: np.ndarray) -> dict:
+    """Per-quantity relative error of records a against reference records b."""
+    return {k: rel_err(a[:, s], b[:, s]) for k, s in QUANTITIES.items()}
