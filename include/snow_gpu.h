@@ -154,6 +154,21 @@ int snow_gpu_step(double* records, int64_t n, const snow_step_params* params,
                   const snow_collider* colliders, int n_colliders, int n_steps,
                   snow_step_timings* timings);
 
+/* Same as snow_gpu_step (FP64, host records in place) but allocates nothing:
+ * for callers that cannot call cudaMalloc (a plugin inside an application that
+ * owns the GPU's memory pool, or a loop that cannot afford an allocation's
+ * implicit synchronisation).  No counterpart in the reference solver.  All
+ * device scratch lives in one fixed file-scope device array (about 24 MB,
+ * held on every GPU that loads the library until exit), which limits a call
+ * to 16,384 particles, 2,048 grid blocks and 16 colliders; larger inputs
+ * return SNOW_E_ARG, a scene that outgrows the blocks SNOW_E_CAPACITY.  The
+ * first call on a device looks up the array's address (make it before any
+ * stream capture).  Calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.  Returns after the steps complete. */
+int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step_params* params,
+                          const snow_collider* colliders, int n_colliders, int n_steps,
+                          void* stream);
+
 /* ---- single stages (the reference's per-stage functions) ----------------
  * Grids cross as node lists: ijk[n][3] (int32) and fields[n][10] (double) =
  * mass, momentum[3], velocity[3], force[3].  Stage entry points run the same

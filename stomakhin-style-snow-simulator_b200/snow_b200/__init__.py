@@ -104,6 +104,8 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_setup": (ctypes.c_int, [_dp, i64, d]),
         "snow_gpu_step": (ctypes.c_int, [_dp, i64, ctypes.POINTER(StepParams), ctypes.POINTER(Collider),
                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(StepTimings)]),
+        "snow_gpu_step_noalloc": (ctypes.c_int, [_dp, i64, ctypes.POINTER(StepParams), ctypes.POINTER(Collider),
+                                                 ctypes.c_int, ctypes.c_int, vp]),
         "snow_gpu_stage_p2g": (ctypes.c_int, [_dp, i64, d, _ip, _dp, i64, _i64p]),
         "snow_gpu_stage_force": (ctypes.c_int, [_dp, i64, d, d, d, d, _ip, _dp, i64, _i64p]),
         "snow_gpu_stage_grid_velocity": (ctypes.c_int, [_dp, i64, _dp, d]),
