@@ -158,7 +158,7 @@ int snow_gpu_step(double* records, int64_t n, const snow_step_params* params,
  * for callers that cannot call cudaMalloc (a plugin inside an application that
  * owns the GPU's memory pool, or a loop that cannot afford an allocation's
  * implicit synchronisation).  No counterpart in the reference solver.  All
- * device scratch lives in one fixed file-scope device array (about 24 MB,
+ * device scratch lives in one fixed file-scope device array (about 26 MB,
  * held on every GPU that loads the library until exit), which limits a call
  * to 16,384 particles, 2,048 grid blocks and 16 colliders; larger inputs
  * return SNOW_E_ARG, a scene that outgrows the blocks SNOW_E_CAPACITY.  The

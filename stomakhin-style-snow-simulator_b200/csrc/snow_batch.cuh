@@ -1,9 +1,9 @@
 // Device-side data layout of a batch of independent snow scenes.
 //
 // Particles (per scene, double-buffered, structure of arrays):
-//   real planes  r[k * stride + i], k = 0..16: x0 x1 x2, v0 v1 v2, m, V_p0,
-//                F_E (9, column-major);  element type R (double, or float in
-//                the mixed-precision form)
+//   real planes  r[k * stride + i], k = 0..22: x0 x1 x2, v0 v1 v2, m, V_p0,
+//                F_E (9, column-major), the force matrix (6, see PFM);
+//                element type R (double, or float in the mixed-precision form)
 //   F_P planes   fp[k * stride + i], k = 0..8, always double
 //   id           original index of the particle within its scene
 // G2P writes each step's output in block-sorted order into the other buffer,
@@ -31,9 +31,11 @@
 
 namespace snow {
 
-constexpr int kRealPlanes = 17;
+constexpr int kRealPlanes = 23;
 constexpr int kFPPlanes = 9;
-enum : int { PX = 0, PV = 3, PM = 6, PVOL = 7, PFE = 8 };
+// PFM: the force matrix -V_p0 P F_E^T of the particle's current state (symmetric:
+// xx, yy, zz, xy, xz, yz), written by G2P for the next step's P2G.
+enum : int { PX = 0, PV = 3, PM = 6, PVOL = 7, PFE = 8, PFM = 17 };
 constexpr int kAccCh = 7;
 constexpr int kVelCh = 6;
 constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
@@ -74,6 +76,7 @@ struct Counters {
   uint32_t sort_bits;   // significant key bits this step
   uint32_t work_p2g, work_grid, work_g2p, work_aux;
   uint32_t status;
+  uint32_t n_items;     // (block, chunk) work items of the particle kernels
 };
 
 struct BatchDev {
@@ -96,6 +99,11 @@ struct BatchDev {
   uint32_t* blk_key;
   int32_t* pblk_start;
   int32_t* pblk_end;
+  // work items of P2G/G2P: (particle block, chunk), chunk = `chunk` consecutive
+  // particles of the block's sorted run, so that large blocks spread over CTAs
+  int2* items;
+  int32_t cap_items;
+  int32_t chunk;
   // grid
   void* acc;                // R[kAccCh][cap_blocks * 64]
   void* vel;                // R[kVelCh][cap_blocks * 64]
@@ -153,9 +161,10 @@ struct StepLaunch {
   static void zero_grid(const BatchDev& b, cudaStream_t s);
   static void finish(const BatchDev& b, cudaStream_t s);
   static void bbox_init(const BatchDev& b, cudaStream_t s);
+  static void prepare_force(const BatchDev& b, cudaStream_t s);
 };
 
-enum P2GMode : int { P2G_FULL = 0, P2G_MASS = 1, P2G_MASS_MOMENTUM = 2, P2G_FORCE = 3 };
+enum P2GMode : int { P2G_FULL = 0, P2G_MASS = 1, P2G_MASS_MOMENTUM = 2, P2G_FORCE = 3, P2G_PRE = 4 };
 enum G2PMode : int { G2P_FULL = 0, G2P_VOLUME = 1, G2P_STRESS = 2, G2P_VELOCITY = 3 };
 
 void radix_sort(const BatchDev& b, cudaStream_t s);

@@ -132,6 +132,8 @@ void Batch::free_grid() {
   dfree(pblk_end_);
   dfree(acc_);
   dfree(vel_);
+  dfree(items_);
+  cap_items_ = 0;
   cap_blocks_ = 0;
   hcap_ = 0;
 }
@@ -222,6 +224,7 @@ void Batch::set_params(int32_t id, const snow_step_params* params, const snow_co
   sc->params = *params;
   set_colliders(*sc, c, n);
   params_dirty_ = true;
+  force_dirty_ = true;
 }
 
 void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s) {
@@ -241,6 +244,7 @@ void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s)
                                                   sc->fp[sc->cur], sc->id[sc->cur], sc->stride);
   check_cuda(cudaGetLastError(), "upload kernel");
   boxes_dirty_ = true;
+  force_dirty_ = true;
 }
 
 void Batch::download(int32_t id, double* records, int64_t n, cudaStream_t s) {
@@ -305,8 +309,20 @@ void Batch::ensure_particle_buffers(int64_t total) {
   cap_p_ = cap;
 }
 
+// Work items: at most one partial chunk per particle block beyond total / chunk.
+void Batch::ensure_items() {
+  const int64_t need = cap_p_ / chunk_ + cap_blocks_ + 64;
+  if (need <= cap_items_) return;
+  dfree(items_);
+  items_ = dalloc<int2>((size_t)need);
+  cap_items_ = (int32_t)need;
+}
+
 void Batch::ensure_grid(int64_t blocks) {
-  if (blocks <= cap_blocks_) return;
+  if (blocks <= cap_blocks_) {
+    ensure_items();
+    return;
+  }
   free_grid();
   const int64_t cap = std::max<int64_t>(blocks, 256);
   cap_blocks_ = (int32_t)cap;
@@ -323,6 +339,7 @@ void Batch::ensure_grid(int64_t blocks) {
   vel_ = dalloc<unsigned char>((size_t)cap * 64 * kVelCh * rsize_);
   check_cuda(cudaMemset(acc_, 0, (size_t)cap * 64 * kAccCh * rsize_), "cudaMemset");
   check_cuda(cudaMemset(vel_, 0, (size_t)cap * 64 * kVelCh * rsize_), "cudaMemset");
+  ensure_items();
 }
 
 BatchDev Batch::dev(SceneDev* scenes, int num_scenes, int64_t total) const {
@@ -346,111 +363,76 @@ BatchDev Batch::dev(SceneDev* scenes, int num_scenes, int64_t total) const {
   b.blk_key = blk_key_;
   b.pblk_start = pblk_start_;
   b.pblk_end = pblk_end_;
+  b.items = items_;
+  b.cap_items = cap_items_;
+  b.chunk = chunk_;
   b.acc = acc_;
   b.vel = vel_;
   b.ctr = d_ctr_;
   return b;
 }
 
-// Uploads the scene table and colliders, measures the scenes' block boxes and
-// sizes the grid for them (twice the box volume, so the scenes can move).
-void Batch::rebuild(cudaStream_t s) {
-  drop_graph();
+// Brings the device scene table, colliders, sort buffers and grid in line
+// with the host's scenes after any change (scenes added or removed, particles
+// uploaded, parameters changed): uploads the host copy of the table, measures
+// every scene's block box from its particles, and grows the grid to twice the
+// box volume so that the scenes can move.  Captured graphs stay valid unless a
+// buffer moved (step() compares the launch arguments).
+void Batch::prepare(cudaStream_t s) {
+  if (!(dirty_ || boxes_dirty_ || params_dirty_)) return;
   total_ = 0;
-  std::vector<SceneDev> table;
-  std::vector<Collider> coll;
+  table_.clear();
+  coll_.clear();
   for (auto& sc : scenes_) {
     SceneDev d = scene_dev(*sc, total_);
-    d.coll_begin = (int32_t)coll.size();
+    d.coll_begin = (int32_t)coll_.size();
     d.coll_count = (int32_t)sc->colliders.size();
-    coll.insert(coll.end(), sc->colliders.begin(), sc->colliders.end());
-    table.push_back(d);
+    coll_.insert(coll_.end(), sc->colliders.begin(), sc->colliders.end());
+    table_.push_back(d);
     total_ += sc->n;
   }
-  if ((int)table.size() > d_scenes_cap_) {
+  if ((int)table_.size() > d_scenes_cap_) {
     dfree(d_scenes_);
-    d_scenes_cap_ = std::max<int>(16, (int)table.size() * 2);
+    d_scenes_cap_ = std::max<int>(16, (int)table_.size() * 2);
     d_scenes_ = dalloc<SceneDev>(d_scenes_cap_);
   }
-  if ((int)coll.size() > d_coll_cap_ || !d_coll_) {
+  if ((int)coll_.size() > d_coll_cap_ || !d_coll_) {
     dfree(d_coll_);
-    d_coll_cap_ = std::max<int>(16, (int)coll.size() * 2);
+    d_coll_cap_ = std::max<int>(16, (int)coll_.size() * 2);
     d_coll_ = dalloc<Collider>(d_coll_cap_);
   }
-  if (!table.empty())
-    check_cuda(cudaMemcpyAsync(d_scenes_, table.data(), table.size() * sizeof(SceneDev),
+  if (!table_.empty())
+    check_cuda(cudaMemcpyAsync(d_scenes_, table_.data(), table_.size() * sizeof(SceneDev),
                                cudaMemcpyHostToDevice, s),
                "scene table");
-  if (!coll.empty())
-    check_cuda(cudaMemcpyAsync(d_coll_, coll.data(), coll.size() * sizeof(Collider),
+  if (!coll_.empty())
+    check_cuda(cudaMemcpyAsync(d_coll_, coll_.data(), coll_.size() * sizeof(Collider),
                                cudaMemcpyHostToDevice, s),
                "colliders");
   ensure_particle_buffers(total_);
-  const BatchDev b = dev(d_scenes_, (int)table.size(), total_);
+  const BatchDev b = dev(d_scenes_, (int)table_.size(), total_);
   if (prec_ == SNOW_FP64)
     StepLaunch<double>::bbox_init(b, s);
   else
     StepLaunch<float>::bbox_init(b, s);
   check_cuda(cudaGetLastError(), "bbox");
-  // size the grid from the measured boxes
-  check_cuda(cudaMemcpyAsync(table.data(), d_scenes_, table.size() * sizeof(SceneDev),
-                             cudaMemcpyDeviceToHost, s),
-             "scene table readback");
+  std::vector<SceneDev> measured(table_.size());
+  if (!measured.empty())
+    check_cuda(cudaMemcpyAsync(measured.data(), d_scenes_, measured.size() * sizeof(SceneDev),
+                               cudaMemcpyDeviceToHost, s),
+               "scene table readback");
   check_cuda(cudaStreamSynchronize(s), "sync");
   int64_t vol = 0;
-  for (const SceneDev& d : table) {
+  for (const SceneDev& d : measured) {
     if (d.nb_lo[0] > d.nb_hi[0]) continue;
     int64_t v = 1;
     for (int a = 0; a < 3; ++a) v *= (int64_t)(d.nb_hi[a] - d.nb_lo[a] + 4);
     vol += v;
   }
-  ensure_grid(std::min<int64_t>(2 * vol + 1024, std::max<int64_t>(8 * total_ + 64, 1024)));
-  num_dev_scenes_ = (int)table.size();
-  dirty_ = false;
-  boxes_dirty_ = false;
-  params_dirty_ = false;
-}
-
-// Re-uploads parameters only (scene table entries keep their device-side state).
-void Batch::refresh_params(cudaStream_t s) {
-  std::vector<SceneDev> table(num_dev_scenes_);
-  check_cuda(cudaMemcpyAsync(table.data(), d_scenes_, table.size() * sizeof(SceneDev),
-                             cudaMemcpyDeviceToHost, s),
-             "scene table readback");
-  check_cuda(cudaStreamSynchronize(s), "sync");
-  std::vector<Collider> coll;
-  for (size_t k = 0; k < scenes_.size(); ++k) {
-    const Scene& sc = *scenes_[k];
-    SceneDev fresh = scene_dev(sc, table[k].begin);
-    SceneDev& d = table[k];
-    d.dx = fresh.dx;
-    d.dt = fresh.dt;
-    for (int a = 0; a < 3; ++a) d.g[a] = fresh.g[a];
-    d.mu0 = fresh.mu0;
-    d.lambda0 = fresh.lambda0;
-    d.xi = fresh.xi;
-    d.theta_c = fresh.theta_c;
-    d.theta_s = fresh.theta_s;
-    d.alpha = fresh.alpha;
-    d.coll_begin = (int32_t)coll.size();
-    d.coll_count = (int32_t)sc.colliders.size();
-    coll.insert(coll.end(), sc.colliders.begin(), sc.colliders.end());
-  }
-  if ((int)coll.size() > d_coll_cap_) {
-    // the collider array moves: captured graphs hold the old pointer
-    drop_graph();
-    dfree(d_coll_);
-    d_coll_cap_ = std::max<int>(16, (int)coll.size() * 2);
-    d_coll_ = dalloc<Collider>(d_coll_cap_);
-  }
-  check_cuda(cudaMemcpyAsync(d_scenes_, table.data(), table.size() * sizeof(SceneDev),
-                             cudaMemcpyHostToDevice, s),
-             "scene table");
-  if (!coll.empty())
-    check_cuda(cudaMemcpyAsync(d_coll_, coll.data(), coll.size() * sizeof(Collider),
-                               cudaMemcpyHostToDevice, s),
-               "colliders");
-  params_dirty_ = false;
+  const int64_t want = std::max<int64_t>(2 * vol + 1024, 2 * last_blocks_ + 1024);
+  ensure_grid(std::min<int64_t>(want, std::max<int64_t>(8 * total_ + 64, 1024)));
+  num_dev_scenes_ = (int)table_.size();
+  dirty_ = boxes_dirty_ = params_dirty_ = false;
 }
 
 template <typename R>
@@ -464,20 +446,13 @@ void Batch::launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev) {
   radix_sort(b, s);
   StepLaunch<R>::blocks(b, s);
   mark(1);
-  StepLaunch<R>::p2g(b, P2G_FULL, s);
+  StepLaunch<R>::p2g(b, P2G_PRE, s);
   mark(2);
   StepLaunch<R>::grid_update(b, s);
   mark(3);
   StepLaunch<R>::g2p(b, G2P_FULL, s);
   StepLaunch<R>::finish(b, s);
   mark(4);
-}
-
-void Batch::prepare(cudaStream_t s) {
-  if (dirty_ || boxes_dirty_)
-    rebuild(s);
-  else if (params_dirty_)
-    refresh_params(s);
 }
 
 void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
@@ -488,6 +463,16 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
   if (!s) s = own_stream_;
   prepare(s);
   const BatchDev b = dev(d_scenes_, num_dev_scenes_, total_);
+  if (force_dirty_) {
+    // P2G reads each particle's force matrix, which G2P keeps current from step
+    // to step; compute it afresh after an upload, setup() or parameter change.
+    if (prec_ == SNOW_FP64)
+      StepLaunch<double>::prepare_force(b, s);
+    else
+      StepLaunch<float>::prepare_force(b, s);
+    check_cuda(cudaGetLastError(), "prepare force");
+    force_dirty_ = false;
+  }
   auto one = [&](cudaEvent_t* ev) {
     if (prec_ == SNOW_FP64)
       launch_step<double>(b, s, ev);
@@ -510,6 +495,7 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
     for (auto& e : ev) cudaEventDestroy(e);
   } else if (use_graphs_) {
     int k = 0;
+    if (gexec_ && std::memcmp(&graph_args_, &b, sizeof b) != 0) drop_graph();  // a buffer moved
     if (!gexec_) {
       // first step eagerly (initialises per-kernel launch settings), then capture
       one(nullptr);
@@ -522,6 +508,7 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
         check_cuda(cudaStreamEndCapture(s, &g), "capture end");
         check_cuda(cudaGraphInstantiate(&gexec_, g, 0), "graph instantiate");
         cudaGraphDestroy(g);
+        graph_args_ = b;
       }
     }
     for (; k < n_steps; ++k) check_cuda(cudaGraphLaunch(gexec_, s), "graph launch");
@@ -536,7 +523,7 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
   last_blocks_ = (int64_t)h_ctr_->n_pblocks + h_ctr_->n_halo;
   check_status();
   // Keep 2x headroom: grow the grid before the next call if the last step came close.
-  if (last_blocks_ * 2 > cap_blocks_) dirty_ = true;
+  if (last_blocks_ * 2 > cap_blocks_) boxes_dirty_ = true;
 }
 
 void Batch::check_status() {
@@ -558,8 +545,6 @@ void Batch::setup(int32_t id, double dx, cudaStream_t s) {
   if (!(dx > 0.0)) throw Error(SNOW_E_ARG, "grid_spacing must be positive");
   Scene* sc = find(id);
   if (sc->n == 0) return;
-  if (dirty_ || boxes_dirty_) rebuild(s);
-  drop_graph();  // the one-scene view reuses the step buffers
   if (!d_tmp_scene_) d_tmp_scene_ = dalloc<SceneDev>(1);
   SceneDev d = scene_dev(*sc, 0);
   d.dx = dx;
@@ -597,8 +582,8 @@ void Batch::setup(int32_t id, double dx, cudaStream_t s) {
   check_cuda(cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, s), "status");
   check_cuda(cudaStreamSynchronize(s), "setup");
   last_status_ = h_ctr_->status;
+  force_dirty_ = true;  // V_p0 changed
   check_status();
-  boxes_dirty_ = true;  // the batch's own scene table must be re-measured
 }
 
 int64_t Batch::device_bytes() const {

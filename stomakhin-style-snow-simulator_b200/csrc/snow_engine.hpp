@@ -63,6 +63,13 @@ class Batch {
   uint32_t last_status() const { return last_status_; }
   int64_t last_blocks() const { return last_blocks_; }
   int64_t capacity_blocks() const { return cap_blocks_; }
+  // Particles per P2G/G2P work item (a power of two, 32..4096).
+  void set_chunk(int chunk) {
+    if (chunk < 32 || chunk > 4096 || (chunk & (chunk - 1))) throw Error(SNOW_E_ARG, "chunk must be a power of two in [32, 4096]");
+    chunk_ = chunk;
+    cap_items_ = 0;  // re-sized on the next prepare
+    boxes_dirty_ = true;
+  }
   void set_graphs(bool on) {
     use_graphs_ = on;
     drop_graph();
@@ -90,10 +97,9 @@ class Batch {
   void ensure_staging(int64_t n);
   void ensure_particle_buffers(int64_t total);
   void ensure_grid(int64_t blocks);
+  void ensure_items();
   void set_colliders(Scene& sc, const snow_collider* c, int n);
   SceneDev scene_dev(const Scene& sc, int64_t begin) const;
-  void rebuild(cudaStream_t s);
-  void refresh_params(cudaStream_t s);
   template <typename R>
   void launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev);
 
@@ -103,6 +109,7 @@ class Batch {
   int32_t next_id_ = 0;
   bool dirty_ = true, boxes_dirty_ = true, params_dirty_ = false;
   bool use_graphs_ = true;
+  bool force_dirty_ = true;  // particles' force matrices must be recomputed
   int64_t total_ = 0;
   int num_dev_scenes_ = 0;
 
@@ -131,11 +138,17 @@ class Batch {
   int32_t* pblk_end_ = nullptr;
   void* acc_ = nullptr;
   void* vel_ = nullptr;
+  int2* items_ = nullptr;
+  int32_t cap_items_ = 0;
+  int32_t chunk_ = 256;
 
   double* staging_ = nullptr;
   int64_t staging_cap_ = 0;
 
   cudaGraphExec_t gexec_ = nullptr;
+  BatchDev graph_args_{};
+  std::vector<SceneDev> table_;
+  std::vector<Collider> coll_;
   cudaStream_t own_stream_ = nullptr;
   uint32_t last_status_ = 0;
   int64_t last_blocks_ = 0;

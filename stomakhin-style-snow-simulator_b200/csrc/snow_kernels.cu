@@ -69,12 +69,21 @@ struct PlaneView {
 };
 
 // ------------------------------------------------------------------ bbox init
+// Atomic min/max into a scene's box, skipped when it cannot improve the value
+// already there (after the first few updates almost every one is skipped).
+__device__ __forceinline__ void box_update(SceneDev& sc, const int lo[3], const int hi[3]) {
+  for (int a = 0; a < 3; ++a) {
+    if (lo[a] < *(volatile int*)&sc.nb_lo[a]) atomicMin(&sc.nb_lo[a], lo[a]);
+    if (hi[a] > *(volatile int*)&sc.nb_hi[a]) atomicMax(&sc.nb_hi[a], hi[a]);
+  }
+}
+
 template <typename R>
-__global__ void k_bbox_init(const BatchDev b) {
+__global__ void __launch_bounds__(256) k_bbox_init(const BatchDev b) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = t < b.total;
-  int s = 0;
-  int c[3] = {INT_MAX, INT_MAX, INT_MAX};
+  int s = -1;
+  int lo[3] = {INT_MAX, INT_MAX, INT_MAX};
   int hi[3] = {INT_MIN, INT_MIN, INT_MIN};
   if (valid) {
     s = scene_of(b, t);
@@ -88,14 +97,20 @@ __global__ void k_bbox_init(const BatchDev b) {
         continue;
       }
       int cell;
-      c[a] = hi[a] = block_coord(x, (R)sc.dx, cell);
+      lo[a] = hi[a] = block_coord(x, (R)sc.dx, cell);
     }
   }
-  if (!valid) return;
-  SceneDev& sc = b.scenes[s];
-  for (int a = 0; a < 3; ++a) {
-    if (c[a] != INT_MAX) atomicMin(&sc.nb_lo[a], c[a]);
-    if (hi[a] != INT_MIN) atomicMax(&sc.nb_hi[a], hi[a]);
+  // One update per warp when its particles belong to one scene (the usual case).
+  const unsigned full = 0xffffffffu;
+  const int s0 = __shfl_sync(full, s, 0);
+  if (__all_sync(full, s == s0 || s < 0)) {
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = __reduce_min_sync(full, lo[a]);
+      hi[a] = __reduce_max_sync(full, hi[a]);
+    }
+    if ((threadIdx.x & 31) == 0 && s0 >= 0) box_update(b.scenes[s0], lo, hi);
+  } else if (valid) {
+    box_update(b.scenes[s], lo, hi);
   }
 }
 
@@ -164,6 +179,7 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
     c->n_pblocks = 0;
     c->n_halo = 0;
     c->work_p2g = c->work_grid = c->work_g2p = c->work_aux = 0;
+    c->n_items = 0;
   }
 }
 
@@ -263,6 +279,16 @@ __global__ void __launch_bounds__(256) k_blocks_b(const BatchDev b) {
         if (K[mid] <= lim) lo = mid + 1; else hi = mid;
       }
       b.pblk_end[pb] = (int32_t)lo;
+      const int n = (int)(lo - b.pblk_start[pb]);
+      const int cnt = (n + b.chunk - 1) / b.chunk;
+      const uint32_t base = atomicAdd(&b.ctr->n_items, (uint32_t)cnt);
+      for (int c = 0; c < cnt; ++c) {
+        if ((int64_t)base + c >= b.cap_items) {
+          flag(b, ST_BLOCK_OVERFLOW);
+          break;
+        }
+        b.items[base + c] = make_int2((int)pb, c);
+      }
       continue;
     }
     const SceneDev& sc = b.scenes[bc.w];
@@ -287,9 +313,6 @@ __global__ void __launch_bounds__(256) k_blocks_b(const BatchDev b) {
 __device__ __forceinline__ uint32_t num_blocks(const BatchDev& b) {
   return min(b.ctr->n_pblocks + b.ctr->n_halo, (uint32_t)b.cap_blocks);
 }
-__device__ __forceinline__ uint32_t num_pblocks(const BatchDev& b) {
-  return min(b.ctr->n_pblocks, (uint32_t)b.cap_blocks);
-}
 
 // Shared per-block header for the particle-block kernels.
 struct BlockHeader {
@@ -298,18 +321,20 @@ struct BlockHeader {
   int32_t nbr[8];
 };
 
-// Claims the next particle block for this CTA; returns false when none is left.
+// Claims the next work item for this CTA: a chunk of consecutive particles of
+// one particle block; returns false when none is left.
 template <bool kNeedNbr>
 __device__ __forceinline__ bool claim_block(const BatchDev& b, uint32_t* counter, BlockHeader& h) {
   __syncthreads();
   if (threadIdx.x == 0) h.blk = (int32_t)atomicAdd(counter, 1u);
   __syncthreads();
-  const uint32_t npb = num_pblocks(b);
-  if ((uint32_t)h.blk >= npb) return false;
+  const uint32_t items = min(b.ctr->n_items, (uint32_t)b.cap_items);
+  if ((uint32_t)h.blk >= items) return false;
   if (threadIdx.x == 0) {
-    const int4 bc = b.blk[h.blk];
-    h.start = b.pblk_start[h.blk];
-    h.end = b.pblk_end[h.blk];
+    const int2 it = b.items[h.blk];
+    const int4 bc = b.blk[it.x];
+    h.start = b.pblk_start[it.x] + it.y * b.chunk;
+    h.end = min(h.start + b.chunk, b.pblk_end[it.x]);
     h.scene = bc.w;
     h.bx = bc.x;
     h.by = bc.y;
@@ -373,8 +398,8 @@ constexpr size_t p2g_smem() {
 template <typename R, int MODE>
 __global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
   constexpr int NCH = P2GChannels<R, MODE>::n;
-  constexpr bool kMom = MODE == P2G_FULL || MODE == P2G_MASS_MOMENTUM;
-  constexpr bool kForce = MODE == P2G_FULL || MODE == P2G_FORCE;
+  constexpr bool kMom = MODE == P2G_FULL || MODE == P2G_PRE || MODE == P2G_MASS_MOMENTUM;
+  constexpr bool kForce = MODE == P2G_FULL || MODE == P2G_PRE || MODE == P2G_FORCE;
   constexpr bool kMass = MODE != P2G_FORCE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][kTileN]
@@ -421,7 +446,11 @@ __global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
           rr[R_MV + 1] = m * pv.at(PV + 1, i);
           rr[R_MV + 2] = m * pv.at(PV + 2, i);
         }
-        if constexpr (kForce) {
+        if constexpr (MODE == P2G_PRE) {
+          // force matrix left by the previous step's G2P (or prepare_force)
+#pragma unroll
+          for (int e = 0; e < 6; ++e) rr[R_F + e] = pv.at(PFM + e, i);
+        } else if constexpr (kForce) {
           M3<R> FE;
 #pragma unroll
           for (int e = 0; e < 9; ++e) FE.a[e] = pv.at(PFE + e, i);
@@ -573,9 +602,34 @@ struct G2PChannels {
   static constexpr int n = MODE == G2P_VOLUME ? 1 : (MODE == G2P_STRESS ? 3 : 6);
 };
 
+// Flushes a CTA's running block box of one scene (warp-reduced, then atomics
+// that are skipped when they cannot improve the stored box).
+__device__ __forceinline__ void flush_box(SceneDev& ps, int bmin[3], int bmax[3]) {
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = __reduce_min_sync(0xffffffffu, bmin[a]);
+    hi[a] = __reduce_max_sync(0xffffffffu, bmax[a]);
+    bmin[a] = INT_MAX;
+    bmax[a] = INT_MIN;
+  }
+  if ((threadIdx.x & 31) == 0) box_update(ps, lo, hi);
+}
+
+// Next step's force matrix from the projected F_E, the square root returned by
+// plastic_projection and the new F_P (hardening in double).
+template <typename R>
+__device__ __forceinline__ Sym3<R> next_force(const M3<R>& FE, const Plastic<R>& pl, const M3<double>& FP,
+                                              const SceneDev& sc, R V0) {
+  const double hard = exp(sc.xi * (1.0 - det3(FP)));
+  if (!pl.regular) return force_matrix<R>(FE, V0, (R)sc.mu0, (R)sc.lambda0, (R)hard);
+  return assemble_force<R>(gram_rows(FE), pl.root, det3(FE), V0, (R)sc.mu0, (R)sc.lambda0, (R)hard);
+}
+
 template <typename R, int MODE>
-__global__ void __launch_bounds__(256) k_g2p(const BatchDev b) {
+__global__ void __launch_bounds__(256, 2) k_g2p(const BatchDev b) {
   constexpr int NCH = G2PChannels<MODE>::n;
+  constexpr bool kGrad = MODE == G2P_FULL || MODE == G2P_STRESS;
+  constexpr bool kVel = MODE == G2P_FULL || MODE == G2P_VELOCITY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][kTileN]
   __shared__ BlockHeader h;
@@ -604,23 +658,7 @@ __global__ void __launch_bounds__(256) k_g2p(const BatchDev b) {
     __syncthreads();
     const int s = h.scene;
     if (MODE == G2P_FULL && s != last_scene) {
-      // flush the bounding box of the previous scene
-      if (last_scene >= 0) {
-        SceneDev& ps = b.scenes[last_scene];
-        for (int a = 0; a < 3; ++a) {
-          int lo = bmin[a], hi = bmax[a];
-          for (int o = 16; o; o >>= 1) {
-            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-          }
-          if ((threadIdx.x & 31) == 0) {
-            if (lo < *(volatile int*)&ps.nb_lo[a]) atomicMin(&ps.nb_lo[a], lo);
-            if (hi > *(volatile int*)&ps.nb_hi[a]) atomicMax(&ps.nb_hi[a], hi);
-          }
-          bmin[a] = INT_MAX;
-          bmax[a] = INT_MIN;
-        }
-      }
+      if (last_scene >= 0) flush_box(b.scenes[last_scene], bmin, bmax);
       last_scene = s;
     }
     const SceneDev& sc = b.scenes[s];
@@ -659,41 +697,65 @@ __global__ void __launch_bounds__(256) k_g2p(const BatchDev b) {
         rw[PVOL * sc.stride + i] = pv.at(PM, i) / density;
         continue;
       } else {
+        // grad v = sum_n v_n (grad w_n)^T, v_pic = sum_n w_n v_n, FLIP term = sum_n w_n dv_n
+        // (grid.cpp:250-276, 295-319), contracted one axis at a time: z, then y, then x.
         R gv[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};  // column-major
         R vpic[3] = {R(0), R(0), R(0)}, dflip[3] = {R(0), R(0), R(0)};
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
+          R SS[NCH], SD[3], TS[3];
+#pragma unroll
+          for (int ch = 0; ch < NCH; ++ch) SS[ch] = R(0);
+#pragma unroll
+          for (int ch = 0; ch < 3; ++ch) SD[ch] = TS[ch] = R(0);
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
-            const R A = wx.w[a] * wy.w[c];
-            const R Bx = wx.dw[a] * wy.w[c];
-            const R By = wx.w[a] * wy.dw[c];
+            R S[NCH], T[3];
+#pragma unroll
+            for (int ch = 0; ch < NCH; ++ch) S[ch] = R(0);
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) T[ch] = R(0);
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               const int t = tile_index(tx + a, ty + c, tz + e);
-              const R v0 = tile[t], v1 = tile[kTileN + t], v2 = tile[2 * kTileN + t];
-              if constexpr (MODE == G2P_FULL || MODE == G2P_STRESS) {
-                const R g0 = Bx * wz.w[e], g1 = By * wz.w[e], g2 = A * wz.dw[e];
-                gv[0] += v0 * g0; gv[1] += v1 * g0; gv[2] += v2 * g0;
-                gv[3] += v0 * g1; gv[4] += v1 * g1; gv[5] += v2 * g1;
-                gv[6] += v0 * g2; gv[7] += v1 * g2; gv[8] += v2 * g2;
+#pragma unroll
+              for (int ch = 0; ch < NCH; ++ch) {
+                const R f = tile[ch * kTileN + t];
+                S[ch] += wz.w[e] * f;
+                if (kGrad && ch < 3) T[ch] += wz.dw[e] * f;
               }
-              if constexpr (MODE == G2P_FULL || MODE == G2P_VELOCITY) {
-                const R w = A * wz.w[e];
-                vpic[0] += w * v0;
-                vpic[1] += w * v1;
-                vpic[2] += w * v2;
-                dflip[0] += w * tile[3 * kTileN + t];
-                dflip[1] += w * tile[4 * kTileN + t];
-                dflip[2] += w * tile[5 * kTileN + t];
+            }
+#pragma unroll
+            for (int ch = 0; ch < NCH; ++ch) SS[ch] += wy.w[c] * S[ch];
+            if constexpr (kGrad) {
+#pragma unroll
+              for (int ch = 0; ch < 3; ++ch) {
+                SD[ch] += wy.dw[c] * S[ch];
+                TS[ch] += wy.w[c] * T[ch];
               }
+            }
+          }
+          if constexpr (kVel) {
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+              vpic[ch] += wx.w[a] * SS[ch];
+              dflip[ch] += wx.w[a] * SS[3 + ch];
+            }
+          }
+          if constexpr (kGrad) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+              gv[r] += wx.dw[a] * SS[r];
+              gv[3 + r] += wx.w[a] * SD[r];
+              gv[6 + r] += wx.w[a] * TS[r];
             }
           }
         }
         const R dt = (R)sc.dt;
         M3<R> FEn;
         M3<double> FPn;
-        if constexpr (MODE == G2P_FULL || MODE == G2P_STRESS) {
+        Plastic<R> pl;
+        if constexpr (kGrad) {
           // stress_update (grid.cpp:277-285)
           M3<R> FE, L;
 #pragma unroll
@@ -705,23 +767,21 @@ __global__ void __launch_bounds__(256) k_g2p(const BatchDev b) {
           L.a[4] += R(1);
           L.a[8] += R(1);
           FEn = mat_mul(L, FE);
-          Sym3<R> Dinv;
-          bool clamped;
-          plastic_projection(FEn, R(1) - (R)sc.theta_c, R(1) + (R)sc.theta_s, Dinv, clamped);
+          pl = plastic_projection(FEn, R(1) - (R)sc.theta_c, R(1) + (R)sc.theta_s);
 #pragma unroll
           for (int e = 0; e < 9; ++e) FPn.a[e] = pv.fp[e * pv.st + i];
-          if (clamped) {
-            const double d[9] = {(double)Dinv.xx, (double)Dinv.xy, (double)Dinv.xz,
-                                 (double)Dinv.xy, (double)Dinv.yy, (double)Dinv.yz,
-                                 (double)Dinv.xz, (double)Dinv.yz, (double)Dinv.zz};
+          if (pl.clamped) {
+            const Sym3<R>& Di = pl.Dinv;
             M3<double> Dm;
+            const double d[9] = {(double)Di.xx, (double)Di.xy, (double)Di.xz, (double)Di.xy, (double)Di.yy,
+                                 (double)Di.yz, (double)Di.xz, (double)Di.yz, (double)Di.zz};
 #pragma unroll
             for (int e = 0; e < 9; ++e) Dm.a[e] = d[e];
             FPn = mat_mul(Dm, FPn);
           }
         }
         R vn[3];
-        if constexpr (MODE == G2P_FULL || MODE == G2P_VELOCITY) {
+        if constexpr (kVel) {
           // G2P (grid.cpp:321-324)
           const R alpha = (R)sc.alpha;
 #pragma unroll
@@ -753,6 +813,8 @@ __global__ void __launch_bounds__(256) k_g2p(const BatchDev b) {
           R xn[3];
 #pragma unroll
           for (int a = 0; a < 3; ++a) xn[a] = x[a] + dt * vn[a];
+          const R V0 = pv.at(PVOL, i);
+          const Sym3<R> Mn = next_force(FEn, pl, FPn, sc, V0);
           const int64_t o = j - sc.begin;  // block-sorted slot in the other buffer
           R* rw = (R*)sc.r[cur ^ 1];
           double* fw = sc.fp[cur ^ 1];
@@ -763,12 +825,18 @@ __global__ void __launch_bounds__(256) k_g2p(const BatchDev b) {
             rw[(PV + a) * st + o] = vn[a];
           }
           rw[PM * st + o] = pv.at(PM, i);
-          rw[PVOL * st + o] = pv.at(PVOL, i);
+          rw[PVOL * st + o] = V0;
 #pragma unroll
           for (int e = 0; e < 9; ++e) {
             rw[(PFE + e) * st + o] = FEn.a[e];
             fw[e * st + o] = FPn.a[e];
           }
+          rw[(PFM + 0) * st + o] = Mn.xx;
+          rw[(PFM + 1) * st + o] = Mn.yy;
+          rw[(PFM + 2) * st + o] = Mn.zz;
+          rw[(PFM + 3) * st + o] = Mn.xy;
+          rw[(PFM + 4) * st + o] = Mn.xz;
+          rw[(PFM + 5) * st + o] = Mn.yz;
           sc.id[cur ^ 1][o] = pv.id[i];
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
@@ -785,20 +853,34 @@ __global__ void __launch_bounds__(256) k_g2p(const BatchDev b) {
       }
     }
   }
-  if (MODE == G2P_FULL && last_scene >= 0) {
-    SceneDev& ps = b.scenes[last_scene];
-    for (int a = 0; a < 3; ++a) {
-      int lo = bmin[a], hi = bmax[a];
-      for (int o = 16; o; o >>= 1) {
-        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-      }
-      if ((threadIdx.x & 31) == 0) {
-        if (lo < *(volatile int*)&ps.nb_lo[a]) atomicMin(&ps.nb_lo[a], lo);
-        if (hi > *(volatile int*)&ps.nb_hi[a]) atomicMax(&ps.nb_hi[a], hi);
-      }
-    }
-  }
+  if (MODE == G2P_FULL && last_scene >= 0) flush_box(b.scenes[last_scene], bmin, bmax);
+}
+
+// Force matrix of every particle from its F_E, F_P and V_p0 (after an upload,
+// setup() or a parameter change; afterwards G2P keeps it current).
+template <typename R>
+__global__ void __launch_bounds__(256) k_prepare_force(const BatchDev b) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.total) return;
+  const SceneDev& sc = b.scenes[scene_of(b, t)];
+  const int64_t i = t - sc.begin;
+  R* r = (R*)sc.r[sc.cur];
+  const double* fp = sc.fp[sc.cur];
+  const int64_t st = sc.stride;
+  M3<R> FE;
+#pragma unroll
+  for (int e = 0; e < 9; ++e) FE.a[e] = r[(PFE + e) * st + i];
+  M3<double> FP;
+#pragma unroll
+  for (int e = 0; e < 9; ++e) FP.a[e] = fp[e * st + i];
+  const double hard = exp(sc.xi * (1.0 - det3(FP)));
+  const Sym3<R> M = force_matrix<R>(FE, r[PVOL * st + i], (R)sc.mu0, (R)sc.lambda0, (R)hard);
+  r[(PFM + 0) * st + i] = M.xx;
+  r[(PFM + 1) * st + i] = M.yy;
+  r[(PFM + 2) * st + i] = M.zz;
+  r[(PFM + 3) * st + i] = M.xy;
+  r[(PFM + 4) * st + i] = M.xz;
+  r[(PFM + 5) * st + i] = M.yz;
 }
 
 __global__ void k_finish(const BatchDev b) {
@@ -872,6 +954,7 @@ void StepLaunch<R>::p2g(const BatchDev& b, int mode, cudaStream_t s) {
     case P2G_MASS: launch_p2g<R, P2G_MASS>(b, s); break;
     case P2G_MASS_MOMENTUM: launch_p2g<R, P2G_MASS_MOMENTUM>(b, s); break;
     case P2G_FORCE: launch_p2g<R, P2G_FORCE>(b, s); break;
+    case P2G_PRE: launch_p2g<R, P2G_PRE>(b, s); break;
   }
 }
 template <typename R>
@@ -905,6 +988,11 @@ void StepLaunch<R>::g2p(const BatchDev& b, int mode, cudaStream_t s) {
     case G2P_STRESS: launch_g2p<R, G2P_STRESS>(b, s); break;
     case G2P_VELOCITY: launch_g2p<R, G2P_VELOCITY>(b, s); break;
   }
+}
+template <typename R>
+void StepLaunch<R>::prepare_force(const BatchDev& b, cudaStream_t s) {
+  if (b.total <= 0) return;
+  k_prepare_force<R><<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
 }
 template <typename R>
 void StepLaunch<R>::finish(const BatchDev& b, cudaStream_t s) {

@@ -170,21 +170,9 @@ SNOW_HD Sym3<T> spectral(const T q[9], const T f[3]) {
 }
 
 // --------------------------------------------------------- constitutive model
-// Force matrix of one particle, M = -V_p0 * P(F_E) * F_E^T (grid.cpp:174-176)
-// with the fixed-corotated stress P = 2 mu (F_E - R_E) + lambda (J-1) J F_E^-T
-// and exponential hardening mu = mu0 h, lambda = lambda0 h, h = exp(xi (1 - det F_P))
-// (grid.cpp:162-172).
-//
-// GPU form: P F^T = 2 mu (F F^T - R F^T) + lambda (J-1) J I, and R F^T = U S U^T
-// = sqrt(F F^T) for every SVD F = U S V^T with S >= 0 (R = U V^T, the reference's
-// polar factor from JacobiSVD).  So M needs only the symmetric square root of
-// B = F F^T (one 3x3 symmetric Jacobi eigensolve) and no inverse; M is symmetric.
-// `hardening` is exp(xi (1 - det F_P)) evaluated by the caller in double.
+// F F^T and F^T F.
 template <typename T>
-SNOW_HD Sym3<T> force_matrix(const M3<T>& F, T V0, T mu0, T lambda0, T hardening) {
-  const T mu = mu0 * hardening;
-  const T lambda = lambda0 * hardening;
-  const T J = det3(F);
+SNOW_HD Sym3<T> gram_rows(const M3<T>& F) {
   Sym3<T> B;
   B.xx = F(0, 0) * F(0, 0) + F(0, 1) * F(0, 1) + F(0, 2) * F(0, 2);
   B.yy = F(1, 0) * F(1, 0) + F(1, 1) * F(1, 1) + F(1, 2) * F(1, 2);
@@ -192,12 +180,54 @@ SNOW_HD Sym3<T> force_matrix(const M3<T>& F, T V0, T mu0, T lambda0, T hardening
   B.xy = F(0, 0) * F(1, 0) + F(0, 1) * F(1, 1) + F(0, 2) * F(1, 2);
   B.xz = F(0, 0) * F(2, 0) + F(0, 1) * F(2, 1) + F(0, 2) * F(2, 2);
   B.yz = F(1, 0) * F(2, 0) + F(1, 1) * F(2, 1) + F(1, 2) * F(2, 2);
-  T lam[3], q[9];
-  sym_eig3(B, lam, q, EigTol<T>::tol, EigTol<T>::sweeps);
-  T sv[3];
+  return B;
+}
+template <typename T>
+SNOW_HD Sym3<T> gram_cols(const M3<T>& F) {
+  Sym3<T> C;
+  C.xx = F(0, 0) * F(0, 0) + F(1, 0) * F(1, 0) + F(2, 0) * F(2, 0);
+  C.yy = F(0, 1) * F(0, 1) + F(1, 1) * F(1, 1) + F(2, 1) * F(2, 1);
+  C.zz = F(0, 2) * F(0, 2) + F(1, 2) * F(1, 2) + F(2, 2) * F(2, 2);
+  C.xy = F(0, 0) * F(0, 1) + F(1, 0) * F(1, 1) + F(2, 0) * F(2, 1);
+  C.xz = F(0, 0) * F(0, 2) + F(1, 0) * F(1, 2) + F(2, 0) * F(2, 2);
+  C.yz = F(0, 1) * F(0, 2) + F(1, 1) * F(1, 2) + F(2, 1) * F(2, 2);
+  return C;
+}
+// G S G^T for symmetric S.
+template <typename T>
+SNOW_HD Sym3<T> sandwich(const M3<T>& G, const Sym3<T>& S) {
+  T H[9];  // H = G S, column-major
 #pragma unroll
-  for (int i = 0; i < 3; ++i) sv[i] = sqrt(lam[i] > T(0) ? lam[i] : T(0));
-  const Sym3<T> R = spectral(q, sv);  // R F^T = sqrt(F F^T)
+  for (int r = 0; r < 3; ++r) {
+    H[r] = G(r, 0) * S.xx + G(r, 1) * S.xy + G(r, 2) * S.xz;
+    H[3 + r] = G(r, 0) * S.xy + G(r, 1) * S.yy + G(r, 2) * S.yz;
+    H[6 + r] = G(r, 0) * S.xz + G(r, 1) * S.yz + G(r, 2) * S.zz;
+  }
+  Sym3<T> o;  // (H G^T)(r,c) = sum_k H(r,k) G(c,k)
+  o.xx = H[0] * G(0, 0) + H[3] * G(0, 1) + H[6] * G(0, 2);
+  o.yy = H[1] * G(1, 0) + H[4] * G(1, 1) + H[7] * G(1, 2);
+  o.zz = H[2] * G(2, 0) + H[5] * G(2, 1) + H[8] * G(2, 2);
+  o.xy = H[0] * G(1, 0) + H[3] * G(1, 1) + H[6] * G(1, 2);
+  o.xz = H[0] * G(2, 0) + H[3] * G(2, 1) + H[6] * G(2, 2);
+  o.yz = H[1] * G(2, 0) + H[4] * G(2, 1) + H[7] * G(2, 2);
+  return o;
+}
+
+// Force matrix of one particle, M = -V_p0 * P(F_E) * F_E^T (grid.cpp:174-176)
+// with the fixed-corotated stress P = 2 mu (F_E - R_E) + lambda (J-1) J F_E^-T
+// and exponential hardening mu = mu0 h, lambda = lambda0 h, h = exp(xi (1 - det F_P))
+// (grid.cpp:162-172).
+//
+// GPU form: P F^T = 2 mu (F F^T - R F^T) + lambda (J-1) J I, and R F^T = U S U^T
+// = sqrt(F F^T) for every SVD F = U S V^T with S >= 0 (R = U V^T, the reference's
+// polar factor from JacobiSVD).  So M needs B = F F^T, its symmetric square root
+// and J; no inverse; M is symmetric.  `hardening` is exp(xi (1 - det F_P))
+// evaluated by the caller in double.
+template <typename T>
+SNOW_HD Sym3<T> assemble_force(const Sym3<T>& B, const Sym3<T>& R, T J, T V0, T mu0, T lambda0,
+                               T hardening) {
+  const T mu = mu0 * hardening;
+  const T lambda = lambda0 * hardening;
   const T two_mu = T(2) * mu;
   const T vol = lambda * (J - T(1)) * J;
   Sym3<T> M;
@@ -210,6 +240,18 @@ SNOW_HD Sym3<T> force_matrix(const M3<T>& F, T V0, T mu0, T lambda0, T hardening
   return M;
 }
 
+// The same from F alone: sqrt(F F^T) by one symmetric Jacobi eigensolve.
+template <typename T>
+SNOW_HD Sym3<T> force_matrix(const M3<T>& F, T V0, T mu0, T lambda0, T hardening) {
+  const Sym3<T> B = gram_rows(F);
+  T lam[3], q[9];
+  sym_eig3(B, lam, q, EigTol<T>::tol, EigTol<T>::sweeps);
+  T sv[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) sv[i] = sqrt(lam[i] > T(0) ? lam[i] : T(0));
+  return assemble_force(B, spectral(q, sv), det3(F), V0, mu0, lambda0, hardening);
+}
+
 // Elastoplastic update (grid.cpp:277-285): trial F_E* = (I + dt grad v) F_E,
 // SVD F_E* = U S V^T, S clamped to [1 - theta_c, 1 + theta_s],
 // F_E <- U S_c V^T,  F_P <- F_E^-1 F_E* F_P.
@@ -218,44 +260,53 @@ SNOW_HD Sym3<T> force_matrix(const M3<T>& F, T V0, T mu0, T lambda0, T hardening
 // D = V diag(s_c / s) V^T,  U S_c V^T = F_E* D  and  F_E^-1 F_E* = V diag(s / s_c) V^T
 // = D^-1, so F_E <- F_E* D and F_P <- D^-1 F_P: no U, no inverse.  Where no
 // singular value is clamped D = I and F_E* passes through unchanged.
-// Returns the trial F_E* in `FE` replaced by the projected F_E, and
-// D^-1 (symmetric) in `Dinv` for the caller to apply to F_P.
+//
+// The same eigenvectors give the square root the next step's force needs:
+// sqrt(F_E F_E^T) = U S_c U^T = F_E* V diag(s_c / s^2) V^T F_E*^T (returned in
+// `root`; `regular` is false when a singular value is too small for it).
 template <typename T>
-SNOW_HD void plastic_projection(M3<T>& FE, T lo, T hi, Sym3<T>& Dinv, bool& clamped) {
-  Sym3<T> C;
-  C.xx = FE(0, 0) * FE(0, 0) + FE(1, 0) * FE(1, 0) + FE(2, 0) * FE(2, 0);
-  C.yy = FE(0, 1) * FE(0, 1) + FE(1, 1) * FE(1, 1) + FE(2, 1) * FE(2, 1);
-  C.zz = FE(0, 2) * FE(0, 2) + FE(1, 2) * FE(1, 2) + FE(2, 2) * FE(2, 2);
-  C.xy = FE(0, 0) * FE(0, 1) + FE(1, 0) * FE(1, 1) + FE(2, 0) * FE(2, 1);
-  C.xz = FE(0, 0) * FE(0, 2) + FE(1, 0) * FE(1, 2) + FE(2, 0) * FE(2, 2);
-  C.yz = FE(0, 1) * FE(0, 2) + FE(1, 1) * FE(1, 2) + FE(2, 1) * FE(2, 2);
+struct Plastic {
+  Sym3<T> Dinv;
+  Sym3<T> root;
+  bool clamped;
+  bool regular;
+};
+
+template <typename T>
+SNOW_HD Plastic<T> plastic_projection(M3<T>& FE, T lo, T hi) {
+  Plastic<T> out;
   T lam[3], q[9];
-  sym_eig3(C, lam, q, EigTol<T>::tol, EigTol<T>::sweeps);
-  T r[3], ri[3];
-  clamped = false;
+  sym_eig3(gram_cols(FE), lam, q, EigTol<T>::tol, EigTol<T>::sweeps);
+  T r[3], ri[3], e[3];
+  out.clamped = false;
+  out.regular = true;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const T s = sqrt(lam[i] > T(0) ? lam[i] : T(0));
     const T sc = s < lo ? lo : (s > hi ? hi : s);  // std::clamp (grid.cpp:281-283)
-    if (sc != s) clamped = true;
+    if (sc != s) out.clamped = true;
+    if (!(s > T(1e-6))) out.regular = false;
     r[i] = s > T(0) ? sc / s : T(1);
     ri[i] = s > T(0) ? s / sc : T(1);
+    e[i] = s > T(0) ? sc / (s * s) : T(0);
   }
-  if (!clamped) {
-    Dinv = Sym3<T>{T(1), T(1), T(1), T(0), T(0), T(0)};
-    return;
+  out.root = sandwich(FE, spectral(q, e));
+  if (!out.clamped) {
+    out.Dinv = Sym3<T>{T(1), T(1), T(1), T(0), T(0), T(0)};
+    return out;
   }
   const Sym3<T> D = spectral(q, r);
-  Dinv = spectral(q, ri);
-  M3<T> out;
+  out.Dinv = spectral(q, ri);
+  M3<T> o;
 #pragma unroll
   for (int rr = 0; rr < 3; ++rr) {
     const T f0 = FE(rr, 0), f1 = FE(rr, 1), f2 = FE(rr, 2);
-    out(rr, 0) = f0 * D.xx + f1 * D.xy + f2 * D.xz;
-    out(rr, 1) = f0 * D.xy + f1 * D.yy + f2 * D.yz;
-    out(rr, 2) = f0 * D.xz + f1 * D.yz + f2 * D.zz;
+    o(rr, 0) = f0 * D.xx + f1 * D.xy + f2 * D.xz;
+    o(rr, 1) = f0 * D.xy + f1 * D.yy + f2 * D.yz;
+    o(rr, 2) = f0 * D.xz + f1 * D.yz + f2 * D.zz;
   }
-  FE = out;
+  FE = o;
+  return out;
 }
 
 // grid_velocity (grid.cpp:195-204): for a node with mass > 0,

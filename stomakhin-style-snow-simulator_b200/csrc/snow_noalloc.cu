@@ -14,7 +14,7 @@
 // Limits: at most kMaxParticles particles, kMaxBlocks grid blocks and
 // kMaxColliders colliders per call; larger inputs are rejected with
 // SNOW_E_ARG, and a step that needs more grid blocks fails with
-// SNOW_E_CAPACITY.  The array (about 24 MB) is held on every GPU that loads
+// SNOW_E_CAPACITY.  The array (about 26 MB) is held on every GPU that loads
 // the library until the process exits.
 //
 // The array's address is looked up with cudaGetSymbolAddress the first time
@@ -46,16 +46,18 @@ constexpr int32_t kMaxBlocks = 2048;
 constexpr int kMaxColliders = 16;
 constexpr uint32_t kHashSlots = 4096;  // power of two, twice kMaxBlocks
 constexpr int kTiles = (int)((kMaxParticles + 2047) / 2048);
+constexpr int kChunk = 256;
+constexpr int kItems = (int)(kMaxParticles / kChunk) + kMaxBlocks + 64;
 
 constexpr size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 
 // Byte offsets of every region inside the arena.
 struct Layout {
   size_t staging, r0, r1, fp0, fp1, id0, id1, k0, k1, v0, v1, hist, dtot, hkeys, hvals, blk,
-      blk_key, pstart, pend, acc, vel, ctr, scene, coll, total;
+      blk_key, pstart, pend, items, acc, vel, ctr, scene, coll, total;
   constexpr Layout()
       : staging(0), r0(0), r1(0), fp0(0), fp1(0), id0(0), id1(0), k0(0), k1(0), v0(0), v1(0),
-        hist(0), dtot(0), hkeys(0), hvals(0), blk(0), blk_key(0), pstart(0), pend(0), acc(0),
+        hist(0), dtot(0), hkeys(0), hvals(0), blk(0), blk_key(0), pstart(0), pend(0), items(0), acc(0),
         vel(0), ctr(0), scene(0), coll(0), total(0) {
     size_t o = 0;
     auto take = [&o](size_t bytes) {
@@ -83,6 +85,7 @@ struct Layout {
     blk_key = take((size_t)kMaxBlocks * sizeof(uint32_t));
     pstart = take((size_t)kMaxBlocks * sizeof(int32_t));
     pend = take((size_t)kMaxBlocks * sizeof(int32_t));
+    items = take((size_t)kItems * sizeof(int2));
     acc = take((size_t)kMaxBlocks * 64 * kAccCh * sizeof(double));
     vel = take((size_t)kMaxBlocks * 64 * kVelCh * sizeof(double));
     ctr = take(sizeof(Counters));
@@ -235,6 +238,9 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
     b.blk_key = reinterpret_cast<uint32_t*>(A + L.blk_key);
     b.pblk_start = reinterpret_cast<int32_t*>(A + L.pstart);
     b.pblk_end = reinterpret_cast<int32_t*>(A + L.pend);
+    b.items = reinterpret_cast<int2*>(A + L.items);
+    b.cap_items = kItems;
+    b.chunk = kChunk;
     b.acc = A + L.acc;
     b.vel = A + L.vel;
     b.ctr = ctr;
