@@ -31,6 +31,14 @@
 
 namespace snow {
 
+// One P2G/G2P work item: a run of particles [start, end) of the block
+// (bx, by, bz) of `scene`, and the ids of the block's +{0,1}^3 neighbours.
+struct BlockHeader {
+  int32_t start, end, scene, bx, by, bz, pad0, pad1;
+  int32_t nbr[8];
+};
+static_assert(sizeof(BlockHeader) == 64, "item header is 16 words");
+
 constexpr int kRealPlanes = 23;
 constexpr int kFPPlanes = 9;
 // PFM: the force matrix -V_p0 P F_E^T of the particle's current state (symmetric:
@@ -102,6 +110,7 @@ struct BatchDev {
   // work items of P2G/G2P: (particle block, chunk), chunk = `chunk` consecutive
   // particles of the block's sorted run, so that large blocks spread over CTAs
   int2* items;
+  BlockHeader* item_hdr;  // resolved header per item (k_items)
   int32_t cap_items;
   int32_t chunk;
   // grid

@@ -133,6 +133,7 @@ void Batch::free_grid() {
   dfree(acc_);
   dfree(vel_);
   dfree(items_);
+  dfree(item_hdr_);
   cap_items_ = 0;
   cap_blocks_ = 0;
   hcap_ = 0;
@@ -314,7 +315,9 @@ void Batch::ensure_items() {
   const int64_t need = cap_p_ / chunk_ + cap_blocks_ + 64;
   if (need <= cap_items_) return;
   dfree(items_);
+  dfree(item_hdr_);
   items_ = dalloc<int2>((size_t)need);
+  item_hdr_ = dalloc<BlockHeader>((size_t)need);
   cap_items_ = (int32_t)need;
 }
 
@@ -364,6 +367,7 @@ BatchDev Batch::dev(SceneDev* scenes, int num_scenes, int64_t total) const {
   b.pblk_start = pblk_start_;
   b.pblk_end = pblk_end_;
   b.items = items_;
+  b.item_hdr = item_hdr_;
   b.cap_items = cap_items_;
   b.chunk = chunk_;
   b.acc = acc_;

@@ -139,6 +139,7 @@ class Batch {
   void* acc_ = nullptr;
   void* vel_ = nullptr;
   int2* items_ = nullptr;
+  BlockHeader* item_hdr_ = nullptr;
   int32_t cap_items_ = 0;
   int32_t chunk_ = 256;
 

@@ -315,43 +315,57 @@ __device__ __forceinline__ uint32_t num_blocks(const BatchDev& b) {
 }
 
 // Shared per-block header for the particle-block kernels.
-struct BlockHeader {
-  int32_t blk, start, end, scene;
-  int32_t bx, by, bz;
-  int32_t nbr[8];
-};
-
-// Claims the next work item for this CTA: a chunk of consecutive particles of
-// one particle block; returns false when none is left.
-template <bool kNeedNbr>
-__device__ __forceinline__ bool claim_block(const BatchDev& b, uint32_t* counter, BlockHeader& h) {
-  __syncthreads();
-  if (threadIdx.x == 0) h.blk = (int32_t)atomicAdd(counter, 1u);
-  __syncthreads();
+// Item headers: everything a P2G/G2P CTA needs for one work item, resolved in
+// parallel over all items once the block table is complete (the 8 neighbour
+// ids come from the hash table).
+__global__ void __launch_bounds__(256) k_items(const BatchDev b) {
   const uint32_t items = min(b.ctr->n_items, (uint32_t)b.cap_items);
-  if ((uint32_t)h.blk >= items) return false;
-  if (threadIdx.x == 0) {
-    const int2 it = b.items[h.blk];
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)items * 8;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int item = (int)(e >> 3), d = (int)(e & 7);
+    const int2 it = b.items[item];
     const int4 bc = b.blk[it.x];
-    h.start = b.pblk_start[it.x] + it.y * b.chunk;
-    h.end = min(h.start + b.chunk, b.pblk_end[it.x]);
-    h.scene = bc.w;
-    h.bx = bc.x;
-    h.by = bc.y;
-    h.bz = bc.z;
-  }
-  __syncthreads();
-  if (kNeedNbr && threadIdx.x < 8) {
-    const int d = threadIdx.x;
-    const SceneDev& sc = b.scenes[h.scene];
-    const uint32_t nk = block_key(sc, h.bx + (d & 1), h.by + ((d >> 1) & 1), h.bz + (d >> 2));
-    const int32_t id = hash_find(b, nk);
+    BlockHeader* hd = b.item_hdr + item;
+    if (d == 0) {
+      const int start = b.pblk_start[it.x] + it.y * b.chunk;
+      hd->start = start;
+      hd->end = min(start + b.chunk, b.pblk_end[it.x]);
+      hd->scene = bc.w;
+      hd->bx = bc.x;
+      hd->by = bc.y;
+      hd->bz = bc.z;
+    }
+    const SceneDev& sc = b.scenes[bc.w];
+    const int32_t id = hash_find(b, block_key(sc, bc.x + (d & 1), bc.y + ((d >> 1) & 1), bc.z + (d >> 2)));
     if (id < 0) flag(b, ST_LOOKUP_MISS);
-    h.nbr[d] = id;
+    hd->nbr[d] = id;
   }
-  __syncthreads();
-  return true;
 }
+
+// Work-item queue of a persistent CTA.  Warp 0 claims the next item and loads
+// its header into registers while the CTA works on the current one, so the
+// claim costs one barrier and no dependent global loads.
+struct ItemQueue {
+  int next;   // item claimed ahead (warp 0)
+  int word;   // header word `lane` of that item (lanes 0..15 of warp 0)
+  __device__ void fetch(const BatchDev& b, uint32_t* counter, uint32_t items) {
+    if (threadIdx.x >= 32) return;
+    int n = 0;
+    if (threadIdx.x == 0) n = (int)atomicAdd(counter, 1u);
+    next = __shfl_sync(0xffffffffu, n, 0);
+    if (threadIdx.x < 16 && (uint32_t)next < items) word = reinterpret_cast<const int*>(b.item_hdr + next)[threadIdx.x];
+  }
+  __device__ bool claim(const BatchDev& b, uint32_t* counter, BlockHeader& h, int& s_next) {
+    const uint32_t items = min(b.ctr->n_items, (uint32_t)b.cap_items);
+    __syncthreads();  // everyone is done with the previous item's header and tile
+    if (threadIdx.x < 16) reinterpret_cast<int*>(&h)[threadIdx.x] = word;
+    if (threadIdx.x == 0) s_next = next;
+    __syncthreads();
+    if ((uint32_t)s_next >= items) return false;
+    fetch(b, counter, items);
+    return true;
+  }
+};
 
 // Tile position of local node `node` (0..63) of neighbour d; false if outside
 // the 7x7x7 region a particle block's stencils can reach.
@@ -414,7 +428,10 @@ __global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
   const int qi = lane >> 4, qj = (lane >> 2) & 3, qk = lane & 3;
   const int off0 = tile_index(qi, qj, qk), off1 = tile_index(qi + 2, qj, qk);
 
-  while (claim_block<true>(b, &b.ctr->work_p2g, h)) {
+  __shared__ int s_item;
+  ItemQueue q;
+  q.fetch(b, &b.ctr->work_p2g, min(b.ctr->n_items, (uint32_t)b.cap_items));
+  while (q.claim(b, &b.ctr->work_p2g, h, s_item)) {
     for (int e = threadIdx.x; e < NCH * kTileN; e += blockDim.x) tile[e] = R(0);
     __syncthreads();
     const SceneDev& sc = b.scenes[h.scene];
@@ -639,7 +656,10 @@ __global__ void __launch_bounds__(256, 2) k_g2p(const BatchDev b) {
   int bmin[3] = {INT_MAX, INT_MAX, INT_MAX}, bmax[3] = {INT_MIN, INT_MIN, INT_MIN};
   int last_scene = -1;
 
-  while (claim_block<true>(b, &b.ctr->work_g2p, h)) {
+  __shared__ int s_item;
+  ItemQueue q;
+  q.fetch(b, &b.ctr->work_g2p, min(b.ctr->n_items, (uint32_t)b.cap_items));
+  while (q.claim(b, &b.ctr->work_g2p, h, s_item)) {
     // Stage the 7x7x7 nodes this block's stencils read.
     for (int e = threadIdx.x; e < 8 * 64; e += blockDim.x) {
       const int d = e >> 6, node = e & 63;
@@ -934,6 +954,7 @@ void StepLaunch<R>::blocks(const BatchDev& b, cudaStream_t s) {
   cudaMemsetAsync(b.hkeys, 0xFF, sizeof(uint32_t) * ((size_t)b.hmask + 1), s);
   k_blocks_a<<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
   k_blocks_b<<<2 * sm_count(), 256, 0, s>>>(b);
+  k_items<<<2 * sm_count(), 256, 0, s>>>(b);
 }
 
 template <typename R, int MODE>

@@ -50,16 +50,20 @@ struct AxisWeights {
   T dw[4];
   int base;
 };
+// The grid position x / dx is a true division, as in the reference, so the
+// stencil base is the reference's exactly; the slopes are scaled by 1 / dx
+// (one rounding away from the reference's N_dash / dx).
 template <typename T>
 SNOW_HD AxisWeights<T> axis_weights(T x, T dx) {
   AxisWeights<T> a;
   const T gp = x / dx;
+  const T inv_dx = T(1) / dx;
   a.base = stencil_base(gp);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const T node = static_cast<T>(a.base + i);
     a.w[i] = bspline(node, gp);
-    a.dw[i] = bspline_slope(node, gp) / dx;
+    a.dw[i] = bspline_slope(node, gp) * inv_dx;
   }
   return a;
 }
@@ -101,16 +105,17 @@ struct Sym3 {
 // rotations (Golub & Van Loan, Matrix Computations, 4th ed., Alg. 8.5.2 with
 // the stable rotation of Alg. 8.5.1).  Converges quadratically; the sweep loop
 // stops when the off-diagonal mass falls below tol^2 of the diagonal mass.
+// The rotation's tangent t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)) with
+// theta = (a_qq - a_pp) / (2 a_pq) is evaluated as
+// t = sgn(a) b / (|a| + sqrt(a^2 + b^2)), a = a_qq - a_pp, b = 2 a_pq
+// (numerator and denominator multiplied by |b|): one division, one square
+// root, and cos = rsqrt(1 + t^2).
 template <typename T>
 SNOW_HD void rotate_pq(T& app, T& aqq, T& apq, T& arp, T& arq, T q[9], int p, int qq) {
   if (apq == T(0)) return;
-  const T theta = (aqq - app) / (T(2) * apq);
-  T t;
-  if (fabs(theta) > T(1e18))
-    t = T(0.5) / theta;
-  else
-    t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
-  const T c = T(1) / sqrt(t * t + T(1));
+  const T a = aqq - app, b = T(2) * apq;
+  const T t = (a >= T(0) ? b : -b) / (fabs(a) + sqrt(a * a + b * b));
+  const T c = rsqrt(t * t + T(1));
   const T s = t * c;
   app -= t * apq;
   aqq += t * apq;

@@ -54,10 +54,10 @@ constexpr size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 // Byte offsets of every region inside the arena.
 struct Layout {
   size_t staging, r0, r1, fp0, fp1, id0, id1, k0, k1, v0, v1, hist, dtot, hkeys, hvals, blk,
-      blk_key, pstart, pend, items, acc, vel, ctr, scene, coll, total;
+      blk_key, pstart, pend, items, item_hdr, acc, vel, ctr, scene, coll, total;
   constexpr Layout()
       : staging(0), r0(0), r1(0), fp0(0), fp1(0), id0(0), id1(0), k0(0), k1(0), v0(0), v1(0),
-        hist(0), dtot(0), hkeys(0), hvals(0), blk(0), blk_key(0), pstart(0), pend(0), items(0), acc(0),
+        hist(0), dtot(0), hkeys(0), hvals(0), blk(0), blk_key(0), pstart(0), pend(0), items(0), item_hdr(0), acc(0),
         vel(0), ctr(0), scene(0), coll(0), total(0) {
     size_t o = 0;
     auto take = [&o](size_t bytes) {
@@ -86,6 +86,7 @@ struct Layout {
     pstart = take((size_t)kMaxBlocks * sizeof(int32_t));
     pend = take((size_t)kMaxBlocks * sizeof(int32_t));
     items = take((size_t)kItems * sizeof(int2));
+    item_hdr = take((size_t)kItems * sizeof(BlockHeader));
     acc = take((size_t)kMaxBlocks * 64 * kAccCh * sizeof(double));
     vel = take((size_t)kMaxBlocks * 64 * kVelCh * sizeof(double));
     ctr = take(sizeof(Counters));
@@ -239,6 +240,7 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
     b.pblk_start = reinterpret_cast<int32_t*>(A + L.pstart);
     b.pblk_end = reinterpret_cast<int32_t*>(A + L.pend);
     b.items = reinterpret_cast<int2*>(A + L.items);
+    b.item_hdr = reinterpret_cast<BlockHeader*>(A + L.item_hdr);
     b.cap_items = kItems;
     b.chunk = kChunk;
     b.acc = A + L.acc;
