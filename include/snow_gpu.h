@@ -145,6 +145,12 @@ int snow_gpu_batch_status(snow_gpu_batch* batch, uint32_t* status, int64_t* bloc
                           int64_t* blocks_capacity);
 /* Use (1) or bypass (0) CUDA-graph replay for timing-free steps. */
 int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable);
+/* Mixed form: particles whose plastic projection was redone in double in the
+ * last step (a singular value within 1e-5 of a clamp bound or of another
+ * singular value).  0 for an FP64 batch. */
+int64_t snow_gpu_batch_fp64_projections(snow_gpu_batch* batch);
+/* Particles per P2G/G2P work item (power of two in [32, 4096]; default 256). */
+int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk);
 
 /* ---- one scene: setup() / step() of the reference ------------------------ */
 /* setup() on host records: records[i].V_p0 is overwritten. */

@@ -85,6 +85,7 @@ struct Counters {
   uint32_t work_p2g, work_grid, work_g2p, work_aux;
   uint32_t status;
   uint32_t n_items;     // (block, chunk) work items of the particle kernels
+  uint32_t fp64_projections;  // mixed form: plastic projections redone in double
 };
 
 struct BatchDev {

@@ -743,6 +743,15 @@ int snow_gpu_batch_status(snow_gpu_batch* batch, uint32_t* status, int64_t* used
     if (cap) *cap = batch->impl->capacity_blocks();
   });
 }
+int64_t snow_gpu_batch_fp64_projections(snow_gpu_batch* batch) {
+  return batch && batch->impl ? batch->impl->last_fp64_projections() : SNOW_E_ARG;
+}
+int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->set_chunk(chunk);
+  });
+}
 int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable) {
   return guarded([&] {
     SNOW_BATCH_OR_FAIL;

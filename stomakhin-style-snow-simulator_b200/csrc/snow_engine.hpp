@@ -62,6 +62,7 @@ class Batch {
   }
   uint32_t last_status() const { return last_status_; }
   int64_t last_blocks() const { return last_blocks_; }
+  int64_t last_fp64_projections() const { return prec_ == SNOW_MIXED ? (int64_t)h_ctr_->fp64_projections : 0; }
   int64_t capacity_blocks() const { return cap_blocks_; }
   // Particles per P2G/G2P work item (a power of two, 32..4096).
   void set_chunk(int chunk) {

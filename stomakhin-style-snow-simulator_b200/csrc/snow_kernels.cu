@@ -29,6 +29,7 @@
 
 #include <climits>
 #include <cstdio>
+#include <type_traits>
 
 #include "snow_batch.cuh"
 
@@ -180,6 +181,7 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
     c->n_halo = 0;
     c->work_p2g = c->work_grid = c->work_g2p = c->work_aux = 0;
     c->n_items = 0;
+    c->fp64_projections = 0;
   }
 }
 
@@ -634,6 +636,39 @@ __device__ __forceinline__ void flush_box(SceneDev& ps, int bmin[3], int bmax[3]
 
 // Next step's force matrix from the projected F_E, the square root returned by
 // plastic_projection and the new F_P (hardening in double).
+// Elastoplastic projection in the batch's precision.  In the mixed form the
+// float eigensolve is redone in double when a singular value lies within
+// kMixedTau of a clamp bound or of another singular value (used_fp64 = true).
+constexpr float kMixedTau = 1e-5f;
+
+template <typename R>
+__device__ __forceinline__ Plastic<R> project(M3<R>& FE, const SceneDev& sc, bool& used_fp64) {
+  if constexpr (std::is_same<R, double>::value) {
+    return plastic_projection(FE, 1.0 - sc.theta_c, 1.0 + sc.theta_s);
+  } else {
+    const M3<float> trial = FE;
+    const float lo = 1.0f - (float)sc.theta_c, hi = 1.0f + (float)sc.theta_s;
+    Plastic<float> pl = plastic_projection(FE, lo, hi);
+    if (!near_critical(pl.sigma, lo, hi, kMixedTau)) return pl;
+    used_fp64 = true;
+    M3<double> Fd;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) Fd.a[e] = (double)trial.a[e];
+    const Plastic<double> pd = plastic_projection(Fd, 1.0 - sc.theta_c, 1.0 + sc.theta_s);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) FE.a[e] = (float)Fd.a[e];
+    pl.Dinv = Sym3<float>{(float)pd.Dinv.xx, (float)pd.Dinv.yy, (float)pd.Dinv.zz,
+                          (float)pd.Dinv.xy, (float)pd.Dinv.xz, (float)pd.Dinv.yz};
+    pl.root = Sym3<float>{(float)pd.root.xx, (float)pd.root.yy, (float)pd.root.zz,
+                          (float)pd.root.xy, (float)pd.root.xz, (float)pd.root.yz};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) pl.sigma[i] = (float)pd.sigma[i];
+    pl.clamped = pd.clamped;
+    pl.regular = pd.regular;
+    return pl;
+  }
+}
+
 template <typename R>
 __device__ __forceinline__ Sym3<R> next_force(const M3<R>& FE, const Plastic<R>& pl, const M3<double>& FP,
                                               const SceneDev& sc, R V0) {
@@ -787,7 +822,13 @@ __global__ void __launch_bounds__(256, 2) k_g2p(const BatchDev b) {
           L.a[4] += R(1);
           L.a[8] += R(1);
           FEn = mat_mul(L, FE);
-          pl = plastic_projection(FEn, R(1) - (R)sc.theta_c, R(1) + (R)sc.theta_s);
+          bool used_fp64 = false;
+          pl = project(FEn, sc, used_fp64);
+          if constexpr (!std::is_same<R, double>::value) {
+            const unsigned act = __activemask();
+            const unsigned fb = __ballot_sync(act, used_fp64);
+            if (fb && (threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&b.ctr->fp64_projections, (uint32_t)__popc(fb));
+          }
 #pragma unroll
           for (int e = 0; e < 9; ++e) FPn.a[e] = pv.fp[e * pv.st + i];
           if (pl.clamped) {

@@ -273,6 +273,7 @@ template <typename T>
 struct Plastic {
   Sym3<T> Dinv;
   Sym3<T> root;
+  T sigma[3];  // singular values of the trial F_E
   bool clamped;
   bool regular;
 };
@@ -288,6 +289,7 @@ SNOW_HD Plastic<T> plastic_projection(M3<T>& FE, T lo, T hi) {
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const T s = sqrt(lam[i] > T(0) ? lam[i] : T(0));
+    out.sigma[i] = s;
     const T sc = s < lo ? lo : (s > hi ? hi : s);  // std::clamp (grid.cpp:281-283)
     if (sc != s) out.clamped = true;
     if (!(s > T(1e-6))) out.regular = false;
@@ -312,6 +314,22 @@ SNOW_HD Plastic<T> plastic_projection(M3<T>& FE, T lo, T hi) {
   }
   FE = o;
   return out;
+}
+
+// Mixed-precision guard: true when a singular value of the trial F_E lies
+// within `tau` of a clamp bound or of another singular value -- the cases where
+// a float eigensolve decides the clamp or the eigenvectors least reliably, and
+// the projection is redone in double.
+template <typename T>
+SNOW_HD bool near_critical(const T s[3], T lo, T hi, T tau) {
+  bool crit = false;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    crit |= fabs(s[i] - lo) < tau || fabs(s[i] - hi) < tau;
+#pragma unroll
+    for (int j = i + 1; j < 3; ++j) crit |= fabs(s[i] - s[j]) < tau;
+  }
+  return crit;
 }
 
 // grid_velocity (grid.cpp:195-204): for a node with mass > 0,

@@ -101,6 +101,8 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_batch_device_bytes": (i64, [vp]),
         "snow_gpu_batch_status": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint32), _i64p, _i64p]),
         "snow_gpu_batch_set_graphs": (ctypes.c_int, [vp, ctypes.c_int]),
+        "snow_gpu_batch_fp64_projections": (i64, [vp]),
+        "snow_gpu_batch_set_chunk": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_setup": (ctypes.c_int, [_dp, i64, d]),
         "snow_gpu_step": (ctypes.c_int, [_dp, i64, ctypes.POINTER(StepParams), ctypes.POINTER(Collider),
                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(StepTimings)]),
@@ -235,6 +237,15 @@ class Batch:
 
     def set_graphs(self, enable: bool) -> None:
         _check(lib().snow_gpu_batch_set_graphs(self._h, int(bool(enable))))
+
+    def set_chunk(self, chunk: int) -> None:
+        """Particles per P2G/G2P work item (power of two, 32..4096)."""
+        _check(lib().snow_gpu_batch_set_chunk(self._h, int(chunk)))
+
+    @property
+    def fp64_projections(self) -> int:
+        """Mixed form: projections redone in double during the last step."""
+        return int(lib().snow_gpu_batch_fp64_projections(self._h))
 
     def status(self) -> tuple[int, int, int]:
         st, used, cap = ctypes.c_uint32(), ctypes.c_int64(), ctypes.c_int64()
