@@ -187,6 +187,21 @@ int snow_gpu_stage_p2g(const double* records, int64_t n, double grid_spacing, in
 int snow_gpu_stage_force(const double* records, int64_t n, double grid_spacing, double mu_0,
                          double lambda_0, double hardening_coefficient, int32_t* ijk,
                          double* fields, int64_t cap_nodes, int64_t* n_nodes);
+/* P2G with a caller's stencil (src/grid.cpp:119-129): for each particle and
+ * each of its 64 stencil weights, the mass and momentum contributions
+ * out[n][64][4] = (m w, m v w); the caller adds them to the stencil's nodes. */
+int snow_gpu_stage_p2g_stencil(const double* records, int64_t n, const double* weights,
+                               double* out);
+/* force_constitutive (src/grid.cpp:162-172): the first Piola-Kirchhoff stress
+ * P of each particle, P_out[n][9] column-major. */
+int snow_gpu_stage_stress(const double* records, int64_t n, double mu_0, double lambda_0,
+                          double hardening_coefficient, double* P_out);
+/* force_grid_accumulation (src/grid.cpp:174-182): for each particle and each
+ * of its 64 stencil entries, the force (-V_p0 P F_E^T) grad w.  P[n][9]
+ * column-major, gradients[n][64][3] as build_stencil stores them; the result
+ * forces[n][64][3] is added to the stencil's nodes by the caller. */
+int snow_gpu_stage_force_scatter(const double* records, int64_t n, const double* P,
+                                 const double* gradients, double* forces);
 int snow_gpu_stage_grid_velocity(double* fields, int64_t n_nodes, const double gravity[3],
                                  double time_step);
 int snow_gpu_stage_grid_collisions(const int32_t* ijk, double* fields, int64_t n_nodes,

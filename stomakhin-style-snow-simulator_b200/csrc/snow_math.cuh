@@ -9,38 +9,9 @@
 #include <cstdint>
 #include <cmath>
 
-#define SNOW_HD __host__ __device__ __forceinline__
+#include "snow_bspline.h"
 
 namespace snow {
-
-template <typename T>
-SNOW_HD T sgn(T x) {  // signum (grid.cpp:15-20)
-  return x > T(0) ? T(1) : (x < T(0) ? T(-1) : T(0));
-}
-
-// Cubic B-spline N(a, b) of |a - b| (grid.cpp:24-40).
-template <typename T>
-SNOW_HD T bspline(T a, T b) {
-  const T d = fabs(a - b);
-  if (d >= T(0) && d < T(1)) return T(0.5) * d * d * d - d * d + T(2.0 / 3.0);
-  if (d >= T(1) && d < T(2)) return T(-1.0 / 6.0) * d * d * d + d * d - T(2) * d + T(4.0 / 3.0);
-  return T(0);
-}
-
-// N_dash(node, x) = dN/dx (grid.cpp:42-58).
-template <typename T>
-SNOW_HD T bspline_slope(T node, T x) {
-  const T d = fabs(node - x);
-  if (d >= T(0) && d < T(1)) return (T(1.5) * d * d - T(2) * d) * sgn(x - node);
-  if (d >= T(1) && d < T(2)) return (T(-1.0 / 2.0) * d * d + T(2) * d - T(2)) * sgn(x - node);
-  return T(0);
-}
-
-// Lower stencil corner base = floor(x / dx) - 1 (grid.cpp:64-67).
-template <typename T>
-SNOW_HD int stencil_base(T gp) {
-  return static_cast<int>(floor(gp)) - 1;
-}
 
 // Weights and weight slopes of the 4 stencil nodes along one axis.
 // slope[i] = N_dash / dx, as build_stencil stores it (grid.cpp:80).

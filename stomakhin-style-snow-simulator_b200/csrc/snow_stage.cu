@@ -145,6 +145,67 @@ __global__ void k_grid_collide_nodes(const int32_t* ijk, double* fields, int64_t
   for (int q = 0; q < nc; ++q) collide(c[q], x, y, z, f[4], f[5], f[6]);
 }
 
+// P = (P F^T) F^-T with P F^T = 2 mu (F F^T - sqrt(F F^T)) + lambda J (J-1) I
+// (force_matrix with V_p0 = -1), F^-T from the transposed cofactors.
+__global__ void k_stress(const double* rec, int64_t n, double mu0, double lambda0, double xi, double* P) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* p = rec + 26 * i;
+  M3<double> F, FP;
+  for (int e = 0; e < 9; ++e) {
+    FP.a[e] = p[8 + e];
+    F.a[e] = p[17 + e];
+  }
+  const double h = exp(xi * (1.0 - det3(FP)));
+  const Sym3<double> S = force_matrix<double>(F, -1.0, mu0, lambda0, h);
+  // cofactor matrix C: F^-T = C / det F
+  M3<double> C;
+  C(0, 0) = F(1, 1) * F(2, 2) - F(1, 2) * F(2, 1);
+  C(0, 1) = F(1, 2) * F(2, 0) - F(1, 0) * F(2, 2);
+  C(0, 2) = F(1, 0) * F(2, 1) - F(1, 1) * F(2, 0);
+  C(1, 0) = F(0, 2) * F(2, 1) - F(0, 1) * F(2, 2);
+  C(1, 1) = F(0, 0) * F(2, 2) - F(0, 2) * F(2, 0);
+  C(1, 2) = F(0, 1) * F(2, 0) - F(0, 0) * F(2, 1);
+  C(2, 0) = F(0, 1) * F(1, 2) - F(0, 2) * F(1, 1);
+  C(2, 1) = F(0, 2) * F(1, 0) - F(0, 0) * F(1, 2);
+  C(2, 2) = F(0, 0) * F(1, 1) - F(0, 1) * F(1, 0);
+  const double inv_det = 1.0 / (F(0, 0) * C(0, 0) + F(0, 1) * C(0, 1) + F(0, 2) * C(0, 2));
+  const double s[3][3] = {{S.xx, S.xy, S.xz}, {S.xy, S.yy, S.yz}, {S.xz, S.yz, S.zz}};
+  double* out = P + 9 * i;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      out[c * 3 + r] = (s[r][0] * C(0, c) + s[r][1] * C(1, c) + s[r][2] * C(2, c)) * inv_det;
+}
+
+// forces[i][e] = (-V_p0 P F_E^T) gradient[i][e] (grid.cpp:176-180).
+__global__ void k_force_scatter(const double* rec, int64_t n, const double* P, const double* grad, double* force) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * 64) return;
+  const int64_t i = t / 64;
+  const double* p = rec + 26 * i;
+  const double* Pi = P + 9 * i;
+  const double V0 = p[7];
+  double M[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k) acc += Pi[k * 3 + r] * p[17 + k * 3 + c];  // P(r,k) F_E(c,k)
+      M[r][c] = -V0 * acc;
+    }
+  const double* g = grad + 3 * t;
+  for (int r = 0; r < 3; ++r) force[3 * t + r] = M[r][0] * g[0] + M[r][1] * g[1] + M[r][2] * g[2];
+}
+
+// out[i][e] = (m w, m v w) for stencil weight w = weights[i][e] (grid.cpp:121-127).
+__global__ void k_p2g_stencil(const double* rec, int64_t n, const double* weights, double* out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * 64) return;
+  const double* p = rec + 26 * (t / 64);
+  const double w = weights[t], m = p[6];
+  out[4 * t] = w * m;
+  for (int a = 0; a < 3; ++a) out[4 * t + 1 + a] = w * (m * p[3 + a]);
+}
+
 __global__ void k_particle_collide(double* rec, int64_t n, const Collider* c, int nc) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -252,6 +313,50 @@ int snow_gpu_stage_force(const double* records, int64_t n, double grid_spacing, 
     StepLaunch<double>::p2g(sg.b, P2G_FORCE, nullptr);
     check_cuda(cudaDeviceSynchronize(), "stage force");
     sg.export_nodes(ijk, fields, cap_nodes, n_nodes);
+  });
+}
+
+int snow_gpu_stage_p2g_stencil(const double* records, int64_t n, const double* weights, double* out) {
+  return guarded([&] {
+    check_records(records, n);
+    if (n > 0 && (!weights || !out)) throw Error(SNOW_E_ARG, "NULL argument");
+    if (n == 0) return;
+    DBuf<double> d((size_t)n * 26), dw((size_t)n * 64), dout((size_t)n * 256);
+    check_cuda(cudaMemcpy(d.p, records, n * 208, cudaMemcpyHostToDevice), "records");
+    check_cuda(cudaMemcpy(dw.p, weights, n * 64 * 8, cudaMemcpyHostToDevice), "weights");
+    k_p2g_stencil<<<blocks_for(n * 64), 256>>>(d.p, n, dw.p, dout.p);
+    check_cuda(cudaGetLastError(), "p2g stencil");
+    check_cuda(cudaMemcpy(out, dout.p, n * 256 * 8, cudaMemcpyDeviceToHost), "contributions");
+  });
+}
+
+int snow_gpu_stage_stress(const double* records, int64_t n, double mu_0, double lambda_0,
+                          double hardening_coefficient, double* P_out) {
+  return guarded([&] {
+    check_records(records, n);
+    if (n > 0 && !P_out) throw Error(SNOW_E_ARG, "P_out is NULL");
+    if (n == 0) return;
+    DBuf<double> d((size_t)n * 26), dp((size_t)n * 9);
+    check_cuda(cudaMemcpy(d.p, records, n * 208, cudaMemcpyHostToDevice), "records");
+    k_stress<<<blocks_for(n), 256>>>(d.p, n, mu_0, lambda_0, hardening_coefficient, dp.p);
+    check_cuda(cudaGetLastError(), "stress");
+    check_cuda(cudaMemcpy(P_out, dp.p, n * 72, cudaMemcpyDeviceToHost), "stress out");
+  });
+}
+
+int snow_gpu_stage_force_scatter(const double* records, int64_t n, const double* P, const double* gradients,
+                                 double* forces) {
+  return guarded([&] {
+    check_records(records, n);
+    if (n > 0 && (!P || !gradients || !forces)) throw Error(SNOW_E_ARG, "NULL argument");
+    if (n == 0) return;
+    DBuf<double> d((size_t)n * 26), dp((size_t)n * 9), dg((size_t)n * 192), df((size_t)n * 192);
+    check_cuda(cudaMemcpy(d.p, records, n * 208, cudaMemcpyHostToDevice), "records");
+    check_cuda(cudaMemcpy(dp.p, P, n * 72, cudaMemcpyHostToDevice), "P");
+    check_cuda(cudaMemcpy(dg.p, gradients, n * 192 * 8, cudaMemcpyHostToDevice), "gradients");
+    k_force_scatter<<<blocks_for(n * 64), 256>>>(d.p, n, dp.p, dg.p, df.p);
+    check_cuda(cudaGetLastError(), "force scatter");
+    check_cuda(cudaMemcpy(forces, df.p, n * 192 * 8, cudaMemcpyDeviceToHost), "forces");
   });
 }
 

@@ -1,0 +1,188 @@
+// CSV particle import and frame export with the reference's semantics
+// (src/import.cpp, src/export.cpp): the same files, columns, skipped header and
+// blank lines, field rules and error messages.  The parser reads each file in
+// one piece and converts numbers with std::from_chars where the text is a
+// plain decimal (falling back to std::stoi/std::stod, the reference's
+// conversions, for anything else), instead of a stringstream per field.
+#include <charconv>
+#include <cstdint>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iterator>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <string_view>
+#include <vector>
+
+#include "snow/export.hpp"
+#include "snow/import.hpp"
+#include "snow_host_detail.hpp"
+
+namespace
+{
+std::string read_file(const std::string& filename)
+{
+    std::ifstream file(filename, std::ios::binary);
+    if (!file.is_open()) throw std::runtime_error{"File not open: " + filename};
+    return std::string(std::istreambuf_iterator<char>(file), std::istreambuf_iterator<char>());
+}
+
+// Lines as std::getline yields them: split at '\n', no empty final segment.
+std::vector<std::string_view> lines_of(const std::string& text)
+{
+    std::vector<std::string_view> out;
+    std::size_t pos = 0;
+    while (pos < text.size())
+    {
+        const std::size_t nl = text.find('\n', pos);
+        if (nl == std::string::npos)
+        {
+            out.emplace_back(text.data() + pos, text.size() - pos);
+            break;
+        }
+        out.emplace_back(text.data() + pos, nl - pos);
+        pos = nl + 1;
+    }
+    return out;
+}
+
+// Comma-separated fields of one line, read as std::getline(row, field, ',')
+// reads them: a read past the last character fails ("Missing"); a trailing
+// '\r' is dropped; an empty field is an error ("Empty").
+class Fields
+{
+public:
+    explicit Fields(std::string_view line) : line_(line) {}
+    std::string_view next(const char* column)
+    {
+        if (pos_ >= line_.size()) throw std::runtime_error{std::string("Missing CSV field: ") + column};
+        const std::size_t comma = line_.find(',', pos_);
+        std::string_view f = comma == std::string_view::npos ? line_.substr(pos_) : line_.substr(pos_, comma - pos_);
+        pos_ = comma == std::string_view::npos ? line_.size() : comma + 1;
+        if (!f.empty() && f.back() == '\r') f.remove_suffix(1);
+        if (f.empty()) throw std::runtime_error{std::string("Empty CSV field: ") + column};
+        return f;
+    }
+
+private:
+    std::string_view line_;
+    std::size_t pos_ = 0;
+};
+
+bool plain_number(std::string_view f)
+{
+    const char c = f.front();
+    if (!(c == '-' || c == '.' || (c >= '0' && c <= '9'))) return false;
+    return f.find_first_of("xX") == std::string_view::npos;
+}
+
+int to_int(std::string_view f)
+{
+    int v = 0;
+    if (plain_number(f) && f.find('.') == std::string_view::npos)
+    {
+        const auto r = std::from_chars(f.data(), f.data() + f.size(), v);
+        if (r.ec == std::errc()) return v;
+    }
+    return std::stoi(std::string(f));  // the reference's conversion and exceptions
+}
+
+double to_double(std::string_view f)
+{
+    double v = 0.0;
+    if (plain_number(f))
+    {
+        const auto r = std::from_chars(f.data(), f.data() + f.size(), v);
+        if (r.ec == std::errc() && r.ptr != f.data()) return v;
+    }
+    return std::stod(std::string(f));
+}
+}  // namespace
+
+std::map<int, ParticleGroup> import_groups(const std::string& filename)
+{
+    const std::string text = read_file(filename);
+    const auto lines = lines_of(text);
+    if (lines.empty()) throw std::runtime_error{"Group data file is empty: " + filename};
+    std::map<int, ParticleGroup> groups;
+    for (std::size_t k = 1; k < lines.size(); ++k)
+    {
+        if (lines[k].empty()) continue;
+        Fields row(lines[k]);
+        const int id = to_int(row.next("group_ID"));
+        const double vx = to_double(row.next("v_x"));
+        const double vy = to_double(row.next("v_y"));
+        const double vz = to_double(row.next("v_z"));
+        const double m = to_double(row.next("m"));
+        if (!groups.emplace(id, ParticleGroup{Eigen::Vector3d{vx, vy, vz}, m}).second)
+            throw std::runtime_error{"Duplicate group id: " + std::to_string(id)};
+    }
+    return groups;
+}
+
+std::vector<ParticleSeed> import_particle_seeds(const std::string& filename)
+{
+    const std::string text = read_file(filename);
+    const auto lines = lines_of(text);
+    if (lines.empty()) throw std::runtime_error{"Particle data file is empty: " + filename};
+    std::vector<ParticleSeed> seeds;
+    seeds.reserve(lines.size());
+    for (std::size_t k = 1; k < lines.size(); ++k)
+    {
+        if (lines[k].empty()) continue;
+        Fields row(lines[k]);
+        const int id = to_int(row.next("group_ID"));
+        const double x = to_double(row.next("x"));
+        const double y = to_double(row.next("y"));
+        const double z = to_double(row.next("z"));
+        seeds.push_back(ParticleSeed{id, Eigen::Vector3d{x, y, z}});
+    }
+    return seeds;
+}
+
+std::vector<Particle> assemble_particles(const std::vector<ParticleSeed>& seeds,
+                                         const std::map<int, ParticleGroup>& groups)
+{
+    std::vector<Particle> particles;
+    particles.reserve(seeds.size());
+    for (const ParticleSeed& s : seeds)
+    {
+        const auto it = groups.find(s.group_id);
+        if (it == groups.end())
+            throw std::runtime_error{"Particle references undefined group id: " + std::to_string(s.group_id)};
+        particles.emplace_back(s.position, it->second.velocity, it->second.mass, 0.0);
+    }
+    return particles;
+}
+
+std::vector<Particle> import_particles(const std::string& filename_group, const std::string& filename_particle_seed)
+{
+    const auto groups = import_groups(filename_group);
+    const auto seeds = import_particle_seeds(filename_particle_seed);
+    return assemble_particles(seeds, groups);
+}
+
+void export_particles(const std::vector<Particle>& particles, int frame_no)
+{
+    // A vector kept on the GPU by resident stepping is read back first.
+    std::vector<double> fresh;
+    const double* rec = reinterpret_cast<const double*>(particles.data());
+    if (!particles.empty())
+    {
+        fresh.resize(particles.size() * SNOW_RECORD_DOUBLES);
+        if (snow_host_resident_copy(particles, fresh.data())) rec = fresh.data();
+    }
+    std::ostringstream name;
+    name << "output/frame_" << std::setw(6) << std::setfill('0') << frame_no << ".csv";
+    std::ofstream file{name.str()};
+    std::ostringstream out;
+    out << "x,y,z\n";
+    for (std::size_t i = 0; i < particles.size(); ++i)
+    {
+        const double* p = rec + SNOW_RECORD_DOUBLES * i;
+        out << p[0] << "," << p[2] * -1 << "," << p[1] << "\n";
+    }
+    file << out.str();
+}

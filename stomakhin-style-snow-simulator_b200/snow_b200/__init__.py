@@ -110,6 +110,9 @@ def lib() -> ctypes.CDLL:
                                                  ctypes.c_int, ctypes.c_int, vp]),
         "snow_gpu_stage_p2g": (ctypes.c_int, [_dp, i64, d, _ip, _dp, i64, _i64p]),
         "snow_gpu_stage_force": (ctypes.c_int, [_dp, i64, d, d, d, d, _ip, _dp, i64, _i64p]),
+        "snow_gpu_stage_p2g_stencil": (ctypes.c_int, [_dp, i64, _dp, _dp]),
+        "snow_gpu_stage_stress": (ctypes.c_int, [_dp, i64, d, d, d, _dp]),
+        "snow_gpu_stage_force_scatter": (ctypes.c_int, [_dp, i64, _dp, _dp, _dp]),
         "snow_gpu_stage_grid_velocity": (ctypes.c_int, [_dp, i64, _dp, d]),
         "snow_gpu_stage_grid_collisions": (ctypes.c_int, [_ip, _dp, i64, ctypes.POINTER(Collider),
                                                           ctypes.c_int, d]),
