@@ -37,7 +37,7 @@ sys.path.insert(0, PKG)
 
 import numpy as np  # noqa: E402
 
-KERNELS_PER_STEP = 19  # keyspace, keys, 4 x 3 sort passes, 2 block builds, p2g, grid, g2p, finish
+KERNELS_PER_STEP = 20  # keyspace, keys, 4 x 3 sort passes, 2 block builds, items, p2g, grid, g2p, finish
 REF_SAMPLE_S = 20.0    # target seconds of reference CPU work per bounded sample
 
 
@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed / batched / served forms")
     return ap.parse_args()
 
 
@@ -173,13 +174,155 @@ def device_selector(torch, dev: int) -> str:
 def alg_bytes(n_p: int, nodes: int, real: int) -> dict:
     """Algorithmic DRAM bytes per launch of the two particle kernels.
 
-    p2g reads the particle state (x, v, m, V_p0, F_E in `real`, F_P in double) and
-        writes the 7 accumulated channels of every grid node;
-    g2p reads the particle state and 6 channels per node and writes the new state.
+    p2g reads x, v, m and the 6-entry force matrix (13 `real` values) per
+        particle and writes the 7 accumulated channels of every grid node;
+    g2p reads x, v, m, V_p0, F_E (17 `real`) and F_P (9 doubles) per particle and
+        the 6 velocity channels per node, and writes the new state: x, v, m, V_p0,
+        F_E, the next force matrix (23 `real`), F_P and the particle id.
     """
-    state = 17 * real + 9 * 8
-    return {"p2g": n_p * state + nodes * 7 * real,
-            "g2p": n_p * 2 * state + nodes * 6 * real}
+    return {"p2g": n_p * 13 * real + nodes * 7 * real,
+            "g2p": n_p * (17 * real + 72) + nodes * 6 * real + n_p * (23 * real + 72 + 4)}
+
+
+def errors(a, b) -> dict:
+    """Per-quantity max relative error of records a against b: ||a_i - b_i|| / max(||b_i||, 1e-6)."""
+    out = {}
+    for k, s in (("x", slice(0, 3)), ("v", slice(3, 6)), ("F_P", slice(8, 17)), ("F_E", slice(17, 26))):
+        num = np.linalg.norm(a[:, s] - b[:, s], axis=1)
+        den = np.maximum(np.linalg.norm(b[:, s], axis=1), 1e-6)
+        out[k] = float(np.max(num / den))
+    return out
+
+
+def timed_steps(batch, steps, sp, torch) -> float:
+    """Device milliseconds of `steps` graph-replayed steps on stream sp."""
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    batch.step(steps, stream=sp)
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
+    """The mixed-precision, batched and served forms (single GPU).
+
+    mixed     the headline scene in the mixed form: particle-steps/s, ratio to the
+              plain FP64 path, error vs the FP64 path after 1 and 10 steps
+    batched   256 independent scenes (log-uniform 1k..64k particles), one launch per
+              stage: FP64 and autotuned mixed particle-steps/s, mixed error after 10 steps
+    served    a Poisson stream of scene requests admitted by memory budget and
+              stepped together: p50/p99 latency and aggregate particle-steps/s
+    snowball  4M-particle sphere, mixed vs FP64 error at steps 1, 10 and 200
+    """
+    from snow_b200 import scenes
+
+    forms = {}
+    # -- mixed form of the headline scene
+    mixed = snow_b200.Batch(snow_b200.SNOW_MIXED)
+    mid = mixed.add(tori, stream=sp)
+    mixed.setup(mid, tori.dx, stream=sp)
+    mixed.step(5, stream=sp)
+    ms = timed_steps(mixed, steps, sp, torch)
+    rate = tori.n * steps / (ms * 1e-3)
+    mixed.close()
+    ref = snow_b200.Batch(snow_b200.SNOW_FP64)
+    rid = ref.add(tori, stream=sp)
+    ref.setup(rid, tori.dx, stream=sp)
+    start = ref.download(rid)
+    errs = {}
+    for n in (1, 10):
+        a = snow_b200.Batch(snow_b200.SNOW_FP64)
+        b = snow_b200.Batch(snow_b200.SNOW_MIXED)
+        ia, ib = a.add_scene(start, tori.params(), tori.planes), b.add_scene(start, tori.params(), tori.planes)
+        a.step(n)
+        b.step(n)
+        errs[f"step{n}"] = errors(b.download(ib), a.download(ia))
+        errs[f"step{n}_fp64_projections"] = b.fp64_projections
+        a.close()
+        b.close()
+    ref.close()
+    forms["mixed"] = {"workload": tori.name, "value": rate, "unit": "particle-steps/s",
+                      "ms_per_step": ms / steps, "vs_plain_fp64": rate / fp64_rate,
+                      "error_vs_fp64": errs}
+    # -- batched: 256 scenes, FP64 and mixed
+    bscenes = scenes.batch_scenes(count=256)
+    nb = sum(s.n for s in bscenes)
+    brates = {}
+    for name, prec in (("fp64", snow_b200.SNOW_FP64), ("mixed", snow_b200.SNOW_MIXED)):
+        b = snow_b200.Batch(prec)
+        ids = [b.add(s, stream=sp) for s in bscenes]
+        for i, s in zip(ids, bscenes):
+            b.setup(i, s.dx, stream=sp)
+        b.step(3, stream=sp)
+        chunk, _ = b.autotune(trial_steps=5, stream=sp)
+        bsteps = max(20, steps // 4)
+        ms_b = timed_steps(b, bsteps, sp, torch)
+        brates[name] = {"value": nb * bsteps / (ms_b * 1e-3), "ms_per_step": ms_b / bsteps,
+                        "work_item": chunk}
+        b.close()
+    berr = {}
+    a = snow_b200.Batch(snow_b200.SNOW_FP64)
+    b = snow_b200.Batch(snow_b200.SNOW_MIXED)
+    sample = bscenes[:16]
+    pa = [a.add(s) for s in sample]
+    pb = [b.add(s) for s in sample]
+    for i, j, s in zip(pa, pb, sample):
+        a.setup(i, s.dx)
+        b.setup(j, s.dx)
+    a.step(10)
+    b.step(10)
+    worst = {}
+    for i, j in zip(pa, pb):
+        e = errors(b.download(j), a.download(i))
+        for k, v in e.items():
+            worst[k] = max(worst.get(k, 0.0), v)
+    a.close()
+    b.close()
+    forms["batched"] = {"scenes": len(bscenes), "particles": nb, "unit": "particle-steps/s",
+                        "fp64": brates["fp64"], "mixed": brates["mixed"],
+                        "mixed_vs_fp64": brates["mixed"]["value"] / brates["fp64"]["value"],
+                        "mixed_vs_plain_fp64_headline": brates["mixed"]["value"] / fp64_rate,
+                        "mixed_error_vs_fp64_step10_first16": worst,
+                        "graph": "CUDA graph per step", "autotuned": "work-item size"}
+    # -- served: Poisson stream, mixed form
+    reqs = scenes.served_requests(count=48, rate=200.0)
+    srv = snow_b200.Server(snow_b200.SNOW_MIXED, budget_bytes=150 * 10**9, max_steps_per_tick=16)
+    for sc, n, t in reqs:
+        srv.submit(sc, n, t)
+    srv.run(stream=sp)
+    st = srv.stats()
+    srv.close()
+    forms["served"] = {"requests": len(reqs), "arrival_rate_per_s": 200.0, "budget_bytes": 150 * 10**9,
+                       "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"],
+                       "mean_latency_s": st["mean_s"], "particle_steps_per_s": st["particle_steps_per_s"],
+                       "served_vs_plain_fp64_headline": st["particle_steps_per_s"] / fp64_rate,
+                       "peak_concurrent_scenes": st["peak_scenes"], "ticks": st["ticks"],
+                       "wall_s": st["wall_s"], "precision": "mixed"}
+    # -- snowball: error of the mixed form at steps 1, 10, 200
+    ball = scenes.snowball_scene()
+    a = snow_b200.Batch(snow_b200.SNOW_FP64)
+    ia = a.add(ball, stream=sp)
+    a.setup(ia, ball.dx, stream=sp)
+    start = a.download(ia)
+    b = snow_b200.Batch(snow_b200.SNOW_MIXED)
+    ib = b.add_scene(start, ball.params(), ball.planes)
+    serr = {}
+    done = 0
+    t_fp64 = t_mixed = 0.0
+    for n in (1, 10, 200):
+        t_fp64 += timed_steps(a, n - done, sp, torch)
+        t_mixed += timed_steps(b, n - done, sp, torch)
+        done = n
+        serr[f"step{n}"] = errors(b.download(ib), a.download(ia))
+    a.close()
+    b.close()
+    forms["snowball"] = {"workload": ball.name, "error_vs_fp64": serr,
+                         "fp64_particle_steps_per_s": ball.n * 200 / (t_fp64 * 1e-3),
+                         "mixed_particle_steps_per_s": ball.n * 200 / (t_mixed * 1e-3)}
+    return forms
 
 
 def measured_peak() -> tuple[float, str]:
@@ -289,6 +432,9 @@ def run_ours(args, ws, rank, local):
                "sample": f"{steps} full-scene steps ({wall:.1f} s) after setup(); {what}"}
 
     value = ws * sc.n * args.steps / (ms * 1e-3)
+    forms = None
+    if ws == 1 and not args.no_forms and args.workload == "tori" and args.precision == "fp64":
+        forms = measure_forms(snow_b200, torch, sp, sc, sc.n * args.steps / (ms * 1e-3), args.steps)
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
@@ -311,6 +457,7 @@ def run_ours(args, ws, rank, local):
         "clocks": clk,
         "grid_blocks": {"used": blocks, "capacity": cap},
         "status": status,
+        "forms": forms,
     }
     batch.close()
     if dist is not None:

@@ -146,11 +146,42 @@ int snow_gpu_batch_status(snow_gpu_batch* batch, uint32_t* status, int64_t* bloc
 /* Use (1) or bypass (0) CUDA-graph replay for timing-free steps. */
 int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable);
 /* Mixed form: particles whose plastic projection was redone in double in the
- * last step (a singular value within 1e-5 of a clamp bound or of another
- * singular value).  0 for an FP64 batch. */
+ * last step (a singular value within 1e-5 of a clamp bound, or a clamp acting
+ * with two singular values within 1e-5 of each other).  0 for an FP64 batch. */
 int64_t snow_gpu_batch_fp64_projections(snow_gpu_batch* batch);
 /* Particles per P2G/G2P work item (power of two in [32, 4096]; default 256). */
 int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk);
+
+/* Autotuner: times `trial_steps` steps of the batch for each work-item size
+ * (particles per P2G/G2P CTA work item: 64 ... 1024) on a snapshot of the
+ * current state, restores the state, keeps the fastest size and reports it in
+ * *chosen (and its ms per step in *ms_per_step).  No reference counterpart. */
+int snow_gpu_batch_autotune(snow_gpu_batch* batch, int trial_steps, int* chosen, double* ms_per_step,
+                            void* stream);
+
+/* ---- serving: continuous batching of independent scenes -----------------
+ * No reference counterpart.  Requests are queued with an arrival time (seconds
+ * on the server's clock, which starts when run() starts); run() admits each
+ * one once it has arrived and the device-memory budget and scene slots allow,
+ * runs setup() on it, advances all admitted scenes together (at most
+ * max_steps_per_tick steps per tick, never past a scene's end), and retires
+ * finished scenes, until every request is done or rejected (a request larger
+ * than the whole budget).  Latency = completion - arrival. */
+typedef struct snow_gpu_server snow_gpu_server;
+typedef struct snow_server_stats {
+  int64_t completed, rejected, peak_scenes, peak_bytes, ticks, particle_steps;
+  double wall_s, p50_s, p99_s, mean_s, particle_steps_per_s;
+} snow_server_stats;
+int snow_gpu_server_create(snow_gpu_server** out, int precision, int64_t hbm_budget_bytes,
+                           int max_scenes, int max_steps_per_tick);
+int snow_gpu_server_destroy(snow_gpu_server* server);
+int snow_gpu_server_submit(snow_gpu_server* server, const double* records, int64_t n,
+                           const snow_step_params* params, const snow_collider* colliders,
+                           int n_colliders, int64_t steps, double arrival_s, int64_t* request_id);
+int snow_gpu_server_run(snow_gpu_server* server, void* stream);
+int snow_gpu_server_result(snow_gpu_server* server, int64_t request_id, double* records, int64_t n,
+                           double* latency_s);
+int snow_gpu_server_stats(snow_gpu_server* server, snow_server_stats* stats);
 
 /* ---- one scene: setup() / step() of the reference ------------------------ */
 /* setup() on host records: records[i].V_p0 is overwritten. */

@@ -590,6 +590,74 @@ void Batch::setup(int32_t id, double dx, cudaStream_t s) {
   check_status();
 }
 
+// Work-item-size autotuner.  Each candidate runs from the same snapshot of the
+// particle state (restored afterwards), two warm-up steps (the second captures
+// the step graph), then `trial_steps` timed steps on the stream.
+int Batch::autotune(int trial_steps, double* best_ms, cudaStream_t s) {
+  if (trial_steps <= 0) throw Error(SNOW_E_ARG, "trial_steps must be positive");
+  if (scenes_.empty()) throw Error(SNOW_E_STATE, "empty batch");
+  if (!s) s = own_stream_;
+  struct Snap {
+    Scene* sc;
+    int cur;
+    unsigned char* buf;
+    size_t r_bytes, fp_bytes, id_bytes;
+  };
+  std::vector<Snap> snaps;
+  for (auto& sc : scenes_) {
+    Snap sn{sc.get(), sc->cur, nullptr, (size_t)sc->stride * kRealPlanes * rsize_,
+            (size_t)sc->stride * kFPPlanes * sizeof(double), (size_t)sc->stride * sizeof(int32_t)};
+    sn.buf = dalloc<unsigned char>(sn.r_bytes + sn.fp_bytes + sn.id_bytes);
+    check_cuda(cudaMemcpyAsync(sn.buf, sc->r[sc->cur], sn.r_bytes, cudaMemcpyDeviceToDevice, s), "snapshot");
+    check_cuda(cudaMemcpyAsync(sn.buf + sn.r_bytes, sc->fp[sc->cur], sn.fp_bytes, cudaMemcpyDeviceToDevice, s), "snapshot");
+    check_cuda(cudaMemcpyAsync(sn.buf + sn.r_bytes + sn.fp_bytes, sc->id[sc->cur], sn.id_bytes,
+                               cudaMemcpyDeviceToDevice, s), "snapshot");
+    snaps.push_back(sn);
+  }
+  auto restore = [&] {
+    for (auto& sn : snaps) {
+      Scene* sc = sn.sc;
+      sc->cur = sn.cur;
+      check_cuda(cudaMemcpyAsync(sc->r[sc->cur], sn.buf, sn.r_bytes, cudaMemcpyDeviceToDevice, s), "restore");
+      check_cuda(cudaMemcpyAsync(sc->fp[sc->cur], sn.buf + sn.r_bytes, sn.fp_bytes, cudaMemcpyDeviceToDevice, s),
+                 "restore");
+      check_cuda(cudaMemcpyAsync(sc->id[sc->cur], sn.buf + sn.r_bytes + sn.fp_bytes, sn.id_bytes,
+                                 cudaMemcpyDeviceToDevice, s), "restore");
+    }
+    boxes_dirty_ = true;
+    force_dirty_ = true;
+  };
+  const int candidates[] = {64, 128, 256, 512, 1024};
+  int best = chunk_;
+  double best_t = 1e300;
+  cudaEvent_t e0, e1;
+  check_cuda(cudaEventCreate(&e0), "event");
+  check_cuda(cudaEventCreate(&e1), "event");
+  for (int c : candidates) {
+    set_chunk(c);
+    restore();
+    step(2, nullptr, s);
+    check_cuda(cudaEventRecord(e0, s), "event");
+    step(trial_steps, nullptr, s);
+    check_cuda(cudaEventRecord(e1, s), "event");
+    check_cuda(cudaEventSynchronize(e1), "event");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_t) {
+      best_t = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  set_chunk(best);
+  restore();
+  check_cuda(cudaStreamSynchronize(s), "restore");
+  for (auto& sn : snaps) dfree(sn.buf);
+  if (best_ms) *best_ms = best_t / trial_steps;
+  return best;
+}
+
 int64_t Batch::device_bytes() const {
   int64_t b = 0;
   for (auto& sc : scenes_) b += 2 * sc->stride * (kRealPlanes * (int64_t)rsize_ + kFPPlanes * 8 + 4);
@@ -741,6 +809,14 @@ int snow_gpu_batch_status(snow_gpu_batch* batch, uint32_t* status, int64_t* used
     if (status) *status = batch->impl->last_status();
     if (used) *used = batch->impl->last_blocks();
     if (cap) *cap = batch->impl->capacity_blocks();
+  });
+}
+int snow_gpu_batch_autotune(snow_gpu_batch* batch, int trial_steps, int* chosen, double* ms_per_step,
+                            void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    const int c = batch->impl->autotune(trial_steps, ms_per_step, as_stream(stream));
+    if (chosen) *chosen = c;
   });
 }
 int64_t snow_gpu_batch_fp64_projections(snow_gpu_batch* batch) {

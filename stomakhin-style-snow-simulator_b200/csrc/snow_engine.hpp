@@ -49,6 +49,7 @@ class Batch {
   void download(int32_t id, double* records, int64_t n, cudaStream_t s);
   void setup(int32_t id, double dx, cudaStream_t s);
   void step(int n_steps, snow_step_timings* timings, cudaStream_t s);
+  int autotune(int trial_steps, double* best_ms, cudaStream_t s);
 
   int scene_count() const { return (int)scenes_.size(); }
   int64_t particles() const {

@@ -638,7 +638,8 @@ __device__ __forceinline__ void flush_box(SceneDev& ps, int bmin[3], int bmax[3]
 // plastic_projection and the new F_P (hardening in double).
 // Elastoplastic projection in the batch's precision.  In the mixed form the
 // float eigensolve is redone in double when a singular value lies within
-// kMixedTau of a clamp bound or of another singular value (used_fp64 = true).
+// kMixedTau of a clamp bound, or a clamp acts on two singular values within
+// kMixedTau of each other (used_fp64 = true; see near_critical).
 constexpr float kMixedTau = 1e-5f;
 
 template <typename R>
@@ -649,7 +650,7 @@ __device__ __forceinline__ Plastic<R> project(M3<R>& FE, const SceneDev& sc, boo
     const M3<float> trial = FE;
     const float lo = 1.0f - (float)sc.theta_c, hi = 1.0f + (float)sc.theta_s;
     Plastic<float> pl = plastic_projection(FE, lo, hi);
-    if (!near_critical(pl.sigma, lo, hi, kMixedTau)) return pl;
+    if (!near_critical(pl.sigma, lo, hi, kMixedTau, pl.clamped)) return pl;
     used_fp64 = true;
     M3<double> Fd;
 #pragma unroll

@@ -288,17 +288,23 @@ SNOW_HD Plastic<T> plastic_projection(M3<T>& FE, T lo, T hi) {
 }
 
 // Mixed-precision guard: true when a singular value of the trial F_E lies
-// within `tau` of a clamp bound or of another singular value -- the cases where
-// a float eigensolve decides the clamp or the eigenvectors least reliably, and
-// the projection is redone in double.
+// within `tau` of a clamp bound (the float eigensolve may decide the clamp
+// wrongly), or when a clamp acts and two singular values lie within `tau` of
+// each other (the float eigenvectors of the nearly repeated pair are then least
+// reliable and the clamp acts along them) -- the cases in which the projection
+// is redone in double.  Without a clamp the projection is the identity, and
+// nearly repeated singular values (F_E close to a rotation, the common
+// unstrained state) need no double.
 template <typename T>
-SNOW_HD bool near_critical(const T s[3], T lo, T hi, T tau) {
+SNOW_HD bool near_critical(const T s[3], T lo, T hi, T tau, bool clamped) {
   bool crit = false;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     crit |= fabs(s[i] - lo) < tau || fabs(s[i] - hi) < tau;
+    if (clamped) {
 #pragma unroll
-    for (int j = i + 1; j < 3; ++j) crit |= fabs(s[i] - s[j]) < tau;
+      for (int j = i + 1; j < 3; ++j) crit |= fabs(s[i] - s[j]) < tau;
+    }
   }
   return crit;
 }

@@ -1,0 +1,273 @@
+// Continuous-batching server for independent snow scenes (no counterpart in
+// the reference, which steps one scene in a loop).
+//
+// Requests -- a particle set, its step parameters and colliders, a number of
+// steps and an arrival time -- are queued, then admitted as their arrival time
+// passes and the device-memory budget and scene slots allow.  Admitted scenes
+// stay resident; every tick advances all of them together by the same number
+// of steps (one launch per kernel for the whole batch, replayed from a CUDA
+// graph), at most until the next scene finishes.  A finished scene is copied
+// back, removed, and its latency (arrival to result) recorded.  Scenes do not
+// interact, so each result is the one the scene would get alone.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <deque>
+#include <memory>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+#include "snow_engine.hpp"
+#include "snow_gpu.h"
+
+namespace snow {
+namespace {
+
+using clock_t_ = std::chrono::steady_clock;
+
+struct Request {
+  int64_t id = 0;
+  std::vector<double> records;
+  snow_step_params params{};
+  std::vector<snow_collider> colliders;
+  int64_t steps = 0;
+  double arrival = 0.0;   // seconds on the server clock
+  // progress
+  int32_t scene = -1;
+  int64_t remaining = 0;
+  double admitted = -1.0, finished = -1.0;
+  int64_t bytes = 0;
+  bool rejected = false;
+};
+
+}  // namespace
+
+class Server {
+ public:
+  Server(int precision, int64_t budget, int max_scenes, int max_tick_steps)
+      : batch_(precision), prec_(precision), budget_(budget), max_scenes_(max_scenes),
+        max_tick_(max_tick_steps) {}
+
+  int64_t submit(const double* rec, int64_t n, const snow_step_params* p, const snow_collider* c, int nc,
+                 int64_t steps, double arrival) {
+    if (n < 0 || (n > 0 && !rec) || steps < 0 || !p || nc < 0 || (nc > 0 && !c))
+      throw Error(SNOW_E_ARG, "bad request");
+    auto r = std::make_unique<Request>();
+    r->id = (int64_t)reqs_.size();
+    r->records.assign(rec, rec + n * 26);
+    r->params = *p;
+    r->colliders.assign(c, c + nc);
+    r->steps = steps;
+    r->arrival = arrival;
+    r->bytes = footprint(n);
+    reqs_.push_back(std::move(r));
+    return reqs_.back()->id;
+  }
+
+  // Device bytes a scene of n particles holds: two particle buffers, sort
+  // buffers, and its share of the grid (about one 4x4x4 block per 32
+  // particles, with the grid's 2x headroom).
+  int64_t footprint(int64_t n) const {
+    const int64_t real = prec_ == SNOW_FP64 ? 8 : 4;
+    const int64_t per_particle = 2 * (kRealPlanes * real + kFPPlanes * 8 + 4) + 16 + 26 * 8 / 4;
+    const int64_t grid = 2 * ((n + 31) / 32) * 64 * (kAccCh + kVelCh) * real;
+    return n * per_particle + grid + (1 << 16);
+  }
+
+  void run(cudaStream_t s) {
+    std::vector<Request*> order;
+    for (auto& r : reqs_)
+      if (r->finished < 0 && !r->rejected) order.push_back(r.get());
+    std::stable_sort(order.begin(), order.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
+    std::deque<Request*> pending(order.begin(), order.end());
+    std::vector<Request*> live;
+    int64_t used = 0;
+    const auto t0 = clock_t_::now();
+    auto now = [&] { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
+    while (!pending.empty() || !live.empty()) {
+      // admit every arrived request that fits, in arrival order
+      while (!pending.empty() && pending.front()->arrival <= now()) {
+        Request* r = pending.front();
+        if (r->bytes > budget_) {  // can never fit
+          r->rejected = true;
+          pending.pop_front();
+          ++rejected_;
+          continue;
+        }
+        if (used + r->bytes > budget_ || (int)live.size() >= max_scenes_) break;
+        pending.pop_front();
+        const int64_t n = (int64_t)r->records.size() / 26;
+        r->scene = batch_.add_scene(r->records.data(), n, &r->params, r->colliders.data(),
+                                    (int)r->colliders.size(), s);
+        batch_.setup(r->scene, r->params.grid_spacing, s);
+        r->remaining = r->steps;
+        r->admitted = now();
+        used += r->bytes;
+        live.push_back(r);
+        peak_scenes_ = std::max<int64_t>(peak_scenes_, (int64_t)live.size());
+        peak_bytes_ = std::max(peak_bytes_, used);
+      }
+      // retire scenes with nothing left to do (zero-step requests)
+      retire(live, used, now, s, true);
+      if (live.empty()) {
+        if (!pending.empty()) {
+          const double wait = pending.front()->arrival - now();
+          if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
+        }
+        continue;
+      }
+      int64_t k = max_tick_;
+      for (Request* r : live) k = std::min(k, r->remaining);
+      batch_.step((int)k, nullptr, s);
+      ++ticks_;
+      for (Request* r : live) {
+        r->remaining -= k;
+        particle_steps_ += k * ((int64_t)r->records.size() / 26);
+      }
+      retire(live, used, now, s, false);
+    }
+    wall_ += now();
+  }
+
+  const Request& req(int64_t id) const {
+    if (id < 0 || id >= (int64_t)reqs_.size()) throw Error(SNOW_E_ARG, "unknown request id");
+    return *reqs_[id];
+  }
+
+  void stats(snow_server_stats* st) const {
+    std::vector<double> lat;
+    for (auto& r : reqs_)
+      if (r->finished >= 0) lat.push_back(r->finished - r->arrival);
+    std::sort(lat.begin(), lat.end());
+    auto pct = [&](double q) {
+      if (lat.empty()) return 0.0;
+      const double pos = q * (lat.size() - 1);
+      const size_t i = (size_t)pos;
+      const double f = pos - i;
+      return i + 1 < lat.size() ? lat[i] * (1 - f) + lat[i + 1] * f : lat[i];
+    };
+    st->completed = (int64_t)lat.size();
+    st->rejected = rejected_;
+    st->peak_scenes = peak_scenes_;
+    st->peak_bytes = peak_bytes_;
+    st->ticks = ticks_;
+    st->particle_steps = particle_steps_;
+    st->wall_s = wall_;
+    st->p50_s = pct(0.50);
+    st->p99_s = pct(0.99);
+    st->mean_s = lat.empty() ? 0.0 : std::accumulate(lat.begin(), lat.end(), 0.0) / lat.size();
+    st->particle_steps_per_s = wall_ > 0 ? particle_steps_ / wall_ : 0.0;
+  }
+
+ private:
+  template <typename Now>
+  void retire(std::vector<Request*>& live, int64_t& used, Now&& now, cudaStream_t s, bool only_zero) {
+    for (size_t i = 0; i < live.size();) {
+      Request* r = live[i];
+      if (r->remaining > 0 || (only_zero && r->steps != 0)) {
+        ++i;
+        continue;
+      }
+      const int64_t n = (int64_t)r->records.size() / 26;
+      batch_.download(r->scene, r->records.data(), n, s);
+      batch_.remove_scene(r->scene);
+      r->finished = now();
+      used -= r->bytes;
+      live.erase(live.begin() + i);
+    }
+  }
+
+  Batch batch_;
+  int prec_;
+  int64_t budget_;
+  int max_scenes_;
+  int64_t max_tick_;
+  std::vector<std::unique_ptr<Request>> reqs_;
+  int64_t rejected_ = 0, peak_scenes_ = 0, peak_bytes_ = 0, ticks_ = 0, particle_steps_ = 0;
+  double wall_ = 0.0;
+};
+
+}  // namespace snow
+
+struct snow_gpu_server {
+  std::unique_ptr<snow::Server> impl;
+};
+
+namespace {
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return SNOW_OK;
+  } catch (const snow::Error& e) {
+    return snow::set_error(e.code, e.what());
+  } catch (const std::exception& e) {
+    return snow::set_error(SNOW_E_ARG, e.what());
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int snow_gpu_server_create(snow_gpu_server** out, int precision, int64_t hbm_budget_bytes, int max_scenes,
+                           int max_steps_per_tick) {
+  return guarded([&] {
+    if (!out || hbm_budget_bytes <= 0 || max_scenes <= 0 || max_steps_per_tick <= 0)
+      throw snow::Error(SNOW_E_ARG, "bad server configuration");
+    auto* s = new snow_gpu_server;
+    try {
+      s->impl = std::make_unique<snow::Server>(precision, hbm_budget_bytes, max_scenes, max_steps_per_tick);
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+  });
+}
+
+int snow_gpu_server_destroy(snow_gpu_server* server) {
+  return guarded([&] {
+    cudaDeviceSynchronize();
+    delete server;
+  });
+}
+
+int snow_gpu_server_submit(snow_gpu_server* server, const double* records, int64_t n,
+                           const snow_step_params* params, const snow_collider* colliders, int n_colliders,
+                           int64_t steps, double arrival_s, int64_t* request_id) {
+  return guarded([&] {
+    if (!server) throw snow::Error(SNOW_E_ARG, "server is NULL");
+    const int64_t id = server->impl->submit(records, n, params, colliders, n_colliders, steps, arrival_s);
+    if (request_id) *request_id = id;
+  });
+}
+
+int snow_gpu_server_run(snow_gpu_server* server, void* stream) {
+  return guarded([&] {
+    if (!server) throw snow::Error(SNOW_E_ARG, "server is NULL");
+    server->impl->run(static_cast<cudaStream_t>(stream));
+  });
+}
+
+int snow_gpu_server_result(snow_gpu_server* server, int64_t request_id, double* records, int64_t n,
+                           double* latency_s) {
+  return guarded([&] {
+    if (!server) throw snow::Error(SNOW_E_ARG, "server is NULL");
+    const auto& r = server->impl->req(request_id);
+    if (r.rejected) throw snow::Error(SNOW_E_CAPACITY, "request was rejected: larger than the memory budget");
+    if (r.finished < 0) throw snow::Error(SNOW_E_STATE, "request has not completed");
+    if (n != (int64_t)r.records.size() / 26) throw snow::Error(SNOW_E_ARG, "particle count differs");
+    std::copy(r.records.begin(), r.records.end(), records);
+    if (latency_s) *latency_s = r.finished - r.arrival;
+  });
+}
+
+int snow_gpu_server_stats(snow_gpu_server* server, snow_server_stats* stats) {
+  return guarded([&] {
+    if (!server || !stats) throw snow::Error(SNOW_E_ARG, "NULL argument");
+    server->impl->stats(stats);
+  });
+}
+
+}  // extern "C"

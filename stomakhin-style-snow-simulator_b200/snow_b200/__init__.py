@@ -62,6 +62,15 @@ class StepTimings(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("completed", "rejected", "peak_scenes", "peak_bytes", "ticks",
+                                               "particle_steps")] + \
+               [(n, ctypes.c_double) for n in ("wall_s", "p50_s", "p99_s", "mean_s", "particle_steps_per_s")]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class SnowError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -102,6 +111,16 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_batch_status": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint32), _i64p, _i64p]),
         "snow_gpu_batch_set_graphs": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_fp64_projections": (i64, [vp]),
+        "snow_gpu_batch_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                   _dp, vp]),
+        "snow_gpu_server_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, i64, ctypes.c_int,
+                                                  ctypes.c_int]),
+        "snow_gpu_server_destroy": (ctypes.c_int, [vp]),
+        "snow_gpu_server_submit": (ctypes.c_int, [vp, _dp, i64, ctypes.POINTER(StepParams),
+                                                  ctypes.POINTER(Collider), ctypes.c_int, i64, d, _i64p]),
+        "snow_gpu_server_run": (ctypes.c_int, [vp, vp]),
+        "snow_gpu_server_result": (ctypes.c_int, [vp, i64, _dp, i64, _dp]),
+        "snow_gpu_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
         "snow_gpu_batch_set_chunk": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_setup": (ctypes.c_int, [_dp, i64, d]),
         "snow_gpu_step": (ctypes.c_int, [_dp, i64, ctypes.POINTER(StepParams), ctypes.POINTER(Collider),
@@ -245,6 +264,13 @@ class Batch:
         """Particles per P2G/G2P work item (power of two, 32..4096)."""
         _check(lib().snow_gpu_batch_set_chunk(self._h, int(chunk)))
 
+    def autotune(self, trial_steps: int = 10, stream: int | None = None) -> tuple[int, float]:
+        """Picks the fastest work-item size on a snapshot of the state; returns (size, ms/step)."""
+        c, ms = ctypes.c_int(), ctypes.c_double()
+        _check(lib().snow_gpu_batch_autotune(self._h, int(trial_steps), ctypes.byref(c), ctypes.byref(ms),
+                                             ctypes.c_void_p(stream)))
+        return c.value, ms.value
+
     @property
     def fp64_projections(self) -> int:
         """Mixed form: projections redone in double during the last step."""
@@ -367,3 +393,49 @@ def stage_position_update(records, dt) -> np.ndarray:
     rec = np.array(records, dtype=np.float64, order="C")
     _check(lib().snow_gpu_stage_position_update(_ptr(rec), rec.shape[0], float(dt)))
     return rec
+
+
+class Server:
+    """Continuous-batching server of independent scenes (snow_gpu_server_*)."""
+
+    def __init__(self, precision: int = SNOW_FP64, budget_bytes: int = 150 * 10**9, max_scenes: int = 4096,
+                 max_steps_per_tick: int = 16):
+        self._h = ctypes.c_void_p()
+        _check(lib().snow_gpu_server_create(ctypes.byref(self._h), precision, int(budget_bytes), int(max_scenes),
+                                            int(max_steps_per_tick)))
+        self.sizes: dict[int, int] = {}
+
+    def close(self) -> None:
+        if self._h:
+            lib().snow_gpu_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, scene, steps: int, arrival_s: float) -> int:
+        rec = _records(scene.particles)
+        prm = StepParams.from_array(scene.params())
+        col = colliders(scene.planes) if len(scene.planes) else (Collider * 1)()
+        rid = ctypes.c_int64()
+        _check(lib().snow_gpu_server_submit(self._h, _ptr(rec), rec.shape[0], ctypes.byref(prm), col,
+                                            len(scene.planes), int(steps), float(arrival_s), ctypes.byref(rid)))
+        self.sizes[rid.value] = rec.shape[0]
+        return rid.value
+
+    def run(self, stream: int | None = None) -> None:
+        _check(lib().snow_gpu_server_run(self._h, ctypes.c_void_p(stream)))
+
+    def result(self, rid: int) -> tuple[np.ndarray, float]:
+        out = np.empty((self.sizes[rid], 26))
+        lat = ctypes.c_double()
+        _check(lib().snow_gpu_server_result(self._h, rid, _ptr(out), out.shape[0], ctypes.byref(lat)))
+        return out, lat.value
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().snow_gpu_server_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()

@@ -193,7 +193,43 @@ def batch_scenes(count: int = 256, lo: int = 1000, hi: int = 64000, seed: int = 
         else:
             rad = (3 * n / (4 * math.pi)) ** (1 / 3) * h
             x, _ = sphere((0.5, 0.3 + rad, 0.5), rad, n, rng)
-            x = x * 0 + x  # keep float64
         out.append(Scene(records(x, np.broadcast_to(vel, x.shape), 400.0 * h ** 3), dx=0.02,
                          dt=dt, steps=steps, material=mat, planes=[GROUND], name=f"batch{s}"))
+    return out
+
+
+def served_requests(count: int = 64, rate: float = 200.0, lo: int = 2000, hi: int = 500_000,
+                    steps_lo: int = 100, steps_hi: int = 2000, seed: int = 4, dt: float = 5e-5):
+    """A Poisson stream of scene requests: (scene, steps, arrival seconds).
+
+    Particle counts are log-uniform in [lo, hi], shapes box / sphere / torus at
+    lattice spacing 0.01 (so the count sets the size), velocity in [-5, 5]^3,
+    material drawn as for the batch scenes, steps uniform in [steps_lo,
+    steps_hi], grid dx = 0.02, ground plane."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for r in range(count):
+        t += rng.exponential(1.0 / rate)
+        n = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        mat = Material(E=float(rng.uniform(4.8e4, 1.4e5)), theta_c=float(rng.uniform(1.9e-2, 2.5e-2)),
+                       theta_s=float(rng.uniform(5e-3, 7.5e-3)), xi=float(rng.uniform(5, 10)))
+        vel = rng.uniform(-5, 5, 3)
+        h = 0.01
+        shape = int(rng.integers(3))
+        if shape == 0:
+            k = max(1, int(round(n ** (1 / 3))))
+            g = np.arange(k) * h
+            x = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+            x = x + np.array([0.5 - k * h / 2, 0.3, 0.5 - k * h / 2]) + rng.uniform(-0.1 * h, 0.1 * h, x.shape)
+        elif shape == 1:
+            rad = (3 * n / (4 * math.pi)) ** (1 / 3) * h
+            x, _ = sphere((0.5, 0.3 + rad, 0.5), rad, n, rng)
+        else:
+            r_minor = (n * h ** 3 / (2 * math.pi ** 2 * 2.5)) ** (1 / 3)  # R = 2.5 r
+            x, _ = torus((0.5, 0.3 + r_minor, 0.5), 2.5 * r_minor, r_minor, n, rng, axis=1)
+        steps = int(rng.integers(steps_lo, steps_hi + 1))
+        sc = Scene(records(x, np.broadcast_to(vel, x.shape), 400.0 * h ** 3), dx=0.02, dt=dt, steps=steps,
+                   material=mat, planes=[GROUND], name=f"request{r}")
+        out.append((sc, steps, t))
     return out

@@ -1,0 +1,90 @@
+"""Continuous-batching server and the work-item autotuner on the GPU.
+
+The server admits requests as they arrive while memory and slots allow and
+advances all admitted scenes together; each scene's result must be the one it
+gets alone (FP64: 1e-12 relative, only atomic order differs; mixed: 1e-5).
+The autotuner must leave the simulation state as it found it.
+"""
+import numpy as np
+import pytest
+
+from oracle_lib import errors
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(n=6, seed=21):
+    from snow_b200 import scenes
+
+    reqs = scenes.served_requests(count=n, rate=2000.0, lo=300, hi=4000, steps_lo=5, steps_hi=37, seed=seed)
+    return reqs
+
+
+def _alone(snow, prec, sc, steps):
+    b = snow.Batch(prec)
+    sid = b.add(sc)
+    b.setup(sid, sc.dx)
+    b.step(steps)
+    out = b.download(sid)
+    b.close()
+    return out
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 1e-5)])
+def test_served_results_match_alone(snow, prec, tol):
+    reqs = _requests()
+    srv = snow.Server(prec, max_steps_per_tick=8)
+    ids = [srv.submit(sc, steps, t) for sc, steps, t in reqs]
+    srv.run()
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["rejected"] == 0
+    assert st["particle_steps"] == sum(sc.n * steps for sc, steps, _ in reqs)
+    assert 0 < st["p50_s"] <= st["p99_s"]
+    assert st["peak_scenes"] >= 2, "requests should overlap on the device"
+    for rid, (sc, steps, _) in zip(ids, reqs):
+        got, lat = srv.result(rid)
+        assert lat > 0
+        e = errors(got, _alone(snow, prec, sc, steps))
+        assert max(e.values()) < tol, (sc.name, e)
+    srv.close()
+
+
+def test_budget_defers_and_rejects(snow):
+    from snow_b200 import scenes
+
+    reqs = _requests(4, seed=5)
+    small = max(r[0].n for r in reqs)
+    # room for about two of these scenes at a time; one request far too large
+    srv = snow.Server(0, budget_bytes=int(2.5 * 900 * small + 2 * 70000), max_scenes=2, max_steps_per_tick=4)
+    ids = [srv.submit(sc, steps, t) for sc, steps, t in reqs]
+    big = scenes.cube_scene(40)
+    big_id = srv.submit(big, 3, 0.0)
+    srv.run()
+    st = srv.stats()
+    assert st["rejected"] == 1 and st["completed"] == len(reqs)
+    assert st["peak_scenes"] <= 2
+    with pytest.raises(snow.SnowError):
+        srv.result(big_id)
+    for rid, (sc, steps, _) in zip(ids, reqs):
+        got, _ = srv.result(rid)
+        assert max(errors(got, _alone(snow, 0, sc, steps)).values()) < 1e-12
+    srv.close()
+
+
+def test_autotune_restores_state(snow):
+    from snow_b200 import scenes
+
+    scs = scenes.batch_scenes(count=4, lo=500, hi=5000, seed=8)
+    recs = [snow.setup(s.particles.copy(), s.dx) for s in scs]
+    ref = snow.Batch(snow.SNOW_FP64)
+    tuned = snow.Batch(snow.SNOW_FP64)
+    rid = [ref.add_scene(r, s.params(), s.planes) for r, s in zip(recs, scs)]
+    tid = [tuned.add_scene(r, s.params(), s.planes) for r, s in zip(recs, scs)]
+    ref.step(3)
+    tuned.step(3)
+    chunk, ms = tuned.autotune(trial_steps=3)
+    assert chunk in (64, 128, 256, 512, 1024) and ms > 0
+    ref.step(4)
+    tuned.step(4)
+    for a, b in zip(rid, tid):
+        assert max(errors(tuned.download(b), ref.download(a)).values()) < 1e-12
