@@ -37,7 +37,6 @@ sys.path.insert(0, PKG)
 
 import numpy as np  # noqa: E402
 
-KERNELS_PER_STEP = 20  # keyspace, keys, 4 x 3 sort passes, 2 block builds, items, p2g, grid, g2p, finish
 REF_SAMPLE_S = 20.0    # target seconds of reference CPU work per bounded sample
 
 
@@ -391,6 +390,7 @@ def run_ours(args, ws, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     status, blocks, cap = batch.status()
+    launches = batch.graph_kernels() * args.steps  # kernel nodes of the replayed step graph
 
     # per-kernel times over K eagerly launched steps (events around each kernel)
     kt = batch.step(args.steps, timings=True, stream=sp)
@@ -453,7 +453,7 @@ def run_ours(args, ws, rank, local):
         "stages_ms_per_step": per,
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "gpu_launches": launches,
         "clocks": clk,
         "grid_blocks": {"used": blocks, "capacity": cap},
         "status": status,

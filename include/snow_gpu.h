@@ -149,8 +149,16 @@ int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable);
  * last step (a singular value within 1e-5 of a clamp bound, or a clamp acting
  * with two singular values within 1e-5 of each other).  0 for an FP64 batch. */
 int64_t snow_gpu_batch_fp64_projections(snow_gpu_batch* batch);
-/* Particles per P2G/G2P work item (power of two in [32, 4096]; default 256). */
+/* Particles per P2G/G2P work item (power of two in [32, 1024]; default 256). */
 int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk);
+/* Particle ordering: 1 (default) a counting sort over dense per-cell key bins
+ * with direct block lookup, used while the scenes' key boxes need at most
+ * 2^26 bins; 0 the radix sort with the block hash table.  Both give the same
+ * step up to the order of floating-point sums.  No reference counterpart. */
+int snow_gpu_batch_set_dense(snow_gpu_batch* batch, int enable);
+/* Kernels launched by one replay of the batch's captured step graph (0 until
+ * a multi-step call captured it).  No reference counterpart. */
+int snow_gpu_batch_graph_kernels(snow_gpu_batch* batch);
 
 /* Autotuner: times `trial_steps` steps of the batch for each work-item size
  * (particles per P2G/G2P CTA work item: 64 ... 1024) on a snapshot of the

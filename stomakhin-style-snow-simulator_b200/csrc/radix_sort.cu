@@ -1,6 +1,6 @@
-// Stable LSD radix sort of the batch's (key, particle index) pairs, 8 bits per
+// Stable LSD radix sort of the batch's (key, particle index) pairs, 9 bits per
 // pass, reduce-then-scan:
-//   upsweep    per 2048-key tile, a 256-bin digit histogram
+//   upsweep    per 2048-key tile, a 512-bin digit histogram
 //   scan       per digit, an exclusive scan over the tiles (digit-major order)
 //   downsweep  per tile, the stable rank of every key among equal digits
 //              (warp match + per-warp counts), then a scatter to
@@ -10,6 +10,7 @@
 // not needed returns at once, so the host launches a fixed 4 passes and the
 // sequence can be captured in a CUDA graph.  Pass p reads buffer p & 1 and
 // writes buffer (p + 1) & 1; the sorted result is in buffer passes & 1.
+// Nine-bit digits sort the 18-bit keys of a 650k-particle scene in two passes.
 #include <cuda_runtime.h>
 
 #include "snow_batch.cuh"
@@ -17,13 +18,15 @@
 namespace snow {
 namespace {
 
-constexpr int kBits = 8;
+constexpr int kBits = kRadixBits;
 constexpr int kDigits = 1 << kBits;
 constexpr int kThreads = 256;
+constexpr int kPerThread = kDigits / kThreads;  // digits owned by each thread
 constexpr int kItems = 8;
 constexpr int kTile = kThreads * kItems;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxPasses = 4;
+constexpr int kMaxPasses = (32 + kBits - 1) / kBits;
+static_assert(kDigits % kThreads == 0, "digits must be a multiple of the block size");
 
 __device__ __forceinline__ bool pass_needed(const BatchDev& b, int pass) {
   return (uint32_t)(pass * kBits) < b.ctr->sort_bits;
@@ -108,12 +111,23 @@ __global__ void __launch_bounds__(kThreads) k_downsweep(const BatchDev b, int pa
   const int shift = pass * kBits;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  {  // digit bases: exclusive scan of digit totals, plus this tile's offset
-    const uint32_t tot = b.digit_total[threadIdx.x];
+  {  // digit bases: exclusive scan of digit totals (thread t owns digits t*kPerThread...),
+     // plus this tile's offset within each digit
+    uint32_t tot[kPerThread], sum = 0;
+#pragma unroll
+    for (int q = 0; q < kPerThread; ++q) {
+      tot[q] = b.digit_total[threadIdx.x * kPerThread + q];
+      sum += tot[q];
+    }
     uint32_t all;
-    const uint32_t ex = block_exclusive_scan(tot, all, s_warp);
-    s_off[threadIdx.x] = ex + b.hist[(int64_t)threadIdx.x * b.ntiles + blockIdx.x];
-    s_run[threadIdx.x] = 0;
+    uint32_t ex = block_exclusive_scan(sum, all, s_warp);
+#pragma unroll
+    for (int q = 0; q < kPerThread; ++q) {
+      const int d = threadIdx.x * kPerThread + q;
+      s_off[d] = ex + b.hist[(int64_t)d * b.ntiles + blockIdx.x];
+      s_run[d] = 0;
+      ex += tot[q];
+    }
   }
   const int64_t base = (int64_t)blockIdx.x * kTile;
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -132,8 +146,9 @@ __global__ void __launch_bounds__(kThreads) k_downsweep(const BatchDev b, int pa
     const uint32_t rank = __popc(peers & lt_mask);
     if (valid && rank == 0) s_cnt[warp][d] = __popc(peers);
     __syncthreads();
-    {  // per digit: prefix over warps, continuing from earlier rounds
-      const int dd = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < kPerThread; ++q) {  // per digit: prefix over warps, continuing from earlier rounds
+      const int dd = threadIdx.x * kPerThread + q;
       uint32_t run = s_run[dd];
 #pragma unroll
       for (int w = 0; w < kWarps; ++w) {
@@ -156,7 +171,7 @@ __global__ void __launch_bounds__(kThreads) k_downsweep(const BatchDev b, int pa
 }  // namespace
 
 void radix_sort(const BatchDev& b, cudaStream_t s) {
-  if (b.total <= 0) return;
+  if (b.total <= 0 || b.dense) return;  // dense bins: counting sort in StepLaunch::blocks
   for (int pass = 0; pass < kMaxPasses; ++pass) {
     k_upsweep<<<b.ntiles, kThreads, 0, s>>>(b, pass);
     k_scan<<<kDigits, kThreads, 0, s>>>(b, pass);
@@ -165,5 +180,6 @@ void radix_sort(const BatchDev& b, cudaStream_t s) {
 }
 
 int radix_tiles(int64_t n) { return (int)((n + kTile - 1) / kTile); }
+int radix_digits() { return kDigits; }
 
 }  // namespace snow

@@ -16,13 +16,20 @@
 //   vel  [0..2] velocity after collisions, [3..5] velocity - momentum/mass
 //        (the FLIP increment; 0 at massless nodes)
 // A block is found through an open-addressing hash table keyed by the block's
-// 32-bit "block key" (see below).
+// 32-bit "block key" (see below); a slot holds the key and the block id in one
+// 64-bit word.
 //
 // Sort key of a particle: the block key (the linear index of its block in its
 // scene's bounding box of blocks, offset by the scene's key base) shifted left
 // by 6, plus its cell within the block (cx + 4 cy + 16 cz).  The bounding box
 // (one block of margin on the high side, so the +{0,1}^3 neighbours used by
 // P2G/G2P are addressable) is measured by G2P for the next step.
+//
+// While the key boxes fit the dense bins (the usual case: their size is the
+// boxes' volume in cells), particles are ordered by a counting sort over the
+// keys, and grid block ids are a prefix sum over the block keys whose
+// +{0,1}^3 neighbourhood holds particles, looked up directly by key.  Larger
+// boxes fall back to the radix sort and the block hash table.
 #pragma once
 
 #include <cstdint>
@@ -44,9 +51,11 @@ constexpr int kFPPlanes = 9;
 // PFM: the force matrix -V_p0 P F_E^T of the particle's current state (symmetric:
 // xx, yy, zz, xy, xz, yz), written by G2P for the next step's P2G.
 enum : int { PX = 0, PV = 3, PM = 6, PVOL = 7, PFE = 8, PFM = 17 };
+constexpr int kRadixBits = 9;  // sort digit width (radix_sort.cu)
 constexpr int kAccCh = 7;
 constexpr int kVelCh = 6;
-constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
+constexpr unsigned long long kEmptyEntry = ~0ull;
+constexpr int kBinTile = 4096;  // keys per tile of the dense-bin scan (64 blocks)
 
 // Status bits reported back to the host (snow_gpu_status).
 enum : uint32_t {
@@ -56,6 +65,8 @@ enum : uint32_t {
   ST_NONFINITE = 1u << 3,        // a particle position became NaN/Inf
   ST_OUT_OF_BOX = 1u << 4,       // a particle fell outside its scene's key box
   ST_LOOKUP_MISS = 1u << 5,      // a block expected in the table was not found
+  ST_BIN_OVERFLOW = 1u << 6,     // key boxes larger than the dense bins
+  ST_SCAN_STALL = 1u << 7,       // a bin-scan tile waited too long for its predecessor
 };
 
 struct SceneDev {
@@ -79,13 +90,14 @@ struct SceneDev {
 };
 
 struct Counters {
-  uint32_t n_pblocks;   // blocks holding particles
-  uint32_t n_halo;      // neighbour-only blocks
+  uint32_t n_blocks;    // grid blocks
+  uint32_t key_blocks;  // block keys over all scenes' key boxes this step
   uint32_t sort_bits;   // significant key bits this step
   uint32_t work_p2g, work_grid, work_g2p, work_aux;
   uint32_t status;
   uint32_t n_items;     // (block, chunk) work items of the particle kernels
   uint32_t fp64_projections;  // mixed form: plastic projections redone in double
+  uint32_t bin_ticket;  // next tile of the dense-bin scan
 };
 
 struct BatchDev {
@@ -99,21 +111,30 @@ struct BatchDev {
   uint32_t* hist;
   uint32_t* digit_total;
   int32_t ntiles;
-  // blocks
-  uint32_t* hkeys;
-  int32_t* hvals;
+  // dense key bins (counting sort by key, used when `dense` is set; otherwise
+  // the radix sort and the block hash table): per key (block key << 6 | cell)
+  // a particle count (zero between steps) and the first sorted position, and
+  // per block key an occupancy byte (zero between steps) and the grid block id
+  int32_t dense;
+  int64_t cap_bins;         // keys (a multiple of kBinTile)
+  uint32_t* bins;
+  uint32_t* bin_off;
+  uint8_t* occ;
+  int32_t* idmap;
+  unsigned long long* bin_state;  // chained-scan state of each bin tile
+  // blocks: hash table of (block key << 32) | block id, empty slots all ones
+  unsigned long long* htab;
   uint32_t hmask;
   int32_t cap_blocks;
   int4* blk;                // (bx, by, bz, scene)
-  uint32_t* blk_key;
-  int32_t* pblk_start;
-  int32_t* pblk_end;
-  // work items of P2G/G2P: (particle block, chunk), chunk = `chunk` consecutive
-  // particles of the block's sorted run, so that large blocks spread over CTAs
-  int2* items;
-  BlockHeader* item_hdr;  // resolved header per item (k_items)
+  // work items of P2G/G2P: runs of at most `chunk` consecutive sorted particles
+  // of one block, so that large blocks spread over CTAs
+  BlockHeader* item_hdr;
   int32_t cap_items;
   int32_t chunk;
+  // mixed form: (scene, output slot, input index) of projections to redo in double
+  int4* fixups;
+  int64_t cap_fixups;
   // grid
   void* acc;                // R[kAccCh][cap_blocks * 64]
   void* vel;                // R[kVelCh][cap_blocks * 64]
@@ -140,9 +161,12 @@ SNOW_HD uint32_t block_key(const SceneDev& s, int bx, int by, int bz) {
 __device__ __forceinline__ int32_t hash_find(const BatchDev& b, uint32_t key) {
   uint32_t slot = hash32(key) & b.hmask;
   for (uint32_t probe = 0; probe <= b.hmask; ++probe) {
-    const uint32_t k = b.hkeys[slot];
-    if (k == key) return b.hvals[slot];
-    if (k == kEmptyKey) return -1;
+    const unsigned long long e = b.htab[slot];
+    if (e == kEmptyEntry) return -1;
+    if ((uint32_t)(e >> 32) == key) {
+      const uint32_t id = (uint32_t)e;
+      return id < (uint32_t)b.cap_blocks ? (int32_t)id : -1;
+    }
     slot = (slot + 1) & b.hmask;
   }
   return -1;
@@ -172,6 +196,7 @@ struct StepLaunch {
   static void finish(const BatchDev& b, cudaStream_t s);
   static void bbox_init(const BatchDev& b, cudaStream_t s);
   static void prepare_force(const BatchDev& b, cudaStream_t s);
+  static void fixup(const BatchDev& b, cudaStream_t s);
 };
 
 enum P2GMode : int { P2G_FULL = 0, P2G_MASS = 1, P2G_MASS_MOMENTUM = 2, P2G_FORCE = 3, P2G_PRE = 4 };

@@ -100,6 +100,7 @@ Batch::~Batch() {
   if (h_ctr_) cudaFreeHost(h_ctr_);
   free_particle_buffers();
   free_grid();
+  free_bins();
   dfree(staging_);
   dfree(d_tmp_scene_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
@@ -119,20 +120,55 @@ void Batch::free_particle_buffers() {
     dfree(vals_[k]);
   }
   dfree(hist_);
+  dfree(fixups_);
   dfree(digit_total_);
   cap_p_ = 0;
 }
 
+void Batch::free_bins() {
+  dfree(bins_);
+  dfree(bin_off_);
+  dfree(occ_);
+  dfree(idmap_);
+  dfree(bin_state_);
+  cap_bins_ = 0;
+}
+
+// Dense key bins for key boxes of up to `bins` cells (rounded up to whole
+// scan tiles).  Counts and occupancy start at zero; every step leaves them so.
+void Batch::ensure_bins(int64_t bins) {
+  bins = (bins + kBinTile - 1) / kBinTile * kBinTile;
+  if (bins <= cap_bins_) return;
+  free_bins();
+  bins_ = dalloc<uint32_t>((size_t)bins);
+  bin_off_ = dalloc<uint32_t>((size_t)bins);
+  occ_ = dalloc<uint8_t>((size_t)(bins / 64));
+  idmap_ = dalloc<int32_t>((size_t)(bins / 64));
+  bin_state_ = dalloc<unsigned long long>((size_t)(bins / kBinTile + 1));
+  cap_bins_ = bins;
+  bins_dirty_ = true;
+}
+
+// Chooses the sort for the coming steps: dense bins with 2x headroom over
+// `key_blocks` block keys when that fits kMaxDenseBins, else the radix sort.
+// Clears the counts if a step may have left some behind.
+void Batch::size_dense(int64_t key_blocks, cudaStream_t s) {
+  const int64_t need = 2 * key_blocks * 64 + 16 * kBinTile;
+  dense_ = want_dense_ && need <= kMaxDenseBins;
+  if (!dense_) return;
+  ensure_bins(need);
+  if (bins_dirty_) {
+    check_cuda(cudaMemsetAsync(bins_, 0, (size_t)cap_bins_ * sizeof(uint32_t), s), "clear bins");
+    check_cuda(cudaMemsetAsync(occ_, 0, (size_t)(cap_bins_ / 64), s), "clear bins");
+    bins_dirty_ = false;
+  }
+}
+
 void Batch::free_grid() {
-  dfree(hkeys_);
-  dfree(hvals_);
+  dfree(htab_);
   dfree(blk_);
-  dfree(blk_key_);
-  dfree(pblk_start_);
-  dfree(pblk_end_);
   dfree(acc_);
   dfree(vel_);
-  dfree(items_);
   dfree(item_hdr_);
   cap_items_ = 0;
   cap_blocks_ = 0;
@@ -305,18 +341,18 @@ void Batch::ensure_particle_buffers(int64_t total) {
     vals_[k] = dalloc<uint32_t>((size_t)cap);
   }
   ntiles_cap_ = radix_tiles(cap);
-  hist_ = dalloc<uint32_t>((size_t)ntiles_cap_ * 256);
-  digit_total_ = dalloc<uint32_t>(256);
+  hist_ = dalloc<uint32_t>((size_t)ntiles_cap_ * (1 << kRadixBits));
+  if (prec_ == SNOW_MIXED) fixups_ = dalloc<int4>((size_t)cap);
+  digit_total_ = dalloc<uint32_t>(1 << kRadixBits);
   cap_p_ = cap;
 }
 
-// Work items: at most one partial chunk per particle block beyond total / chunk.
+// Work items: one per chunk of the sorted particles, plus one more for every
+// block run that starts inside a chunk.
 void Batch::ensure_items() {
   const int64_t need = cap_p_ / chunk_ + cap_blocks_ + 64;
   if (need <= cap_items_) return;
-  dfree(items_);
   dfree(item_hdr_);
-  items_ = dalloc<int2>((size_t)need);
   item_hdr_ = dalloc<BlockHeader>((size_t)need);
   cap_items_ = (int32_t)need;
 }
@@ -332,12 +368,8 @@ void Batch::ensure_grid(int64_t blocks) {
   uint32_t h = 1;
   while (h < 2 * (uint64_t)cap) h <<= 1;
   hcap_ = h;
-  hkeys_ = dalloc<uint32_t>(h);
-  hvals_ = dalloc<int32_t>(h);
+  htab_ = dalloc<unsigned long long>(h);
   blk_ = dalloc<int4>((size_t)cap);
-  blk_key_ = dalloc<uint32_t>((size_t)cap);
-  pblk_start_ = dalloc<int32_t>((size_t)cap);
-  pblk_end_ = dalloc<int32_t>((size_t)cap);
   acc_ = dalloc<unsigned char>((size_t)cap * 64 * kAccCh * rsize_);
   vel_ = dalloc<unsigned char>((size_t)cap * 64 * kVelCh * rsize_);
   check_cuda(cudaMemset(acc_, 0, (size_t)cap * 64 * kAccCh * rsize_), "cudaMemset");
@@ -358,21 +390,25 @@ BatchDev Batch::dev(SceneDev* scenes, int num_scenes, int64_t total) const {
   b.hist = hist_;
   b.digit_total = digit_total_;
   b.ntiles = radix_tiles(std::max<int64_t>(total, 1));
-  b.hkeys = hkeys_;
-  b.hvals = hvals_;
+  b.htab = htab_;
   b.hmask = hcap_ - 1;
   b.cap_blocks = cap_blocks_;
   b.blk = blk_;
-  b.blk_key = blk_key_;
-  b.pblk_start = pblk_start_;
-  b.pblk_end = pblk_end_;
-  b.items = items_;
   b.item_hdr = item_hdr_;
   b.cap_items = cap_items_;
   b.chunk = chunk_;
+  b.fixups = fixups_;
+  b.cap_fixups = fixups_ ? cap_p_ : 0;
   b.acc = acc_;
   b.vel = vel_;
   b.ctr = d_ctr_;
+  b.dense = dense_ ? 1 : 0;
+  b.cap_bins = cap_bins_;
+  b.bins = bins_;
+  b.bin_off = bin_off_;
+  b.occ = occ_;
+  b.idmap = idmap_;
+  b.bin_state = bin_state_;
   return b;
 }
 
@@ -435,6 +471,7 @@ void Batch::prepare(cudaStream_t s) {
   }
   const int64_t want = std::max<int64_t>(2 * vol + 1024, 2 * last_blocks_ + 1024);
   ensure_grid(std::min<int64_t>(want, std::max<int64_t>(8 * total_ + 64, 1024)));
+  size_dense(std::max<int64_t>(vol, last_key_blocks_), s);
   num_dev_scenes_ = (int)table_.size();
   dirty_ = boxes_dirty_ = params_dirty_ = false;
 }
@@ -455,6 +492,7 @@ void Batch::launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev) {
   StepLaunch<R>::grid_update(b, s);
   mark(3);
   StepLaunch<R>::g2p(b, G2P_FULL, s);
+  StepLaunch<R>::fixup(b, s);
   StepLaunch<R>::finish(b, s);
   mark(4);
 }
@@ -510,6 +548,18 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
         check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
         one(nullptr);
         check_cuda(cudaStreamEndCapture(s, &g), "capture end");
+        {
+          size_t nodes = 0;
+          check_cuda(cudaGraphGetNodes(g, nullptr, &nodes), "graph nodes");
+          std::vector<cudaGraphNode_t> list(nodes);
+          check_cuda(cudaGraphGetNodes(g, list.data(), &nodes), "graph nodes");
+          graph_kernels_ = 0;
+          for (cudaGraphNode_t nd : list) {
+            cudaGraphNodeType type;
+            check_cuda(cudaGraphNodeGetType(nd, &type), "graph node type");
+            if (type == cudaGraphNodeTypeKernel) ++graph_kernels_;
+          }
+        }
         check_cuda(cudaGraphInstantiate(&gexec_, g, 0), "graph instantiate");
         cudaGraphDestroy(g);
         graph_args_ = b;
@@ -524,16 +574,25 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
   check_cuda(cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, s), "status");
   check_cuda(cudaStreamSynchronize(s), "step");
   last_status_ = h_ctr_->status;
-  last_blocks_ = (int64_t)h_ctr_->n_pblocks + h_ctr_->n_halo;
-  check_status();
-  // Keep 2x headroom: grow the grid before the next call if the last step came close.
+  last_blocks_ = (int64_t)h_ctr_->n_blocks;
+  last_key_blocks_ = (int64_t)h_ctr_->key_blocks;
+  // Keep 2x headroom: grow the grid and the bins before the next call if the
+  // last step came close.
   if (last_blocks_ * 2 > cap_blocks_) boxes_dirty_ = true;
+  if (dense_ && last_key_blocks_ * 64 * 2 > cap_bins_) boxes_dirty_ = true;
+  check_status();
 }
 
 void Batch::check_status() {
   const uint32_t st = last_status_;
   if (!st) return;
   cudaMemset(&d_ctr_->status, 0, sizeof(uint32_t));
+  bins_dirty_ = true;  // a step that stopped early may leave counts behind
+  boxes_dirty_ = true;
+  if (st & ST_BIN_OVERFLOW)
+    throw Error(SNOW_E_CAPACITY, "scene key boxes outgrew the dense bins (" + std::to_string(cap_bins_) +
+                                     "); the step result is not valid");
+  if (st & ST_SCAN_STALL) throw Error(SNOW_E_STATE, "bin scan stalled; the step result is not valid");
   if (st & (ST_BLOCK_OVERFLOW | ST_HASH_FULL))
     throw Error(SNOW_E_CAPACITY, "grid block capacity exceeded (" + std::to_string(cap_blocks_) +
                                      " blocks); the step result is not valid");
@@ -566,6 +625,7 @@ void Batch::setup(int32_t id, double dx, cudaStream_t s) {
     int64_t vol = 1;
     for (int a = 0; a < 3; ++a) vol *= (int64_t)(d.nb_hi[a] - d.nb_lo[a] + 4);
     ensure_grid(std::min<int64_t>(vol + 1024, 8 * sc->n + 1024));
+    size_dense(vol, s);
   }
   const BatchDev b = dev(d_tmp_scene_, 1, sc->n);
   auto run = [&](auto tag) {
@@ -661,8 +721,11 @@ int Batch::autotune(int trial_steps, double* best_ms, cudaStream_t s) {
 int64_t Batch::device_bytes() const {
   int64_t b = 0;
   for (auto& sc : scenes_) b += 2 * sc->stride * (kRealPlanes * (int64_t)rsize_ + kFPPlanes * 8 + 4);
-  b += cap_p_ * 16 + (int64_t)ntiles_cap_ * 256 * 4;
-  b += (int64_t)cap_blocks_ * (64 * (kAccCh + kVelCh) * (int64_t)rsize_ + 16 + 12) + (int64_t)hcap_ * 8;
+  b += cap_p_ * 16 + (int64_t)ntiles_cap_ * (1 << kRadixBits) * 4;
+  if (prec_ == SNOW_MIXED) b += cap_p_ * (int64_t)sizeof(int4);
+  b += (int64_t)cap_blocks_ * (64 * (kAccCh + kVelCh) * (int64_t)rsize_ + 16) + (int64_t)hcap_ * 8;
+  b += (int64_t)cap_items_ * (int64_t)sizeof(BlockHeader);
+  b += cap_bins_ * 8 + cap_bins_ / 64 * 5 + (cap_bins_ / kBinTile + 1) * 8;
   b += staging_cap_ * 208;
   return b;
 }
@@ -826,6 +889,15 @@ int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk) {
   return guarded([&] {
     SNOW_BATCH_OR_FAIL;
     batch->impl->set_chunk(chunk);
+  });
+}
+int snow_gpu_batch_graph_kernels(snow_gpu_batch* batch) {
+  return batch && batch->impl ? batch->impl->graph_kernels() : SNOW_E_ARG;
+}
+int snow_gpu_batch_set_dense(snow_gpu_batch* batch, int enable) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->set_dense(enable != 0);
   });
 }
 int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable) {

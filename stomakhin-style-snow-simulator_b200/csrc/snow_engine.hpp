@@ -65,9 +65,9 @@ class Batch {
   int64_t last_blocks() const { return last_blocks_; }
   int64_t last_fp64_projections() const { return prec_ == SNOW_MIXED ? (int64_t)h_ctr_->fp64_projections : 0; }
   int64_t capacity_blocks() const { return cap_blocks_; }
-  // Particles per P2G/G2P work item (a power of two, 32..4096).
+  // Particles per P2G/G2P work item (a power of two, 32..1024).
   void set_chunk(int chunk) {
-    if (chunk < 32 || chunk > 4096 || (chunk & (chunk - 1))) throw Error(SNOW_E_ARG, "chunk must be a power of two in [32, 4096]");
+    if (chunk < 32 || chunk > 1024 || (chunk & (chunk - 1))) throw Error(SNOW_E_ARG, "chunk must be a power of two in [32, 1024]");
     chunk_ = chunk;
     cap_items_ = 0;  // re-sized on the next prepare
     boxes_dirty_ = true;
@@ -76,6 +76,17 @@ class Batch {
     use_graphs_ = on;
     drop_graph();
   }
+  // Counting sort over dense key bins (default) or the radix sort with the
+  // block hash table; the latter is also taken when the key boxes would need
+  // more than kMaxDenseBins bins.
+  void set_dense(bool on) {
+    want_dense_ = on;
+    boxes_dirty_ = true;
+  }
+  bool dense() const { return dense_; }
+  // Kernel launches in one replay of the captured step graph (0 before capture).
+  int graph_kernels() const { return graph_kernels_; }
+  static constexpr int64_t kMaxDenseBins = int64_t(1) << 26;
   int64_t device_bytes() const;
   int precision() const { return prec_; }
   Scene* find(int32_t id);
@@ -100,6 +111,9 @@ class Batch {
   void ensure_particle_buffers(int64_t total);
   void ensure_grid(int64_t blocks);
   void ensure_items();
+  void ensure_bins(int64_t bins);
+  void free_bins();
+  void size_dense(int64_t key_blocks, cudaStream_t s);
   void set_colliders(Scene& sc, const snow_collider* c, int n);
   SceneDev scene_dev(const Scene& sc, int64_t begin) const;
   template <typename R>
@@ -126,21 +140,26 @@ class Batch {
   uint32_t* keys_[2] = {nullptr, nullptr};
   uint32_t* vals_[2] = {nullptr, nullptr};
   uint32_t* hist_ = nullptr;
+  int4* fixups_ = nullptr;
   uint32_t* digit_total_ = nullptr;
+  uint32_t* bins_ = nullptr;
+  uint32_t* bin_off_ = nullptr;
+  uint8_t* occ_ = nullptr;
+  int32_t* idmap_ = nullptr;
+  unsigned long long* bin_state_ = nullptr;
+  int64_t cap_bins_ = 0;
+  bool want_dense_ = true, dense_ = false, bins_dirty_ = false;
+  int64_t last_key_blocks_ = 0;
+  int graph_kernels_ = 0;
   int64_t cap_p_ = 0;
   int ntiles_cap_ = 0;
 
-  uint32_t* hkeys_ = nullptr;
-  int32_t* hvals_ = nullptr;
+  unsigned long long* htab_ = nullptr;
   uint32_t hcap_ = 0;
   int32_t cap_blocks_ = 0;
   int4* blk_ = nullptr;
-  uint32_t* blk_key_ = nullptr;
-  int32_t* pblk_start_ = nullptr;
-  int32_t* pblk_end_ = nullptr;
   void* acc_ = nullptr;
   void* vel_ = nullptr;
-  int2* items_ = nullptr;
   BlockHeader* item_hdr_ = nullptr;
   int32_t cap_items_ = 0;
   int32_t chunk_ = 256;

@@ -2,11 +2,15 @@
 //
 //   keyspace     (1 block)  per-scene key boxes and key bases, sort bit count,
 //                            counter resets
-//   keys         (1/particle) block key + cell of every particle
-//   radix_sort   (radix_sort.cu) stable sort of (key, particle) pairs
-//   blocks_a     (1/particle) one grid block per run of equal block keys,
-//                            inserted into the block hash table
-//   blocks_b     (8/block)   the +{0,1}^3 neighbour blocks the stencils reach
+//   keys         (1/particle) block key + cell of every particle; with dense
+//                            bins, per-key counts (warp-aggregated atomics)
+//   bins         (persistent, chained scan over the key bins)
+//                            sorted offsets per key, grid block ids per block
+//                            key (prefix over keys whose -{0,1}^3 neighbours
+//                            hold particles), work items per particle run
+//   scatter      (1/particle) counting-sort scatter; work items' neighbour ids
+//   (fallback for key boxes beyond the dense bins: radix_sort.cu, then
+//    blocks: one pass building the block hash table and the work items)
 //   p2g          (persistent, 1 CTA per particle block)
 //                            stencil weights, hardening, stress, and the
 //                            scatter of mass, momentum and force into a shared
@@ -27,6 +31,7 @@
 // position_update = g2p.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <type_traits>
@@ -39,15 +44,27 @@ int radix_tiles(int64_t n);
 
 namespace {
 
+template <typename R>
+struct Vec;
+template <>
+struct Vec<float> {
+  using two = float2;
+};
+template <>
+struct Vec<double> {
+  using two = double2;
+};
+
 constexpr int kTileN = 544;  // 8 x 8 x 8 node tile, z stride padded to 68
 SNOW_HD int tile_index(int x, int y, int z) { return x + 8 * y + 68 * z; }
 
 __device__ __forceinline__ const uint32_t* sorted_keys(const BatchDev& b) {
-  const uint32_t passes = (b.ctr->sort_bits + 7) / 8;
+  const uint32_t passes = (b.ctr->sort_bits + kRadixBits - 1) / kRadixBits;
   return b.keys[passes & 1];
 }
 __device__ __forceinline__ const uint32_t* sorted_vals(const BatchDev& b) {
-  const uint32_t passes = (b.ctr->sort_bits + 7) / 8;
+  if (b.dense) return b.vals[1];
+  const uint32_t passes = (b.ctr->sort_bits + kRadixBits - 1) / kRadixBits;
   return b.vals[passes & 1];
 }
 __device__ __forceinline__ void flag(const BatchDev& b, uint32_t bit) { atomicOr(&b.ctr->status, bit); }
@@ -134,7 +151,12 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
         sc.dim[a] = empty ? 0 : (hi - lo + 2);  // +1 block of margin for the neighbours
       }
       if (empty) {
-        for (int a = 0; a < 3; ++a) sc.dim[a] = 0;
+        // no finite position (or no particles): a one-block box keeps the keys
+        // of any particles inside this scene's key range
+        for (int a = 0; a < 3; ++a) {
+          sc.lo[a] = 0;
+          sc.dim[a] = sc.n > 0 ? 2 : 0;
+        }
       }
       cnt = (unsigned long long)sc.dim[0] * sc.dim[1] * sc.dim[2];
       for (int a = 0; a < 3; ++a) {
@@ -177,8 +199,10 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
     }
     Counters* c = b.ctr;
     c->sort_bits = bits;
-    c->n_pblocks = 0;
-    c->n_halo = 0;
+    c->key_blocks = (uint32_t)min(total, (unsigned long long)UINT32_MAX);
+    if (b.dense && total * 64 > (unsigned long long)b.cap_bins) atomicOr(&c->status, ST_BIN_OVERFLOW);
+    c->bin_ticket = 0;
+    c->n_blocks = 0;
     c->work_p2g = c->work_grid = c->work_g2p = c->work_aux = 0;
     c->n_items = 0;
     c->fp64_projections = 0;
@@ -186,52 +210,355 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
 }
 
 // ---------------------------------------------------------------------- keys
+// Dense bins hold every key of this step's key boxes.
+__device__ __forceinline__ bool bins_fit(const BatchDev& b) {
+  return (int64_t)b.ctr->key_blocks * 64 <= b.cap_bins;
+}
+
+// Sort key of every particle (and its index within its scene).  With dense
+// bins, also the per-key particle counts (one atomic per run of equal keys in
+// a warp: the particles arrive nearly sorted from the previous step) and the
+// occupancy of each block key; the tile states of the bin scan are cleared.
 template <typename R>
 __global__ void __launch_bounds__(256) k_keys(const BatchDev b) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= b.total) return;
-  const int s = scene_of(b, t);
-  const SceneDev& sc = b.scenes[s];
-  const R* r = (const R*)sc.r[sc.cur];
-  const int64_t i = t - sc.begin;
-  const R dx = (R)sc.dx;
-  int blk[3], cell[3];
-  bool ok = true;
-  for (int a = 0; a < 3; ++a) {
-    const R x = r[(PX + a) * sc.stride + i];
-    if (!isfinite((double)x)) {
-      ok = false;
-      blk[a] = sc.lo[a];
-      cell[a] = 0;
-      continue;
-    }
-    blk[a] = block_coord(x, dx, cell[a]);
-    if (blk[a] < sc.lo[a] || blk[a] > sc.lo[a] + sc.dim[a] - 2) {
-      ok = false;
-      blk[a] = sc.lo[a];
-    }
+  const bool dense = b.dense && bins_fit(b);
+  if (dense) {
+    const int64_t ntiles = ((int64_t)b.ctr->key_blocks * 64 + kBinTile - 1) / kBinTile;
+    for (int64_t j = t; j < ntiles; j += (int64_t)gridDim.x * blockDim.x) b.bin_state[j] = 0;
   }
-  if (!ok) flag(b, ST_OUT_OF_BOX);
-  const uint32_t bk = block_key(sc, blk[0], blk[1], blk[2]);
-  b.keys[0][t] = (bk << 6) | (uint32_t)(cell[0] + 4 * cell[1] + 16 * cell[2]);
-  b.vals[0][t] = (uint32_t)i;
+  const bool valid = t < b.total;
+  uint32_t key = 0xFFFFFFFFu;
+  if (valid) {
+    const int s = scene_of(b, t);
+    const SceneDev& sc = b.scenes[s];
+    const R* r = (const R*)sc.r[sc.cur];
+    const int64_t i = t - sc.begin;
+    const R dx = (R)sc.dx;
+    int blk[3], cell[3];
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+      const R x = r[(PX + a) * sc.stride + i];
+      if (!isfinite((double)x)) {
+        ok = false;
+        blk[a] = sc.lo[a];
+        cell[a] = 0;
+        continue;
+      }
+      blk[a] = block_coord(x, dx, cell[a]);
+      if (blk[a] < sc.lo[a] || blk[a] > sc.lo[a] + sc.dim[a] - 2) {
+        ok = false;
+        blk[a] = sc.lo[a];
+      }
+    }
+    if (!ok) flag(b, ST_OUT_OF_BOX);
+    const uint32_t bk = block_key(sc, blk[0], blk[1], blk[2]);
+    key = (bk << 6) | (uint32_t)(cell[0] + 4 * cell[1] + 16 * cell[2]);
+    b.keys[0][t] = key;
+    b.vals[0][t] = (uint32_t)i;
+  }
+  if (!dense) return;
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
+  if (valid && (threadIdx.x & 31) == __ffs(peers) - 1) {
+    atomicAdd(&b.bins[key], (uint32_t)__popc(peers));
+    b.occ[key >> 6] = 1;
+  }
+}
+
+// ---------------------------------------------------------------- dense bins
+// Index of the scene whose key range holds block key bk (the last scene with
+// key_base <= bk: scenes with empty boxes share the next scene's base).
+__device__ __forceinline__ int scene_of_key(const BatchDev& b, uint32_t bk) {
+  int lo = 0, hi = b.num_scenes - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (b.scenes[mid].key_base <= bk) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Chained-scan tile state: flag in bits 62-63 (1 aggregate, 2 inclusive
+// prefix), particles in bits 0-35, grid blocks in bits 36-61.
+constexpr unsigned long long kTileAgg = 1ull << 62, kTileIncl = 2ull << 62;
+constexpr unsigned long long kTileVal = (1ull << 62) - 1;
+constexpr int kBlkShift = 36;
+constexpr unsigned long long kPartMask = (1ull << kBlkShift) - 1;
+
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One pass over the dense bins (a chained scan with decoupled look-back; tiles
+// are taken in order from a ticket, so a tile only waits on tiles whose CTAs
+// are already running).  Thread q = 0..3 of each group of four owns 16 cells
+// of one block key.  Per key: the first sorted position (exclusive prefix of
+// the counts), and the counts re-zeroed.  Per block key: whether any of the
+// blocks at -{0,1}^3 holds particles (then it is a grid block, id = prefix of
+// such keys), its coordinates, and the work items of its particle run.
+__global__ void __launch_bounds__(256) k_bins(const BatchDev b) {
+  __shared__ unsigned long long s_warp[8];
+  __shared__ unsigned long long s_prefix;
+  __shared__ uint32_t s_items[8];
+  __shared__ uint32_t s_tile, s_item_base;
+  if (!bins_fit(b)) return;
+  const int64_t K = b.ctr->key_blocks;
+  const int64_t ntiles = (K * 64 + kBinTile - 1) / kBinTile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, q = threadIdx.x & 3;
+  volatile unsigned long long* state = b.bin_state;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(&b.ctr->bin_ticket, 1u);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    if (tile >= ntiles) return;
+    const int64_t bin0 = tile * kBinTile + threadIdx.x * 16;
+    const int64_t bk = bin0 >> 6;
+    const bool live = bk < K;
+    uint32_t c[16];
+    uint32_t sum = 0;
+    if (live) {
+      const uint4* src = reinterpret_cast<const uint4*>(b.bins + bin0);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const uint4 w = src[v];
+        c[4 * v] = w.x;
+        c[4 * v + 1] = w.y;
+        c[4 * v + 2] = w.z;
+        c[4 * v + 3] = w.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) c[k] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) sum += c[k];
+    uint32_t blk_count = sum + __shfl_xor_sync(0xffffffffu, sum, 1);
+    blk_count += __shfl_xor_sync(0xffffffffu, blk_count, 2);
+    int s = 0, cx = 0, cy = 0, cz = 0;
+    bool need = false;
+    if (live && q == 0) {
+      s = scene_of_key(b, (uint32_t)bk);
+      const SceneDev& sc = b.scenes[s];
+      const uint32_t local = (uint32_t)bk - sc.key_base;
+      const uint32_t d0 = (uint32_t)sc.dim[0], d01 = d0 * (uint32_t)sc.dim[1];
+      cx = (int)(local % d0);
+      cy = (int)((local / d0) % (uint32_t)sc.dim[1]);
+      cz = (int)(local / d01);
+#pragma unroll
+      for (int d = 0; d < 8; ++d) {
+        const int ox = d & 1, oy = (d >> 1) & 1, oz = d >> 2;
+        if (cx >= ox && cy >= oy && cz >= oz) need |= b.occ[bk - (ox + oy * d0 + oz * d01)] != 0;
+      }
+    }
+    const unsigned long long v = sum + (need ? (1ull << kBlkShift) : 0ull);
+    // inclusive scan of v over the CTA
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    // work items of the block's particle run (owned by q == 0)
+    const uint32_t n_it = (q == 0 && blk_count > 0) ? (blk_count + b.chunk - 1) / b.chunk : 0u;
+    uint32_t it_x = n_it;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, it_x, o);
+      if (lane >= o) it_x += y;
+    }
+    if (lane == 31) s_items[warp] = it_x;
+    __syncthreads();
+    unsigned long long before = 0;
+    uint32_t it_before = 0;
+    for (int w = 0; w < warp; ++w) {
+      before += s_warp[w];
+      it_before += s_items[w];
+    }
+    if (warp == 0) {
+      unsigned long long agg = 0;
+      uint32_t it_total = 0;
+      for (int w = 0; w < 8; ++w) {
+        agg += s_warp[w];
+        it_total += s_items[w];
+      }
+      if (lane == 0) {
+        state[tile] = (tile == 0 ? kTileIncl : kTileAgg) | agg;
+        s_item_base = it_total ? atomicAdd(&b.ctr->n_items, it_total) : 0u;
+      }
+      unsigned long long excl = 0;
+      if (tile > 0) {
+        int64_t p = tile - 1;
+        int spin = 0;
+        for (;;) {
+          const int64_t j = p - lane;
+          unsigned long long st = 2ull << 62;  // before tile 0: an empty inclusive prefix
+          if (j >= 0) st = state[j];
+          if (__any_sync(0xffffffffu, (st >> 62) == 0)) {
+            if (++spin > (1 << 22)) {
+              if (lane == 0) flag(b, ST_SCAN_STALL);
+              break;
+            }
+            __nanosleep(32);
+            continue;
+          }
+          const unsigned incl = __ballot_sync(0xffffffffu, (st >> 62) == 2);
+          if (incl) {
+            const int first = __ffs(incl) - 1;
+            excl += warp_sum64(lane <= first ? (st & kTileVal) : 0ull);
+            break;
+          }
+          excl += warp_sum64(st & kTileVal);
+          p -= 32;
+        }
+        if (lane == 0) state[tile] = kTileIncl | (excl + agg);
+      }
+      if (lane == 0) {
+        s_prefix = excl;
+        if (tile == ntiles - 1) b.ctr->n_blocks = (uint32_t)((excl + agg) >> kBlkShift);
+      }
+    }
+    __syncthreads();
+    const unsigned long long run = s_prefix + before + x - v;
+    uint32_t pos = (uint32_t)(run & kPartMask);
+    if (live) {
+      uint4* off = reinterpret_cast<uint4*>(b.bin_off + bin0);
+      uint4* zero = reinterpret_cast<uint4*>(b.bins + bin0);
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        uint4 o;
+        o.x = pos;
+        pos += c[4 * w];
+        o.y = pos;
+        pos += c[4 * w + 1];
+        o.z = pos;
+        pos += c[4 * w + 2];
+        o.w = pos;
+        pos += c[4 * w + 3];
+        off[w] = o;
+        zero[w] = make_uint4(0, 0, 0, 0);
+      }
+    }
+    if (live && q == 0) {
+      const uint32_t id = (uint32_t)(run >> kBlkShift);
+      int32_t mapped = -1;
+      if (need) {
+        if ((int64_t)id < b.cap_blocks) {
+          const SceneDev& sc = b.scenes[s];
+          b.blk[id] = make_int4(sc.lo[0] + cx, sc.lo[1] + cy, sc.lo[2] + cz, s);
+          mapped = (int32_t)id;
+        } else {
+          flag(b, ST_BLOCK_OVERFLOW);
+        }
+      }
+      b.idmap[bk] = mapped;
+      const uint32_t start = (uint32_t)(run & kPartMask);
+      if (n_it && (int64_t)start + blk_count > b.total) flag(b, ST_LOOKUP_MISS);
+      else if (n_it) {
+        const SceneDev& sc = b.scenes[s];
+        uint32_t item = s_item_base + it_before + it_x - n_it;
+        for (uint32_t k = 0; k < n_it; ++k, ++item) {
+          if ((int64_t)item >= b.cap_items) {
+            flag(b, ST_BLOCK_OVERFLOW);
+            break;
+          }
+          BlockHeader* h = b.item_hdr + item;
+          const uint32_t a = start + k * (uint32_t)b.chunk;
+          h->start = (int32_t)a;
+          h->end = (int32_t)min(a + (uint32_t)b.chunk, start + blk_count);
+          h->scene = s;
+          h->bx = sc.lo[0] + cx;
+          h->by = sc.lo[1] + cy;
+          h->bz = sc.lo[2] + cz;
+          h->pad0 = h->pad1 = 0;
+        }
+      }
+    }
+    __syncthreads();  // s_tile, s_prefix and s_item_base are reused by the next tile
+  }
+}
+
+// Counting-sort scatter (the order of particles with equal keys is that of
+// the warps' atomics; within a warp it follows the input), the occupancy
+// bytes cleared for the next step, and the neighbour ids of every work item.
+__global__ void __launch_bounds__(256) k_scatter(const BatchDev b) {
+  if (!bins_fit(b)) return;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool valid = t < b.total;
+  const uint32_t key = valid ? b.keys[0][t] : 0xFFFFFFFFu;
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
+  const int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if (valid && lane == leader) {
+    base = atomicAdd(&b.bin_off[key], (uint32_t)__popc(peers));
+    b.occ[key >> 6] = 0;
+  }
+  base = __shfl_sync(0xffffffffu, base, leader);
+  const uint32_t pos = base + __popc(peers & ((1u << lane) - 1u));
+  if (valid) {
+    if (pos < b.total)
+      b.vals[1][pos] = b.vals[0][t];
+    else
+      flag(b, ST_LOOKUP_MISS);
+  }
+  const int64_t work = (int64_t)min(b.ctr->n_items, (uint32_t)b.cap_items) * 8;
+  for (int64_t e = t; e < work; e += (int64_t)gridDim.x * blockDim.x) {
+    BlockHeader* h = b.item_hdr + (e >> 3);
+    const int d = (int)(e & 7);
+    const SceneDev& sc = b.scenes[h->scene];
+    const int32_t id = b.idmap[block_key(sc, h->bx + (d & 1), h->by + ((d >> 1) & 1), h->bz + (d >> 2))];
+    if (id < 0) flag(b, ST_LOOKUP_MISS);
+    h->nbr[d] = id;
+  }
 }
 
 // -------------------------------------------------------------------- blocks
-__device__ __forceinline__ bool hash_insert_new(const BatchDev& b, uint32_t key, uint32_t& slot_out,
-                                                bool& created) {
+// Id of block `key` (coordinates and scene in bc), inserting it if absent.
+// Table entries hold (key << 32) | id.  The thread whose CAS claims an empty
+// slot stores the key with a pending id, takes the next block id and publishes
+// it; a thread that meets the key while its id is pending waits for it (the
+// claiming thread is running, so the wait is short; it is bounded all the
+// same and reports ST_HASH_FULL if it runs out).
+constexpr uint32_t kPendingId = 0xFFFFFFFFu;
+__device__ __forceinline__ int32_t block_id(const BatchDev& b, uint32_t key, int4 bc) {
   uint32_t slot = hash32(key) & b.hmask;
+  volatile unsigned long long* tab = b.htab;
+  const unsigned long long pending = ((unsigned long long)key << 32) | kPendingId;
   for (uint32_t probe = 0; probe <= b.hmask; ++probe) {
-    const uint32_t prev = atomicCAS(&b.hkeys[slot], kEmptyKey, key);
-    if (prev == kEmptyKey || prev == key) {
-      slot_out = slot;
-      created = prev == kEmptyKey;
-      return true;
+    unsigned long long e = tab[slot];
+    if (e == kEmptyEntry) {
+      e = atomicCAS(&b.htab[slot], kEmptyEntry, pending);
+      if (e == kEmptyEntry) {
+        const uint32_t id = atomicAdd(&b.ctr->n_blocks, 1u);
+        if ((int64_t)id >= b.cap_blocks) {
+          flag(b, ST_BLOCK_OVERFLOW);
+          atomicExch(&b.htab[slot], ((unsigned long long)key << 32) | 0x7FFFFFFFu);
+          return -1;
+        }
+        b.blk[id] = bc;
+        __threadfence();
+        atomicExch(&b.htab[slot], ((unsigned long long)key << 32) | id);
+        return (int32_t)id;
+      }
+    }
+    if ((uint32_t)(e >> 32) == key) {
+      for (int spin = 0; (uint32_t)e == kPendingId; ++spin) {
+        if (spin == (1 << 20)) {
+          flag(b, ST_HASH_FULL);
+          return -1;
+        }
+        __nanosleep(20);
+        e = tab[slot];
+      }
+      const int32_t id = (int32_t)(uint32_t)e;
+      return id < b.cap_blocks ? id : -1;
     }
     slot = (slot + 1) & b.hmask;
   }
   flag(b, ST_HASH_FULL);
-  return false;
+  return -1;
 }
 
 __device__ __forceinline__ int4 decode_block(const SceneDev& sc, uint32_t bk, int s) {
@@ -243,105 +570,62 @@ __device__ __forceinline__ int4 decode_block(const SceneDev& sc, uint32_t bk, in
   return make_int4(bx, by, bz, s);
 }
 
-__global__ void __launch_bounds__(256) k_blocks_a(const BatchDev b) {
+// Block table and work items in one pass, one CTA per `chunk` sorted positions
+// (blockDim.x == chunk).  A work item is a run of consecutive particles of one
+// block inside one chunk: it starts at a chunk start or at the first particle of
+// a block (a change of block key) and ends at the next such position.  The
+// thread at an item's start inserts or finds the ids of the item's block and
+// its +{0,1}^3 neighbours (the blocks its particles' stencils reach) and writes
+// the item header the particle kernels read.
+__global__ void __launch_bounds__(1024) k_blocks(const BatchDev b) {
+  __shared__ unsigned s_mask[32];
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= b.total) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
+  const bool valid = t < b.total;
   const uint32_t* K = sorted_keys(b);
-  const uint32_t bk = K[t] >> 6;
-  if (t > 0 && (K[t - 1] >> 6) == bk) return;
-  const uint32_t pb = atomicAdd(&b.ctr->n_pblocks, 1u);
-  if ((int64_t)pb >= b.cap_blocks) {
+  const uint32_t bk = valid ? K[t] >> 6 : 0;
+  const bool start = valid && (threadIdx.x == 0 || t == 0 || (K[t - 1] >> 6) != bk);
+  const unsigned m = __ballot_sync(0xffffffffu, start);
+  if (lane == 0) s_mask[warp] = m;
+  __syncthreads();
+  if (!start) return;
+  // the next item start inside this chunk (or the chunk's end)
+  int next = blockDim.x;
+  for (int w = warp; w < nwarps; ++w) {
+    unsigned rest = s_mask[w];
+    if (w == warp) rest = lane == 31 ? 0u : rest & (~0u << (lane + 1));
+    if (rest) {
+      next = w * 32 + __ffs(rest) - 1;
+      break;
+    }
+  }
+  const int s = scene_of(b, t);
+  const SceneDev& sc = b.scenes[s];
+  const int4 c = decode_block(sc, bk, s);
+  BlockHeader h;
+  h.start = (int32_t)t;
+  h.end = (int32_t)min((int64_t)blockIdx.x * blockDim.x + next, b.total);
+  h.scene = s;
+  h.bx = c.x;
+  h.by = c.y;
+  h.bz = c.z;
+  h.pad0 = h.pad1 = 0;
+#pragma unroll
+  for (int d = 0; d < 8; ++d) {
+    const int nx = c.x + (d & 1), ny = c.y + ((d >> 1) & 1), nz = c.z + (d >> 2);
+    h.nbr[d] = block_id(b, block_key(sc, nx, ny, nz), make_int4(nx, ny, nz, s));
+  }
+  const uint32_t item = atomicAdd(&b.ctr->n_items, 1u);
+  if ((int64_t)item >= b.cap_items) {
     flag(b, ST_BLOCK_OVERFLOW);
     return;
   }
-  const int s = scene_of(b, t);
-  b.pblk_start[pb] = (int32_t)t;
-  b.blk_key[pb] = bk;
-  b.blk[pb] = decode_block(b.scenes[s], bk, s);
-  uint32_t slot;
-  bool created;
-  if (hash_insert_new(b, bk, slot, created)) b.hvals[slot] = (int32_t)pb;
-}
-
-__global__ void __launch_bounds__(256) k_blocks_b(const BatchDev b) {
-  const uint32_t npb = min(b.ctr->n_pblocks, (uint32_t)b.cap_blocks);
-  const uint32_t* K = sorted_keys(b);
-  const int64_t work = (int64_t)npb * 8;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < work;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t pb = (uint32_t)(e >> 3);
-    const int d = (int)(e & 7);
-    const int4 bc = b.blk[pb];
-    if (d == 0) {
-      // end of the particle run of this block: first key above (bk << 6) | 63
-      const uint32_t lim = (b.blk_key[pb] << 6) | 63u;
-      int64_t lo = b.pblk_start[pb], hi = b.total;
-      while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (K[mid] <= lim) lo = mid + 1; else hi = mid;
-      }
-      b.pblk_end[pb] = (int32_t)lo;
-      const int n = (int)(lo - b.pblk_start[pb]);
-      const int cnt = (n + b.chunk - 1) / b.chunk;
-      const uint32_t base = atomicAdd(&b.ctr->n_items, (uint32_t)cnt);
-      for (int c = 0; c < cnt; ++c) {
-        if ((int64_t)base + c >= b.cap_items) {
-          flag(b, ST_BLOCK_OVERFLOW);
-          break;
-        }
-        b.items[base + c] = make_int2((int)pb, c);
-      }
-      continue;
-    }
-    const SceneDev& sc = b.scenes[bc.w];
-    const int nx = bc.x + (d & 1), ny = bc.y + ((d >> 1) & 1), nz = bc.z + (d >> 2);
-    const uint32_t nk = block_key(sc, nx, ny, nz);
-    uint32_t slot;
-    bool created;
-    if (!hash_insert_new(b, nk, slot, created) || !created) continue;
-    const uint32_t id = npb + atomicAdd(&b.ctr->n_halo, 1u);
-    if ((int64_t)id >= b.cap_blocks) {
-      flag(b, ST_BLOCK_OVERFLOW);
-      b.hvals[slot] = -1;
-      continue;
-    }
-    b.hvals[slot] = (int32_t)id;
-    b.blk[id] = make_int4(nx, ny, nz, bc.w);
-    b.blk_key[id] = nk;
-  }
+  b.item_hdr[item] = h;
 }
 
 // Number of grid blocks this step.
 __device__ __forceinline__ uint32_t num_blocks(const BatchDev& b) {
-  return min(b.ctr->n_pblocks + b.ctr->n_halo, (uint32_t)b.cap_blocks);
-}
-
-// Shared per-block header for the particle-block kernels.
-// Item headers: everything a P2G/G2P CTA needs for one work item, resolved in
-// parallel over all items once the block table is complete (the 8 neighbour
-// ids come from the hash table).
-__global__ void __launch_bounds__(256) k_items(const BatchDev b) {
-  const uint32_t items = min(b.ctr->n_items, (uint32_t)b.cap_items);
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)items * 8;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int item = (int)(e >> 3), d = (int)(e & 7);
-    const int2 it = b.items[item];
-    const int4 bc = b.blk[it.x];
-    BlockHeader* hd = b.item_hdr + item;
-    if (d == 0) {
-      const int start = b.pblk_start[it.x] + it.y * b.chunk;
-      hd->start = start;
-      hd->end = min(start + b.chunk, b.pblk_end[it.x]);
-      hd->scene = bc.w;
-      hd->bx = bc.x;
-      hd->by = bc.y;
-      hd->bz = bc.z;
-    }
-    const SceneDev& sc = b.scenes[bc.w];
-    const int32_t id = hash_find(b, block_key(sc, bc.x + (d & 1), bc.y + ((d >> 1) & 1), bc.z + (d >> 2)));
-    if (id < 0) flag(b, ST_LOOKUP_MISS);
-    hd->nbr[d] = id;
-  }
+  return min(b.ctr->n_blocks, (uint32_t)b.cap_blocks);
 }
 
 // Work-item queue of a persistent CTA.  Warp 0 claims the next item and loads
@@ -511,25 +795,40 @@ __global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
           cur = cell;
         }
         if (cell < 0) continue;
+        // The record's (weight, slope) pairs and its m, m v, force-matrix runs are
+        // 2- and 4-element aligned (record stride and offsets are even), so they
+        // are read as vectors: 7 shared loads per particle in float, 9 in double.
+        using R2 = typename Vec<R>::two;
         const R* rr = wrec + q * kRec;
-        const R wy = rr[RW_Y + 2 * qj], dwy = rr[RW_Y + 2 * qj + 1];
-        const R wz = rr[RW_Z + 2 * qk], dwz = rr[RW_Z + 2 * qk + 1];
+        const R2 py = *reinterpret_cast<const R2*>(rr + RW_Y + 2 * qj);
+        const R2 pz = *reinterpret_cast<const R2*>(rr + RW_Z + 2 * qk);
+        const R2 px0 = *reinterpret_cast<const R2*>(rr + RW_X + 2 * qi);
+        const R2 px1 = *reinterpret_cast<const R2*>(rr + RW_X + 2 * (qi + 2));
+        const R2 mm0 = *reinterpret_cast<const R2*>(rr + R_M);       // m, m v_x
+        const R2 mm1 = *reinterpret_cast<const R2*>(rr + R_M + 2);   // m v_y, m v_z
+        R2 f0 = {}, f1 = {}, f2 = {};
+        if constexpr (kForce) {
+          f0 = *reinterpret_cast<const R2*>(rr + R_F);      // xx, yy
+          f1 = *reinterpret_cast<const R2*>(rr + R_F + 2);  // zz, xy
+          f2 = *reinterpret_cast<const R2*>(rr + R_F + 4);  // xz, yz
+        }
+        const R wy = py.x, dwy = py.y, wz = pz.x, dwz = pz.y;
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
           R* acc = s == 0 ? a0 : a1;
-          const R wxv = rr[RW_X + 2 * (qi + 2 * s)], dwx = rr[RW_X + 2 * (qi + 2 * s) + 1];
+          const R2 px = s == 0 ? px0 : px1;
+          const R wxv = px.x, dwx = px.y;
           const R A = wxv * wy;
           const R w = A * wz;
-          if constexpr (kMass) acc[0] += w * rr[R_M];
+          if constexpr (kMass) acc[0] += w * mm0.x;
           if constexpr (kMom) {
-            acc[1] += w * rr[R_MV];
-            acc[2] += w * rr[R_MV + 1];
-            acc[3] += w * rr[R_MV + 2];
+            acc[1] += w * mm0.y;
+            acc[2] += w * mm1.x;
+            acc[3] += w * mm1.y;
           }
           if constexpr (kForce) {
             const R gx = (dwx * wy) * wz, gy = (wxv * dwy) * wz, gz = A * dwz;
-            const R mxx = rr[R_F], myy = rr[R_F + 1], mzz = rr[R_F + 2];
-            const R mxy = rr[R_F + 3], mxz = rr[R_F + 4], myz = rr[R_F + 5];
+            const R mxx = f0.x, myy = f0.y, mzz = f1.x, mxy = f1.y, mxz = f2.x, myz = f2.y;
             acc[4] += mxx * gx + mxy * gy + mxz * gz;
             acc[5] += mxy * gx + myy * gy + myz * gz;
             acc[6] += mxz * gx + myz * gy + mzz * gz;
@@ -679,10 +978,11 @@ __device__ __forceinline__ Sym3<R> next_force(const M3<R>& FE, const Plastic<R>&
 }
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(256, 2) k_g2p(const BatchDev b) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const BatchDev b) {
   constexpr int NCH = G2PChannels<MODE>::n;
   constexpr bool kGrad = MODE == G2P_FULL || MODE == G2P_STRESS;
   constexpr bool kVel = MODE == G2P_FULL || MODE == G2P_VELOCITY;
+  constexpr bool kDeferDouble = MODE == G2P_FULL && !std::is_same<R, double>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][kTileN]
   __shared__ BlockHeader h;
@@ -808,9 +1108,11 @@ __global__ void __launch_bounds__(256, 2) k_g2p(const BatchDev b) {
           }
         }
         const R dt = (R)sc.dt;
-        M3<R> FEn;
+        M3<R> FEn, trial;
         M3<double> FPn;
         Plastic<R> pl;
+        bool needs_double = false;
+        (void)trial;
         if constexpr (kGrad) {
           // stress_update (grid.cpp:277-285)
           M3<R> FE, L;
@@ -823,12 +1125,21 @@ __global__ void __launch_bounds__(256, 2) k_g2p(const BatchDev b) {
           L.a[4] += R(1);
           L.a[8] += R(1);
           FEn = mat_mul(L, FE);
-          bool used_fp64 = false;
-          pl = project(FEn, sc, used_fp64);
-          if constexpr (!std::is_same<R, double>::value) {
-            const unsigned act = __activemask();
-            const unsigned fb = __ballot_sync(act, used_fp64);
-            if (fb && (threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&b.ctr->fp64_projections, (uint32_t)__popc(fb));
+          if constexpr (kDeferDouble) {
+            // Mixed form: a projection that needs double is redone by k_fixup
+            // from the trial F_E, which is kept for it in the output slot.
+            trial = FEn;
+            const R lo = R(1) - (R)sc.theta_c, hi = R(1) + (R)sc.theta_s;
+            pl = plastic_projection(FEn, lo, hi);
+            needs_double = near_critical(pl.sigma, lo, hi, (R)kMixedTau, pl.clamped);
+          } else {
+            bool used_fp64 = false;
+            pl = project(FEn, sc, used_fp64);
+            if constexpr (!std::is_same<R, double>::value) {
+              const unsigned act = __activemask();
+              const unsigned fb = __ballot_sync(act, used_fp64);
+              if (fb && (threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&b.ctr->fp64_projections, (uint32_t)__popc(fb));
+            }
           }
 #pragma unroll
           for (int e = 0; e < 9; ++e) FPn.a[e] = pv.fp[e * pv.st + i];
@@ -890,8 +1201,23 @@ __global__ void __launch_bounds__(256, 2) k_g2p(const BatchDev b) {
           rw[PVOL * st + o] = V0;
 #pragma unroll
           for (int e = 0; e < 9; ++e) {
-            rw[(PFE + e) * st + o] = FEn.a[e];
+            rw[(PFE + e) * st + o] = needs_double ? trial.a[e] : FEn.a[e];
             fw[e * st + o] = FPn.a[e];
+          }
+          if constexpr (kDeferDouble) {
+            const unsigned act = __activemask();
+            const unsigned fb = __ballot_sync(act, needs_double);
+            if (fb) {
+              const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
+              uint32_t base = 0;
+              if (lane == leader) base = atomicAdd(&b.ctr->fp64_projections, (uint32_t)__popc(fb));
+              base = __shfl_sync(act, base, leader);
+              if (needs_double) {
+                const uint32_t slot = base + __popc(fb & ((1u << lane) - 1u));
+                if (slot < (uint32_t)b.cap_fixups) b.fixups[slot] = make_int4(s, (int)o, (int)i, 0);
+                else flag(b, ST_BLOCK_OVERFLOW);
+              }
+            }
           }
           rw[(PFM + 0) * st + o] = Mn.xx;
           rw[(PFM + 1) * st + o] = Mn.yy;
@@ -916,6 +1242,53 @@ __global__ void __launch_bounds__(256, 2) k_g2p(const BatchDev b) {
     }
   }
   if (MODE == G2P_FULL && last_scene >= 0) flush_box(b.scenes[last_scene], bmin, bmax);
+}
+
+// Mixed form: the plastic projections G2P flagged as near-critical, redone in
+// double from the trial F_E it left in the output slot, with the new F_P and
+// the next force matrix (runs after G2P, before the buffers swap).
+__global__ void __launch_bounds__(256) k_fixup(const BatchDev b) {
+  const uint32_t n = min(b.ctr->fp64_projections, (uint32_t)b.cap_fixups);
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int4 f = b.fixups[e];
+    const SceneDev& sc = b.scenes[f.x];
+    const int cur = sc.cur;
+    float* rw = (float*)sc.r[cur ^ 1];
+    double* fw = sc.fp[cur ^ 1];
+    const double* fp_old = sc.fp[cur];
+    const int64_t st = sc.stride, o = f.y, i = f.z;
+    M3<double> F, FP;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      F.a[k] = (double)rw[(PFE + k) * st + o];
+      FP.a[k] = fp_old[k * st + i];
+    }
+    const Plastic<double> pl = plastic_projection(F, 1.0 - sc.theta_c, 1.0 + sc.theta_s);
+    if (pl.clamped) {
+      const Sym3<double>& Di = pl.Dinv;
+      M3<double> Dm;
+      const double d[9] = {Di.xx, Di.xy, Di.xz, Di.xy, Di.yy, Di.yz, Di.xz, Di.yz, Di.zz};
+#pragma unroll
+      for (int k = 0; k < 9; ++k) Dm.a[k] = d[k];
+      FP = mat_mul(Dm, FP);
+    }
+    const double hard = exp(sc.xi * (1.0 - det3(FP)));
+    const double V0 = (double)rw[PVOL * st + o];
+    const Sym3<double> M = pl.regular
+                               ? assemble_force(gram_rows(F), pl.root, det3(F), V0, sc.mu0, sc.lambda0, hard)
+                               : force_matrix(F, V0, sc.mu0, sc.lambda0, hard);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      rw[(PFE + k) * st + o] = (float)F.a[k];
+      fw[k * st + o] = FP.a[k];
+    }
+    rw[(PFM + 0) * st + o] = (float)M.xx;
+    rw[(PFM + 1) * st + o] = (float)M.yy;
+    rw[(PFM + 2) * st + o] = (float)M.zz;
+    rw[(PFM + 3) * st + o] = (float)M.xy;
+    rw[(PFM + 4) * st + o] = (float)M.xz;
+    rw[(PFM + 5) * st + o] = (float)M.yz;
+  }
 }
 
 // Force matrix of every particle from its F_E, F_P and V_p0 (after an upload,
@@ -993,10 +1366,16 @@ void StepLaunch<R>::keys(const BatchDev& b, cudaStream_t s) {
 template <typename R>
 void StepLaunch<R>::blocks(const BatchDev& b, cudaStream_t s) {
   if (b.total <= 0) return;
-  cudaMemsetAsync(b.hkeys, 0xFF, sizeof(uint32_t) * ((size_t)b.hmask + 1), s);
-  k_blocks_a<<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
-  k_blocks_b<<<2 * sm_count(), 256, 0, s>>>(b);
-  k_items<<<2 * sm_count(), 256, 0, s>>>(b);
+  if (b.dense) {
+    static int grid = 0;
+    if (!grid) grid = persistent_grid(k_bins, 256, 0);
+    const int64_t tiles = b.cap_bins / kBinTile;
+    k_bins<<<(unsigned)std::min<int64_t>(grid, std::max<int64_t>(tiles, 1)), 256, 0, s>>>(b);
+    k_scatter<<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
+    return;
+  }
+  cudaMemsetAsync(b.htab, 0xFF, sizeof(unsigned long long) * ((size_t)b.hmask + 1), s);
+  k_blocks<<<(unsigned)((b.total + b.chunk - 1) / b.chunk), b.chunk, 0, s>>>(b);
 }
 
 template <typename R, int MODE>
@@ -1051,6 +1430,11 @@ void StepLaunch<R>::g2p(const BatchDev& b, int mode, cudaStream_t s) {
     case G2P_STRESS: launch_g2p<R, G2P_STRESS>(b, s); break;
     case G2P_VELOCITY: launch_g2p<R, G2P_VELOCITY>(b, s); break;
   }
+}
+template <typename R>
+void StepLaunch<R>::fixup(const BatchDev& b, cudaStream_t s) {
+  if (std::is_same<R, double>::value || b.total <= 0) return;
+  k_fixup<<<2 * sm_count(), 256, 0, s>>>(b);
 }
 template <typename R>
 void StepLaunch<R>::prepare_force(const BatchDev& b, cudaStream_t s) {

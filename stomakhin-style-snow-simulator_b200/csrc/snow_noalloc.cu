@@ -53,12 +53,12 @@ constexpr size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 
 // Byte offsets of every region inside the arena.
 struct Layout {
-  size_t staging, r0, r1, fp0, fp1, id0, id1, k0, k1, v0, v1, hist, dtot, hkeys, hvals, blk,
-      blk_key, pstart, pend, items, item_hdr, acc, vel, ctr, scene, coll, total;
+  size_t staging, r0, r1, fp0, fp1, id0, id1, k0, k1, v0, v1, hist, dtot, htab, blk, item_hdr, acc,
+      vel, ctr, scene, coll, total;
   constexpr Layout()
       : staging(0), r0(0), r1(0), fp0(0), fp1(0), id0(0), id1(0), k0(0), k1(0), v0(0), v1(0),
-        hist(0), dtot(0), hkeys(0), hvals(0), blk(0), blk_key(0), pstart(0), pend(0), items(0), item_hdr(0), acc(0),
-        vel(0), ctr(0), scene(0), coll(0), total(0) {
+        hist(0), dtot(0), htab(0), blk(0), item_hdr(0), acc(0), vel(0), ctr(0), scene(0), coll(0),
+        total(0) {
     size_t o = 0;
     auto take = [&o](size_t bytes) {
       const size_t at = o;
@@ -77,15 +77,10 @@ struct Layout {
     k1 = take(N * sizeof(uint32_t));
     v0 = take(N * sizeof(uint32_t));
     v1 = take(N * sizeof(uint32_t));
-    hist = take((size_t)kTiles * 256 * sizeof(uint32_t));
-    dtot = take(256 * sizeof(uint32_t));
-    hkeys = take(kHashSlots * sizeof(uint32_t));
-    hvals = take(kHashSlots * sizeof(int32_t));
+    hist = take((size_t)kTiles * (1 << kRadixBits) * sizeof(uint32_t));
+    dtot = take((1 << kRadixBits) * sizeof(uint32_t));
+    htab = take(kHashSlots * sizeof(unsigned long long));
     blk = take((size_t)kMaxBlocks * sizeof(int4));
-    blk_key = take((size_t)kMaxBlocks * sizeof(uint32_t));
-    pstart = take((size_t)kMaxBlocks * sizeof(int32_t));
-    pend = take((size_t)kMaxBlocks * sizeof(int32_t));
-    items = take((size_t)kItems * sizeof(int2));
     item_hdr = take((size_t)kItems * sizeof(BlockHeader));
     acc = take((size_t)kMaxBlocks * 64 * kAccCh * sizeof(double));
     vel = take((size_t)kMaxBlocks * 64 * kVelCh * sizeof(double));
@@ -231,15 +226,10 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
     b.hist = reinterpret_cast<uint32_t*>(A + L.hist);
     b.digit_total = reinterpret_cast<uint32_t*>(A + L.dtot);
     b.ntiles = radix_tiles(n);
-    b.hkeys = reinterpret_cast<uint32_t*>(A + L.hkeys);
-    b.hvals = reinterpret_cast<int32_t*>(A + L.hvals);
+    b.htab = reinterpret_cast<unsigned long long*>(A + L.htab);
     b.hmask = kHashSlots - 1;
     b.cap_blocks = kMaxBlocks;
     b.blk = reinterpret_cast<int4*>(A + L.blk);
-    b.blk_key = reinterpret_cast<uint32_t*>(A + L.blk_key);
-    b.pblk_start = reinterpret_cast<int32_t*>(A + L.pstart);
-    b.pblk_end = reinterpret_cast<int32_t*>(A + L.pend);
-    b.items = reinterpret_cast<int2*>(A + L.items);
     b.item_hdr = reinterpret_cast<BlockHeader*>(A + L.item_hdr);
     b.cap_items = kItems;
     b.chunk = kChunk;

@@ -5,6 +5,7 @@
 // API and its tests, not for speed.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -34,6 +35,7 @@ struct StageGrid {
   BatchDev b{};
   StageGrid(const double* rec, int64_t n_, const snow_step_params& p) : n(n_) {
     id = batch.add_scene(rec, n, &p, nullptr, 0, nullptr);
+    batch.set_dense(false);  // the node export reads the block hash table
     batch.prepare(nullptr);
     b = batch.dev(batch.device_scenes(), 1, n);
     StepLaunch<double>::keyspace(b, nullptr, true);
@@ -49,38 +51,52 @@ struct StageGrid {
   }
   int64_t blocks() const {
     const Counters* c = const_cast<StageGrid*>(this)->batch.host_counters();
-    return (int64_t)c->n_pblocks + c->n_halo;
+    return std::min<int64_t>(c->n_blocks, b.cap_blocks);
   }
   // Every node of every block, with the channels of acc.
   void export_nodes(int32_t* ijk, double* fields, int64_t cap, int64_t* n_nodes) {
     finish_checked();
     const int64_t nb = blocks();
-    const int64_t nn = nb * 64;
+    std::vector<int4> blk((size_t)nb);
+    check_cuda(cudaMemcpy(blk.data(), b.blk, nb * sizeof(int4), cudaMemcpyDeviceToHost), "blocks");
+    // ids that lost an insertion race hold no nodes: keep only the ids in the table
+    std::vector<unsigned long long> tab((size_t)b.hmask + 1);
+    check_cuda(cudaMemcpy(tab.data(), b.htab, tab.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+               "block table");
+    std::vector<char> live((size_t)nb, 0);
+    int64_t n_live = 0;
+    for (const unsigned long long e : tab)
+      if (e != kEmptyEntry && (int64_t)(uint32_t)e < nb && !live[(uint32_t)e]) {
+        live[(uint32_t)e] = 1;
+        ++n_live;
+      }
+    const int64_t nn = n_live * 64;
     if (n_nodes) *n_nodes = nn;
     if (nn > cap) throw Error(SNOW_E_ARG, "node capacity too small: need " + std::to_string(nn));
-    std::vector<int4> blk((size_t)nb);
-    std::vector<double> acc((size_t)(nb * 64));
-    check_cuda(cudaMemcpy(blk.data(), b.blk, nb * sizeof(int4), cudaMemcpyDeviceToHost), "blocks");
     const int64_t plane = (int64_t)b.cap_blocks * 64;
     std::vector<std::vector<double>> ch(kAccCh);
     for (int c = 0; c < kAccCh; ++c) {
-      ch[c].resize((size_t)nn);
-      check_cuda(cudaMemcpy(ch[c].data(), (const double*)b.acc + c * plane, nn * sizeof(double),
+      ch[c].resize((size_t)(nb * 64));
+      check_cuda(cudaMemcpy(ch[c].data(), (const double*)b.acc + c * plane, nb * 64 * sizeof(double),
                             cudaMemcpyDeviceToHost),
                  "grid");
     }
-    for (int64_t k = 0; k < nn; ++k) {
-      const int4 bc = blk[(size_t)(k >> 6)];
-      const int node = (int)(k & 63);
-      ijk[3 * k] = 4 * bc.x + (node & 3);
-      ijk[3 * k + 1] = 4 * bc.y + ((node >> 2) & 3);
-      ijk[3 * k + 2] = 4 * bc.z + (node >> 4);
-      double* f = fields + 10 * k;
-      f[0] = ch[0][k];
-      for (int a = 0; a < 3; ++a) {
-        f[1 + a] = ch[1 + a][k];
-        f[4 + a] = 0.0;
-        f[7 + a] = ch[4 + a][k];
+    int64_t k = 0;
+    for (int64_t id = 0; id < nb; ++id) {
+      if (!live[(size_t)id]) continue;
+      const int4 bc = blk[(size_t)id];
+      for (int node = 0; node < 64; ++node, ++k) {
+        const int64_t e = id * 64 + node;
+        ijk[3 * k] = 4 * bc.x + (node & 3);
+        ijk[3 * k + 1] = 4 * bc.y + ((node >> 2) & 3);
+        ijk[3 * k + 2] = 4 * bc.z + (node >> 4);
+        double* f = fields + 10 * k;
+        f[0] = ch[0][(size_t)e];
+        for (int a = 0; a < 3; ++a) {
+          f[1 + a] = ch[1 + a][(size_t)e];
+          f[4 + a] = 0.0;
+          f[7 + a] = ch[4 + a][(size_t)e];
+        }
       }
     }
     StepLaunch<double>::zero_grid(b, nullptr);
@@ -120,7 +136,7 @@ __global__ void k_load_nodes(const BatchDev b, const int32_t* ijk, const double*
 
 __global__ void k_zero_vel(const BatchDev b) {
   const int64_t plane = (int64_t)b.cap_blocks * 64;
-  const int64_t work = (int64_t)(b.ctr->n_pblocks + b.ctr->n_halo) * 64;
+  const int64_t work = (int64_t)min(b.ctr->n_blocks, (uint32_t)b.cap_blocks) * 64;
   double* vel = (double*)b.vel;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < work; e += (int64_t)gridDim.x * blockDim.x)
     for (int c = 0; c < kVelCh; ++c) vel[c * plane + e] = 0.0;

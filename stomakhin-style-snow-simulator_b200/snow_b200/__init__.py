@@ -17,7 +17,7 @@ import os
 import numpy as np
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "libsnow_b200.so")
+LIB_PATH = os.environ.get("SNOW_B200_LIB") or os.path.join(PKG_DIR, "libsnow_b200.so")
 
 SNOW_FP64, SNOW_MIXED = 0, 1
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "grid capacity exceeded",
@@ -122,6 +122,8 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_server_result": (ctypes.c_int, [vp, i64, _dp, i64, _dp]),
         "snow_gpu_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
         "snow_gpu_batch_set_chunk": (ctypes.c_int, [vp, ctypes.c_int]),
+        "snow_gpu_batch_set_dense": (ctypes.c_int, [vp, ctypes.c_int]),
+        "snow_gpu_batch_graph_kernels": (ctypes.c_int, [vp]),
         "snow_gpu_setup": (ctypes.c_int, [_dp, i64, d]),
         "snow_gpu_step": (ctypes.c_int, [_dp, i64, ctypes.POINTER(StepParams), ctypes.POINTER(Collider),
                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(StepTimings)]),
@@ -260,8 +262,16 @@ class Batch:
     def set_graphs(self, enable: bool) -> None:
         _check(lib().snow_gpu_batch_set_graphs(self._h, int(bool(enable))))
 
+    def graph_kernels(self) -> int:
+        """Kernel launches in one replay of the captured step graph (0 before capture)."""
+        return int(lib().snow_gpu_batch_graph_kernels(self._h))
+
+    def set_dense(self, enable: bool) -> None:
+        """Counting sort over dense key bins (default) or the radix sort with the block hash table."""
+        _check(lib().snow_gpu_batch_set_dense(self._h, int(bool(enable))))
+
     def set_chunk(self, chunk: int) -> None:
-        """Particles per P2G/G2P work item (power of two, 32..4096)."""
+        """Particles per P2G/G2P work item (power of two, 32..1024)."""
         _check(lib().snow_gpu_batch_set_chunk(self._h, int(chunk)))
 
     def autotune(self, trial_steps: int = 10, stream: int | None = None) -> tuple[int, float]:

@@ -16,9 +16,10 @@ TOL = 1e-10
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
-def _run_batch(snow, rec, params, planes, steps, graphs=True):
+def _run_batch(snow, rec, params, planes, steps, graphs=True, dense=True):
     b = snow.Batch(snow.SNOW_FP64)
     b.set_graphs(graphs)
+    b.set_dense(dense)
     sid = b.add_scene(rec, params, planes)
     b.step(steps)
     out = b.download(sid)
@@ -47,14 +48,16 @@ def test_step_matches_reference_golden(snow, name, steps):
 
 @pytest.mark.parametrize("steps", [1, 10])
 @pytest.mark.parametrize("graphs", [True, False])
-def test_cube_32_matches_oracle(snow, oracle, steps, graphs):
-    """The small-case cube (32^3 = 32,768 particles) against the oracle."""
+@pytest.mark.parametrize("dense", [True, False])
+def test_cube_32_matches_oracle(snow, oracle, steps, graphs, dense):
+    """The small-case cube (32^3 = 32,768 particles) against the oracle, with
+    the counting sort over dense key bins and with the radix-sort fallback."""
     from snow_b200 import scenes
 
     sc = scenes.cube_scene(32)
     rec = oracle.setup(sc.particles, sc.dx)
     want, _ = oracle.step(rec, sc.params(), sc.plane_array(), steps)
-    got = _run_batch(snow, rec, sc.params(), sc.planes, steps, graphs)
+    got = _run_batch(snow, rec, sc.params(), sc.planes, steps, graphs, dense)
     e = errors(got, want)
     assert max(e.values()) < TOL, e
 
