@@ -205,6 +205,23 @@ def timed_steps(batch, steps, sp, torch) -> float:
     return e0.elapsed_time(e1)
 
 
+def plain_fp64_rate(snow_b200, torch, sp, items) -> float:
+    """Particle-steps/s of the plain FP64 path on the given scenes: each scene
+    alone in its own one-scene batch (the drop-in step on resident state, with
+    its captured step graph), one scene after another.  items: (scene, steps,
+    timed steps); a scene's time is its timed steps' time scaled to `steps`."""
+    particle_steps, ms = 0.0, 0.0
+    for sc, n_steps, k in items:
+        b = snow_b200.Batch(snow_b200.SNOW_FP64)
+        i = b.add(sc, stream=sp)
+        b.setup(i, sc.dx, stream=sp)
+        b.step(3, stream=sp)
+        ms += timed_steps(b, k, sp, torch) * n_steps / k
+        particle_steps += sc.n * n_steps
+        b.close()
+    return particle_steps / (ms * 1e-3)
+
+
 def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
     """The mixed-precision, batched and served forms (single GPU).
 
@@ -280,8 +297,13 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
             worst[k] = max(worst.get(k, 0.0), v)
     a.close()
     b.close()
+    bsteps = max(20, steps // 4)
+    plain_b = plain_fp64_rate(snow_b200, torch, sp, [(sc, bsteps, bsteps) for sc in bscenes])
     forms["batched"] = {"scenes": len(bscenes), "particles": nb, "unit": "particle-steps/s",
                         "fp64": brates["fp64"], "mixed": brates["mixed"],
+                        "plain_fp64_one_scene_at_a_time": plain_b,
+                        "mixed_vs_plain_fp64_same_scenes": brates["mixed"]["value"] / plain_b,
+                        "fp64_batched_vs_plain_fp64_same_scenes": brates["fp64"]["value"] / plain_b,
                         "mixed_vs_fp64": brates["mixed"]["value"] / brates["fp64"]["value"],
                         "mixed_vs_plain_fp64_headline": brates["mixed"]["value"] / fp64_rate,
                         "mixed_error_vs_fp64_step10_first16": worst,
@@ -294,7 +316,12 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
     srv.run(stream=sp)
     st = srv.stats()
     srv.close()
+    plain_s = plain_fp64_rate(snow_b200, torch, sp, [(sc, n, min(n, 40)) for sc, n, _ in reqs])
     forms["served"] = {"requests": len(reqs), "arrival_rate_per_s": 200.0, "budget_bytes": 150 * 10**9,
+                       "plain_fp64_one_request_at_a_time": plain_s,
+                       "plain_fp64_sample": "each request's scene alone, min(steps, 40) timed steps "
+                                            "scaled to its requested steps",
+                       "served_vs_plain_fp64_same_requests": st["particle_steps_per_s"] / plain_s,
                        "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"],
                        "mean_latency_s": st["mean_s"], "particle_steps_per_s": st["particle_steps_per_s"],
                        "served_vs_plain_fp64_headline": st["particle_steps_per_s"] / fp64_rate,

@@ -55,8 +55,11 @@ struct Vec<double> {
   using two = double2;
 };
 
-constexpr int kTileN = 544;  // 8 x 8 x 8 node tile, z stride padded to 68
-SNOW_HD int tile_index(int x, int y, int z) { return x + 8 * y + 68 * z; }
+// 7 x 7 x 7 node tile of a block and its +{0,1}^3 neighbours.  Strides 9 (y)
+// and 68 (z) put the 16 (y, z) columns a warp's lanes own in P2G on distinct
+// shared-memory banks for 4- and 8-byte elements.
+constexpr int kTileN = 476;
+SNOW_HD int tile_index(int x, int y, int z) { return x + 9 * y + 68 * z; }
 
 __device__ __forceinline__ const uint32_t* sorted_keys(const BatchDev& b) {
   const uint32_t passes = (b.ctr->sort_bits + kRadixBits - 1) / kRadixBits;
@@ -671,33 +674,52 @@ struct P2GChannels {
 
 // Per-particle record staged in shared memory for the scatter: interleaved
 // (weight, slope) pairs per axis and stencil offset, then m, m v, and the
-// symmetric force matrix.
-constexpr int kRec = 36;
-enum : int { RW_X = 0, RW_Y = 8, RW_Z = 16, R_M = 24, R_MV = 25, R_F = 28 };
+// symmetric force matrix.  Record strides (36 floats, 34 doubles) make the
+// 16-byte record stores of a warp conflict-free.
+enum : int { RW_X = 0, RW_Y = 8, RW_Z = 16, R_M = 24, R_MV = 25, R_F = 28, kRecFields = 34 };
 constexpr int kP2GWarps = 8;
+
+template <typename R>
+constexpr int rec_stride() {
+  return sizeof(R) == 4 ? 36 : 34;
+}
 
 template <typename R, int MODE>
 constexpr size_t p2g_smem() {
-  return sizeof(R) * (P2GChannels<R, MODE>::n * kTileN + kP2GWarps * 32 * kRec) +
+  return sizeof(R) * (P2GChannels<R, MODE>::n * kTileN + kP2GWarps * 32 * rec_stride<R>()) +
          sizeof(int) * kP2GWarps * 32;
+}
+
+// Stores a 34-field record with 16-byte stores.
+__device__ __forceinline__ void store_record(float* rr, const float (&v)[kRecFields]) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    reinterpret_cast<float4*>(rr)[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+  reinterpret_cast<float2*>(rr)[16] = make_float2(v[32], v[33]);
+}
+__device__ __forceinline__ void store_record(double* rr, const double (&v)[kRecFields]) {
+#pragma unroll
+  for (int k = 0; k < 17; ++k) reinterpret_cast<double2*>(rr)[k] = make_double2(v[2 * k], v[2 * k + 1]);
 }
 
 // P2G with the lanes of a warp mapped to stencil nodes rather than particles.
 //
 // A warp takes 32 consecutive particles of the block's cell-sorted run.  First
-// every lane evaluates one particle -- weights, hardening, stress (the Jacobi
-// eigensolve) -- into a shared-memory record.  Then the warp walks the 32
-// records in order; lane l owns the two stencil nodes (l>>4 + {0,2}, (l>>2)&3,
-// l&3) of the current particle and adds that particle's mass, momentum and
-// force contributions into registers.  Consecutive particles share a cell, so
-// the register sums only leave the warp (as shared-memory atomics into the
-// block tile) when the cell changes.  Compared with one particle per lane this
-// removes the 7 x 64 shared-memory atomics per particle, which for doubles are
-// compare-and-swap loops.  The tile is flushed to the global grid with one
-// atomic per node and channel.
+// every lane evaluates one particle -- weights, m v, the force matrix -- into a
+// shared-memory record.  Then the warp walks the 32 records in order; lane l
+// owns the two stencil nodes (l>>4 + {0,2}, (l>>2)&3, l&3) of the current
+// particle and adds that particle's mass, momentum and force into registers.
+// Per (y, z) column the lane forms A = wy wz, B = dwy wz, C = wy dwz once,
+// then U = A M e_x and V = B M e_y + C M e_z, so a node (wx, dwx) of the
+// column takes wx (m, m v) A and dwx U + wx V: M grad w with grad w =
+// (dwx A, wx B, wx C).  Consecutive particles share a cell, so the register sums only leave
+// the warp (as shared-memory atomics into the block tile) when the cell
+// changes.  The tile is flushed to the global grid with one atomic per node and
+// channel.
 template <typename R, int MODE>
-__global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const BatchDev b) {
   constexpr int NCH = P2GChannels<R, MODE>::n;
+  constexpr int kRec = rec_stride<R>();
   constexpr bool kMom = MODE == P2G_FULL || MODE == P2G_PRE || MODE == P2G_MASS_MOMENTUM;
   constexpr bool kForce = MODE == P2G_FULL || MODE == P2G_PRE || MODE == P2G_FORCE;
   constexpr bool kMass = MODE != P2G_FORCE;
@@ -712,7 +734,7 @@ __global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
   R* wrec = recs + warp * 32 * kRec;
   int* wcell = cells + warp * 32;
   const int qi = lane >> 4, qj = (lane >> 2) & 3, qk = lane & 3;
-  const int off0 = tile_index(qi, qj, qk), off1 = tile_index(qi + 2, qj, qk);
+  const int col = tile_index(0, qj, qk);
 
   __shared__ int s_item;
   ItemQueue q;
@@ -732,27 +754,30 @@ __global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
         const R x0 = pv.at(PX, i), x1 = pv.at(PX + 1, i), x2 = pv.at(PX + 2, i);
         const AxisWeights<R> wx = axis_weights(x0, dx), wy = axis_weights(x1, dx), wz = axis_weights(x2, dx);
         const int tx = wx.base - 4 * h.bx, ty = wy.base - 4 * h.by, tz = wz.base - 4 * h.bz;
-        R* rr = wrec + lane * kRec;
+        R v[kRecFields];
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          rr[RW_X + 2 * a] = wx.w[a];
-          rr[RW_X + 2 * a + 1] = wx.dw[a];
-          rr[RW_Y + 2 * a] = wy.w[a];
-          rr[RW_Y + 2 * a + 1] = wy.dw[a];
-          rr[RW_Z + 2 * a] = wz.w[a];
-          rr[RW_Z + 2 * a + 1] = wz.dw[a];
+          v[RW_X + 2 * a] = wx.w[a];
+          v[RW_X + 2 * a + 1] = wx.dw[a];
+          v[RW_Y + 2 * a] = wy.w[a];
+          v[RW_Y + 2 * a + 1] = wy.dw[a];
+          v[RW_Z + 2 * a] = wz.w[a];
+          v[RW_Z + 2 * a + 1] = wz.dw[a];
         }
         const R m = pv.at(PM, i);
-        rr[R_M] = m;
+        v[R_M] = m;
+        v[R_MV] = v[R_MV + 1] = v[R_MV + 2] = R(0);
         if constexpr (kMom) {
-          rr[R_MV] = m * pv.at(PV, i);
-          rr[R_MV + 1] = m * pv.at(PV + 1, i);
-          rr[R_MV + 2] = m * pv.at(PV + 2, i);
+          v[R_MV] = m * pv.at(PV, i);
+          v[R_MV + 1] = m * pv.at(PV + 1, i);
+          v[R_MV + 2] = m * pv.at(PV + 2, i);
         }
+#pragma unroll
+        for (int e = 0; e < 6; ++e) v[R_F + e] = R(0);
         if constexpr (MODE == P2G_PRE) {
           // force matrix left by the previous step's G2P (or prepare_force)
 #pragma unroll
-          for (int e = 0; e < 6; ++e) rr[R_F + e] = pv.at(PFM + e, i);
+          for (int e = 0; e < 6; ++e) v[R_F + e] = pv.at(PFM + e, i);
         } else if constexpr (kForce) {
           M3<R> FE;
 #pragma unroll
@@ -762,88 +787,89 @@ __global__ void __launch_bounds__(256) k_p2g(const BatchDev b) {
           for (int e = 0; e < 9; ++e) FP.a[e] = pv.fp[e * pv.st + i];
           const double hard = exp(sc.xi * (1.0 - det3(FP)));
           const Sym3<R> M = force_matrix<R>(FE, pv.at(PVOL, i), (R)sc.mu0, (R)sc.lambda0, (R)hard);
-          rr[R_F] = M.xx;
-          rr[R_F + 1] = M.yy;
-          rr[R_F + 2] = M.zz;
-          rr[R_F + 3] = M.xy;
-          rr[R_F + 4] = M.xz;
-          rr[R_F + 5] = M.yz;
+          v[R_F] = M.xx;
+          v[R_F + 1] = M.yy;
+          v[R_F + 2] = M.zz;
+          v[R_F + 3] = M.xy;
+          v[R_F + 4] = M.xz;
+          v[R_F + 5] = M.yz;
         }
+        store_record(wrec + lane * kRec, v);
         const bool inside = (unsigned)tx <= 3u && (unsigned)ty <= 3u && (unsigned)tz <= 3u;
         if (!inside) flag(b, ST_OUT_OF_BOX);  // non-finite or mis-sorted: never index the tile with it
         wcell[lane] = inside ? tile_index(tx, ty, tz) : -1;
       }
       __syncwarp();
       const int cnt = min(32, n - base);
-      R a0[NCH], a1[NCH];
+      R acc[2][NCH];
 #pragma unroll
-      for (int c = 0; c < NCH; ++c) a0[c] = a1[c] = R(0);
-      int cur = -1;
-      for (int q = 0; q < cnt; ++q) {
-        const int cell = wcell[q];  // uniform across the warp
-        if (cell != cur) {
-          if (cur >= 0) {
+      for (int x = 0; x < 2; ++x)
 #pragma unroll
-            for (int c = 0; c < NCH; ++c) {
-              if (c == 0 && !kMass) continue;
-              if (c >= 1 && c <= 3 && !kMom) continue;
-              atomicAdd(&tile[c * kTileN + cur + off0], a0[c]);
-              atomicAdd(&tile[c * kTileN + cur + off1], a1[c]);
-              a0[c] = a1[c] = R(0);
-            }
+        for (int c = 0; c < NCH; ++c) acc[x][c] = R(0);
+      auto flush = [&](int at) {
+#pragma unroll
+        for (int x = 0; x < 2; ++x)
+#pragma unroll
+          for (int c = 0; c < NCH; ++c) {
+            if (c == 0 && !kMass) continue;
+            if (c >= 1 && c <= 3 && !kMom) continue;
+            atomicAdd(&tile[c * kTileN + at + col + qi + 2 * x], acc[x][c]);
+            acc[x][c] = R(0);
           }
+      };
+      int cur = -1;
+      for (int qq = 0; qq < cnt; ++qq) {
+        const int cell = wcell[qq];  // uniform across the warp
+        if (cell != cur) {
+          if (cur >= 0) flush(cur);
           cur = cell;
         }
         if (cell < 0) continue;
-        // The record's (weight, slope) pairs and its m, m v, force-matrix runs are
-        // 2- and 4-element aligned (record stride and offsets are even), so they
-        // are read as vectors: 7 shared loads per particle in float, 9 in double.
+        const R* rr = wrec + qq * kRec;
         using R2 = typename Vec<R>::two;
-        const R* rr = wrec + q * kRec;
         const R2 py = *reinterpret_cast<const R2*>(rr + RW_Y + 2 * qj);
         const R2 pz = *reinterpret_cast<const R2*>(rr + RW_Z + 2 * qk);
-        const R2 px0 = *reinterpret_cast<const R2*>(rr + RW_X + 2 * qi);
-        const R2 px1 = *reinterpret_cast<const R2*>(rr + RW_X + 2 * (qi + 2));
-        const R2 mm0 = *reinterpret_cast<const R2*>(rr + R_M);       // m, m v_x
-        const R2 mm1 = *reinterpret_cast<const R2*>(rr + R_M + 2);   // m v_y, m v_z
-        R2 f0 = {}, f1 = {}, f2 = {};
-        if constexpr (kForce) {
-          f0 = *reinterpret_cast<const R2*>(rr + R_F);      // xx, yy
-          f1 = *reinterpret_cast<const R2*>(rr + R_F + 2);  // zz, xy
-          f2 = *reinterpret_cast<const R2*>(rr + R_F + 4);  // xz, yz
+        const R A = py.x * pz.x;
+        R P[4], U[3], V[3];
+        {
+          const R2 mm0 = *reinterpret_cast<const R2*>(rr + R_M);      // m, m v_x
+          const R2 mm1 = *reinterpret_cast<const R2*>(rr + R_M + 2);  // m v_y, m v_z
+          P[0] = A * mm0.x;
+          P[1] = A * mm0.y;
+          P[2] = A * mm1.x;
+          P[3] = A * mm1.y;
         }
-        const R wy = py.x, dwy = py.y, wz = pz.x, dwz = pz.y;
+        if constexpr (kForce) {
+          const R2 f0 = *reinterpret_cast<const R2*>(rr + R_F);      // xx, yy
+          const R2 f1 = *reinterpret_cast<const R2*>(rr + R_F + 2);  // zz, xy
+          const R2 f2 = *reinterpret_cast<const R2*>(rr + R_F + 4);  // xz, yz
+          const R B = py.y * pz.x, C = py.x * pz.y;
+          const R mxx = f0.x, myy = f0.y, mzz = f1.x, mxy = f1.y, mxz = f2.x, myz = f2.y;
+          U[0] = A * mxx;
+          U[1] = A * mxy;
+          U[2] = A * mxz;
+          V[0] = B * mxy + C * mxz;
+          V[1] = B * myy + C * myz;
+          V[2] = B * myz + C * mzz;
+        }
 #pragma unroll
-        for (int s = 0; s < 2; ++s) {
-          R* acc = s == 0 ? a0 : a1;
-          const R2 px = s == 0 ? px0 : px1;
+        for (int x = 0; x < 2; ++x) {
+          const R2 px = *reinterpret_cast<const R2*>(rr + RW_X + 2 * (qi + 2 * x));
           const R wxv = px.x, dwx = px.y;
-          const R A = wxv * wy;
-          const R w = A * wz;
-          if constexpr (kMass) acc[0] += w * mm0.x;
+          if constexpr (kMass) acc[x][0] += wxv * P[0];
           if constexpr (kMom) {
-            acc[1] += w * mm0.y;
-            acc[2] += w * mm1.x;
-            acc[3] += w * mm1.y;
+            acc[x][1] += wxv * P[1];
+            acc[x][2] += wxv * P[2];
+            acc[x][3] += wxv * P[3];
           }
           if constexpr (kForce) {
-            const R gx = (dwx * wy) * wz, gy = (wxv * dwy) * wz, gz = A * dwz;
-            const R mxx = f0.x, myy = f0.y, mzz = f1.x, mxy = f1.y, mxz = f2.x, myz = f2.y;
-            acc[4] += mxx * gx + mxy * gy + mxz * gz;
-            acc[5] += mxy * gx + myy * gy + myz * gz;
-            acc[6] += mxz * gx + myz * gy + mzz * gz;
+            acc[x][4] += dwx * U[0] + wxv * V[0];
+            acc[x][5] += dwx * U[1] + wxv * V[1];
+            acc[x][6] += dwx * U[2] + wxv * V[2];
           }
         }
       }
-      if (cur >= 0) {
-#pragma unroll
-        for (int c = 0; c < NCH; ++c) {
-          if (c == 0 && !kMass) continue;
-          if (c >= 1 && c <= 3 && !kMom) continue;
-          atomicAdd(&tile[c * kTileN + cur + off0], a0[c]);
-          atomicAdd(&tile[c * kTileN + cur + off1], a1[c]);
-        }
-      }
+      if (cur >= 0) flush(cur);
       __syncwarp();
     }
     __syncthreads();
