@@ -326,7 +326,8 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
                        "mean_latency_s": st["mean_s"], "particle_steps_per_s": st["particle_steps_per_s"],
                        "served_vs_plain_fp64_headline": st["particle_steps_per_s"] / fp64_rate,
                        "peak_concurrent_scenes": st["peak_scenes"], "ticks": st["ticks"],
-                       "wall_s": st["wall_s"], "precision": "mixed"}
+                       "wall_s": st["wall_s"], "precision": "mixed",
+                       "host_phases_s": {"admit": st["admit_s"], "step": st["step_s"], "retire": st["retire_s"]}}
     # -- snowball: error of the mixed form at steps 1, 10, 200
     ball = scenes.snowball_scene()
     a = snow_b200.Batch(snow_b200.SNOW_FP64)

@@ -179,6 +179,10 @@ typedef struct snow_gpu_server snow_gpu_server;
 typedef struct snow_server_stats {
   int64_t completed, rejected, peak_scenes, peak_bytes, ticks, particle_steps;
   double wall_s, p50_s, p99_s, mean_s, particle_steps_per_s;
+  /* host wall time of the loop's phases: admission (upload + setup),
+   * stepping (batched steps, including graph capture after a change of
+   * membership), retirement (download + release) */
+  double admit_s, step_s, retire_s;
 } snow_server_stats;
 int snow_gpu_server_create(snow_gpu_server** out, int precision, int64_t hbm_budget_bytes,
                            int max_scenes, int max_steps_per_tick);

@@ -78,7 +78,74 @@ __global__ void k_planes_to_records(double* rec, int64_t n, const R* r, const do
 
 int64_t pad32(int64_t n) { return (n + 31) / 32 * 32; }
 
+// True for host memory that is page-locked (registered or cudaHostAlloc'd).
+bool page_locked(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 }  // namespace
+
+// Host <-> device copies of particle records.  Page-locked host memory is
+// copied by direct DMA.  Pageable memory goes through two page-locked chunks
+// of kXferChunk bytes: the host copy of one chunk overlaps the DMA of the
+// other, and no pageable copy is left to the driver's own staging.
+void Batch::ensure_pinned() {
+  if (pinned_[0]) return;
+  for (int k = 0; k < 2; ++k) {
+    check_cuda(cudaHostAlloc((void**)&pinned_[k], kXferChunk, cudaHostAllocDefault), "cudaHostAlloc");
+    check_cuda(cudaEventCreateWithFlags(&pinned_ev_[k], cudaEventDisableTiming), "cudaEventCreate");
+  }
+}
+
+void Batch::copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (page_locked(src)) {
+    // the caller may reuse its buffer once the call returns
+    check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "upload copy");
+    check_cuda(cudaStreamSynchronize(s), "upload sync");
+    return;
+  }
+  ensure_pinned();
+  for (size_t off = 0, c = 0; off < bytes; off += kXferChunk, ++c) {
+    const size_t len = std::min(kXferChunk, bytes - off);
+    const int k = (int)(c & 1);
+    check_cuda(cudaEventSynchronize(pinned_ev_[k]), "upload chunk");  // the chunk's last DMA is done
+    std::memcpy(pinned_[k], static_cast<const unsigned char*>(src) + off, len);
+    check_cuda(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, pinned_[k], len, cudaMemcpyHostToDevice, s),
+               "upload copy");
+    check_cuda(cudaEventRecord(pinned_ev_[k], s), "upload chunk");
+  }
+}
+
+void Batch::copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (page_locked(dst)) {
+    check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "download copy");
+    check_cuda(cudaStreamSynchronize(s), "download sync");
+    return;
+  }
+  ensure_pinned();
+  const size_t chunks = (bytes + kXferChunk - 1) / kXferChunk;
+  auto issue = [&](size_t c) {
+    const size_t off = c * kXferChunk, len = std::min(kXferChunk, bytes - off);
+    const int k = (int)(c & 1);
+    check_cuda(cudaMemcpyAsync(pinned_[k], static_cast<const unsigned char*>(src) + off, len,
+                               cudaMemcpyDeviceToHost, s),
+               "download copy");
+    check_cuda(cudaEventRecord(pinned_ev_[k], s), "download chunk");
+  };
+  if (chunks) issue(0);
+  for (size_t c = 0; c < chunks; ++c) {
+    if (c + 1 < chunks) issue(c + 1);
+    const size_t off = c * kXferChunk, len = std::min(kXferChunk, bytes - off);
+    const int k = (int)(c & 1);
+    check_cuda(cudaEventSynchronize(pinned_ev_[k]), "download chunk");
+    std::memcpy(static_cast<unsigned char*>(dst) + off, pinned_[k], len);
+  }
+}
 
 // ---------------------------------------------------------------- Batch impl
 Batch::Batch(int precision) : prec_(precision) {
@@ -103,6 +170,14 @@ Batch::~Batch() {
   free_bins();
   dfree(staging_);
   dfree(d_tmp_scene_);
+  for (auto& c : cache_) free_scene(c);
+  for (int k = 0; k < 2; ++k) {
+    if (pinned_ev_[k]) {
+      cudaEventSynchronize(pinned_ev_[k]);
+      cudaEventDestroy(pinned_ev_[k]);
+    }
+    if (pinned_[k]) cudaFreeHost(pinned_[k]);
+  }
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
@@ -209,10 +284,28 @@ int32_t Batch::add_scene(const double* records, int64_t n, const snow_step_param
   sc->sid = next_id_++;
   sc->n = n;
   sc->stride = pad32(std::max<int64_t>(n, 1));
-  for (int k = 0; k < 2; ++k) {
-    sc->r[k] = dalloc<unsigned char>((size_t)sc->stride * kRealPlanes * rsize_);
-    sc->fp[k] = dalloc<double>((size_t)sc->stride * kFPPlanes);
-    sc->id[k] = dalloc<int32_t>((size_t)sc->stride);
+  // reuse the smallest cached buffer set that fits (at most twice the size)
+  int best = -1;
+  for (int c = 0; c < (int)cache_.size(); ++c)
+    if (cache_[c].stride >= sc->stride && cache_[c].stride <= 2 * sc->stride &&
+        (best < 0 || cache_[c].stride < cache_[best].stride))
+      best = c;
+  if (best >= 0) {
+    Scene& c = cache_[best];
+    cached_bytes_ -= scene_bytes(c.stride);
+    sc->stride = c.stride;
+    for (int k = 0; k < 2; ++k) {
+      sc->r[k] = c.r[k];
+      sc->fp[k] = c.fp[k];
+      sc->id[k] = c.id[k];
+    }
+    cache_.erase(cache_.begin() + best);
+  } else {
+    for (int k = 0; k < 2; ++k) {
+      sc->r[k] = dalloc<unsigned char>((size_t)sc->stride * kRealPlanes * rsize_);
+      sc->fp[k] = dalloc<double>((size_t)sc->stride * kFPPlanes);
+      sc->id[k] = dalloc<int32_t>((size_t)sc->stride);
+    }
   }
   sc->params = *params;
   set_colliders(*sc, colliders, n_colliders);
@@ -247,7 +340,25 @@ void Batch::remove_scene(int32_t id) {
   for (size_t k = 0; k < scenes_.size(); ++k)
     if (scenes_[k]->sid == id) {
       cudaDeviceSynchronize();
-      free_scene(*scenes_[k]);
+      // keep the buffers for a later scene (serving admits and retires scenes
+      // continuously); the cache holds at most kSceneCacheBytes
+      Scene c;
+      c.stride = scenes_[k]->stride;
+      for (int b = 0; b < 2; ++b) {
+        c.r[b] = scenes_[k]->r[b];
+        c.fp[b] = scenes_[k]->fp[b];
+        c.id[b] = scenes_[k]->id[b];
+        scenes_[k]->r[b] = nullptr;
+        scenes_[k]->fp[b] = nullptr;
+        scenes_[k]->id[b] = nullptr;
+      }
+      cache_.push_back(c);
+      cached_bytes_ += scene_bytes(c.stride);
+      while (cached_bytes_ > kSceneCacheBytes && !cache_.empty()) {
+        cached_bytes_ -= scene_bytes(cache_.front().stride);
+        free_scene(cache_.front());
+        cache_.erase(cache_.begin());
+      }
       scenes_.erase(scenes_.begin() + k);
       dirty_ = true;
       return;
@@ -269,9 +380,7 @@ void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s)
   if (n != sc->n) throw Error(SNOW_E_ARG, "upload: particle count differs from the scene's");
   if (n == 0) return;
   ensure_staging(n);
-  check_cuda(cudaMemcpyAsync(staging_, records, (size_t)n * 26 * sizeof(double),
-                             cudaMemcpyHostToDevice, s),
-             "upload copy");
+  copy_in(staging_, records, (size_t)n * 26 * sizeof(double), s);
   const unsigned g = (unsigned)((n + 255) / 256);
   if (prec_ == SNOW_FP64)
     k_records_to_planes<double><<<g, 256, 0, s>>>(staging_, n, (double*)sc->r[sc->cur],
@@ -297,10 +406,7 @@ void Batch::download(int32_t id, double* records, int64_t n, cudaStream_t s) {
     k_planes_to_records<float><<<g, 256, 0, s>>>(staging_, n, (const float*)sc->r[sc->cur],
                                                   sc->fp[sc->cur], sc->id[sc->cur], sc->stride);
   check_cuda(cudaGetLastError(), "download kernel");
-  check_cuda(cudaMemcpyAsync(records, staging_, (size_t)n * 26 * sizeof(double),
-                             cudaMemcpyDeviceToHost, s),
-             "download copy");
-  check_cuda(cudaStreamSynchronize(s), "download sync");
+  copy_out(records, staging_, (size_t)n * 26 * sizeof(double), s);
 }
 
 SceneDev Batch::scene_dev(const Scene& sc, int64_t begin) const {
@@ -727,6 +833,7 @@ int64_t Batch::device_bytes() const {
   b += (int64_t)cap_items_ * (int64_t)sizeof(BlockHeader);
   b += cap_bins_ * 8 + cap_bins_ / 64 * 5 + (cap_bins_ / kBinTile + 1) * 8;
   b += staging_cap_ * 208;
+  b += cached_bytes_;
   return b;
 }
 

@@ -108,6 +108,12 @@ class Batch {
   void free_grid();
   void drop_graph();
   void ensure_staging(int64_t n);
+  void ensure_pinned();
+  void copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s);
+  void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);
+  int64_t scene_bytes(int64_t stride) const {
+    return 2 * stride * (kRealPlanes * (int64_t)rsize_ + kFPPlanes * 8 + 4);
+  }
   void ensure_particle_buffers(int64_t total);
   void ensure_grid(int64_t blocks);
   void ensure_items();
@@ -166,6 +172,13 @@ class Batch {
 
   double* staging_ = nullptr;
   int64_t staging_cap_ = 0;
+  static constexpr size_t kXferChunk = size_t(16) << 20;
+  unsigned char* pinned_[2] = {nullptr, nullptr};
+  cudaEvent_t pinned_ev_[2] = {nullptr, nullptr};
+  // particle buffers of removed scenes, reused by later scenes
+  static constexpr int64_t kSceneCacheBytes = int64_t(8) << 30;
+  std::vector<Scene> cache_;
+  int64_t cached_bytes_ = 0;
 
   cudaGraphExec_t gexec_ = nullptr;
   BatchDev graph_args_{};

@@ -87,6 +87,7 @@ class Server {
     auto now = [&] { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
     while (!pending.empty() || !live.empty()) {
       // admit every arrived request that fits, in arrival order
+      double t_phase = now();
       while (!pending.empty() && pending.front()->arrival <= now()) {
         Request* r = pending.front();
         if (r->bytes > budget_) {  // can never fit
@@ -108,8 +109,11 @@ class Server {
         peak_scenes_ = std::max<int64_t>(peak_scenes_, (int64_t)live.size());
         peak_bytes_ = std::max(peak_bytes_, used);
       }
+      admit_s_ += now() - t_phase;
       // retire scenes with nothing left to do (zero-step requests)
+      t_phase = now();
       retire(live, used, now, s, true);
+      retire_s_ += now() - t_phase;
       if (live.empty()) {
         if (!pending.empty()) {
           const double wait = pending.front()->arrival - now();
@@ -119,13 +123,17 @@ class Server {
       }
       int64_t k = max_tick_;
       for (Request* r : live) k = std::min(k, r->remaining);
+      t_phase = now();
       batch_.step((int)k, nullptr, s);
+      step_s_ += now() - t_phase;
       ++ticks_;
       for (Request* r : live) {
         r->remaining -= k;
         particle_steps_ += k * ((int64_t)r->records.size() / 26);
       }
+      t_phase = now();
       retire(live, used, now, s, false);
+      retire_s_ += now() - t_phase;
     }
     wall_ += now();
   }
@@ -158,6 +166,9 @@ class Server {
     st->p99_s = pct(0.99);
     st->mean_s = lat.empty() ? 0.0 : std::accumulate(lat.begin(), lat.end(), 0.0) / lat.size();
     st->particle_steps_per_s = wall_ > 0 ? particle_steps_ / wall_ : 0.0;
+    st->admit_s = admit_s_;
+    st->step_s = step_s_;
+    st->retire_s = retire_s_;
   }
 
  private:
@@ -185,7 +196,7 @@ class Server {
   int64_t max_tick_;
   std::vector<std::unique_ptr<Request>> reqs_;
   int64_t rejected_ = 0, peak_scenes_ = 0, peak_bytes_ = 0, ticks_ = 0, particle_steps_ = 0;
-  double wall_ = 0.0;
+  double wall_ = 0.0, admit_s_ = 0.0, step_s_ = 0.0, retire_s_ = 0.0;
 };
 
 }  // namespace snow

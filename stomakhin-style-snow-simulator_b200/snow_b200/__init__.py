@@ -65,7 +65,8 @@ class StepTimings(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("completed", "rejected", "peak_scenes", "peak_bytes", "ticks",
                                                "particle_steps")] + \
-               [(n, ctypes.c_double) for n in ("wall_s", "p50_s", "p99_s", "mean_s", "particle_steps_per_s")]
+               [(n, ctypes.c_double) for n in ("wall_s", "p50_s", "p99_s", "mean_s", "particle_steps_per_s",
+                                                "admit_s", "step_s", "retire_s")]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
