@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tori", choices=["tori", "cube", "snowball"])
+    ap.add_argument("--workload", default="tori", choices=["tori", "cube", "snowball", "batch"],
+                    help="batch: the 256 independent scenes, split across ranks by work (strong scaling)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -100,8 +101,41 @@ def cpu_rate(sc, max_steps: int, budget_s: float = REF_SAMPLE_S):
     return sc.n * steps / wall, steps, wall, kind, what
 
 
+def cpu_rate_batch(scs, budget_s: float = REF_SAMPLE_S):
+    """Reference CPU particle-steps/s over the batch scenes: each scene in turn
+    (a few steps each, as one process would step them) until the budget is spent."""
+    lib, kind, what = reference_lib()
+    done_ps, wall, used, steps_each = 0.0, 0.0, 0, 5
+    for sc in scs:
+        rec = lib.setup(sc.particles, sc.dx)
+        rec, ms = lib.step(rec, sc.params(), sc.plane_array(), steps_each)
+        done_ps += sc.n * steps_each
+        wall += ms[10] / 1e3
+        used += 1
+        if wall > budget_s:
+            break
+    return done_ps / wall, steps_each, wall, kind, f"{what}; {used} of {len(scs)} scenes, {steps_each} steps each"
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
+        return
+    if args.workload == "batch":
+        from snow_b200 import scenes
+
+        scs = scenes.batch_scenes(count=256)
+        rate, steps, wall, kind, what = cpu_rate_batch(scs)
+        line = {
+            "impl": "reference", "metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s",
+            "n_gpus": args.gpus, "steps": steps, "warmup": 0, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": "batch-256-scenes", "scenes": len(scs),
+                                                      "particles": sum(x.n for x in scs)},
+            "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": os.cpu_count(), "kind": kind,
+                             "sample": what},
+            "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     sc = workload(args.workload)
     rate, steps, wall, kind, what = cpu_rate(sc, max(1, args.steps))
@@ -175,12 +209,12 @@ def alg_bytes(n_p: int, nodes: int, real: int) -> dict:
 
     p2g reads x, v, m and the 6-entry force matrix (13 `real` values) per
         particle and writes the 7 accumulated channels of every grid node;
-    g2p reads x, v, m, V_p0, F_E (17 `real`) and F_P (9 doubles) per particle and
-        the 6 velocity channels per node, and writes the new state: x, v, m, V_p0,
-        F_E, the next force matrix (23 `real`), F_P and the particle id.
+    g2p reads x, v, m, V_p0, F_E (17 `real`), F_P (9 doubles) and the particle id
+        per particle and the 6 velocity channels per node, and writes the new
+        state: x, v, m, V_p0, F_E, the next force matrix (23 `real`), F_P and the id.
     """
     return {"p2g": n_p * 13 * real + nodes * 7 * real,
-            "g2p": n_p * (17 * real + 72) + nodes * 6 * real + n_p * (23 * real + 72 + 4)}
+            "g2p": n_p * (17 * real + 72 + 4) + nodes * 6 * real + n_p * (23 * real + 72 + 4)}
 
 
 def errors(a, b) -> dict:
@@ -495,11 +529,133 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_batch(args, ws, rank, local):
+    """The 256 independent scenes, split across ranks by work (snow_b200.shard):
+    one batch per rank, one launch per stage, CUDA graph per step, autotuned
+    work-item size; value = all scenes' particle-steps / max-over-ranks time."""
+    import torch
+
+    torch.cuda.set_device(local)
+    import snow_b200
+    from snow_b200 import scenes, shard
+
+    snow_b200.init(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    prec = snow_b200.SNOW_FP64 if args.precision == "fp64" else snow_b200.SNOW_MIXED
+    allsc = scenes.batch_scenes(count=256)
+    total = sum(s.n for s in allsc)
+    mine = [allsc[i] for i in shard.shard([s.n for s in allsc], ws, rank)]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    batch = snow_b200.Batch(prec)
+    ids = [batch.add(s, stream=sp) for s in mine]
+    for i, s in zip(ids, mine):
+        batch.setup(i, s.dx, stream=sp)
+    chunk, _ = batch.autotune(trial_steps=5, stream=sp)
+    batch.step(max(3, args.warmup), stream=sp)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    clocks = Clocks(device_selector(torch, local))
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.step(args.steps, stream=sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    status, blocks, cap = batch.status()
+    launches = batch.graph_kernels() * args.steps
+    kt = batch.step(args.steps, timings=True, stream=sp)
+    per = {k: v / args.steps for k, v in kt.items() if v > 0}
+    real = 8 if args.precision == "fp64" else 4
+    ab = alg_bytes(sum(s.n for s in mine), blocks * 64, real)
+    dom = "g2p" if per.get("stress_update", 0) >= per.get("p2g", 0) else "p2g"
+    dom_ms = per["stress_update"] if dom == "g2p" else per["p2g"]
+    peak, peak_src = measured_peak()
+    achieved = ab[dom] / (dom_ms * 1e-3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        # every step: this rank's scenes uploaded from pinned host records, one
+        # batched step, every scene downloaded
+        hosts = []
+        for i, s in zip(ids, mine):
+            h = torch.empty((s.n, 26), dtype=torch.float64, pin_memory=True).numpy()
+            batch.download(i, h, stream=sp)
+            hosts.append(h)
+        ke = max(3, min(args.steps // 10, 20))
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            for i, h in zip(ids, hosts):
+                batch.upload(i, h, stream=sp)
+            batch.step(1, stream=sp)
+            for i, h in zip(ids, hosts):
+                batch.download(i, h, stream=sp)
+        dt_e = max_over_ranks(time.perf_counter() - t0)
+        nb = sum(s.n for s in mine)
+        e2e = {"value": total * ke / dt_e, "unit": "particle-steps/s", "h2d_bytes_per_step": nb * 208,
+               "d2h_bytes_per_step": nb * 208, "steps": ke,
+               "api": "snow_gpu_batch_upload / _step / _download per step (this rank's bytes)"}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        rate, steps_each, wall, kind, what = cpu_rate_batch(allsc)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": os.cpu_count(), "kind": kind, "sample": what}
+    line = {
+        "metric": "particle-steps/s", "value": total * args.steps / (ms * 1e-3), "unit": "particle-steps/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic: 256 seeded box/sphere scenes, log-uniform 1k..64k particles",
+        "config": {"workload": "batch-256-scenes", "scenes": len(allsc), "particles": total,
+                   "precision": args.precision, "parallelism": f"scene shards x{ws}" if ws > 1 else "single GPU",
+                   "rank0_scenes": len(mine), "work_item": chunk,
+                   "l2": "particle state > 126 MB L2 (no flush needed)", "graph": "CUDA graph per step"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src, "alg_bytes_per_launch": ab[dom],
+                     "launch_ms": dom_ms, "traffic": None},
+        "stages_ms_per_step": per, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk, "grid_blocks": {"used": blocks, "capacity": cap}, "status": status,
+    }
+    batch.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, ws, rank)
+    elif args.workload == "batch":
+        run_batch(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 
