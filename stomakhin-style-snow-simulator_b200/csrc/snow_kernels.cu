@@ -55,11 +55,24 @@ struct Vec<double> {
   using two = double2;
 };
 
-// 7 x 7 x 7 node tile of a block and its +{0,1}^3 neighbours.  Strides 9 (y)
-// and 68 (z) put the 16 (y, z) columns a warp's lanes own in P2G on distinct
-// shared-memory banks for 4- and 8-byte elements.
-constexpr int kTileN = 476;
-SNOW_HD int tile_index(int x, int y, int z) { return x + 9 * y + 68 * z; }
+// 7 x 7 x 7 node tile of a block and its +{0,1}^3 neighbours, x fastest.  The
+// y and z strides put the 32 nodes a warp's lanes own in one P2G atomic
+// (x in {0,1} + 2k, all (y, z) columns) on 32 distinct banks for float, and
+// each half-warp's 16 on distinct 8-byte bank pairs for double.
+template <typename R>
+struct TileShape;
+template <>
+struct TileShape<float> {
+  static constexpr int Y = 8, Z = 58, N = 408;
+};
+template <>
+struct TileShape<double> {
+  static constexpr int Y = 9, Z = 68, N = 470;
+};
+template <typename R>
+SNOW_HD int tile_index(int x, int y, int z) {
+  return x + TileShape<R>::Y * y + TileShape<R>::Z * z;
+}
 
 __device__ __forceinline__ const uint32_t* sorted_keys(const BatchDev& b) {
   const uint32_t passes = (b.ctr->sort_bits + kRadixBits - 1) / kRadixBits;
@@ -658,11 +671,12 @@ struct ItemQueue {
 
 // Tile position of local node `node` (0..63) of neighbour d; false if outside
 // the 7x7x7 region a particle block's stencils can reach.
+template <typename R>
 __device__ __forceinline__ bool tile_of(int d, int node, int& t) {
   const int x = 4 * (d & 1) + (node & 3);
   const int y = 4 * ((d >> 1) & 1) + ((node >> 2) & 3);
   const int z = 4 * (d >> 2) + (node >> 4);
-  t = tile_index(x, y, z);
+  t = tile_index<R>(x, y, z);
   return x <= 6 && y <= 6 && z <= 6;
 }
 
@@ -686,7 +700,7 @@ constexpr int rec_stride() {
 
 template <typename R, int MODE>
 constexpr size_t p2g_smem() {
-  return sizeof(R) * (P2GChannels<R, MODE>::n * kTileN + kP2GWarps * 32 * rec_stride<R>()) +
+  return sizeof(R) * (P2GChannels<R, MODE>::n * TileShape<R>::N + kP2GWarps * 32 * rec_stride<R>()) +
          sizeof(int) * kP2GWarps * 32;
 }
 
@@ -724,8 +738,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
   constexpr bool kForce = MODE == P2G_FULL || MODE == P2G_PRE || MODE == P2G_FORCE;
   constexpr bool kMass = MODE != P2G_FORCE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][kTileN]
-  R* recs = tile + NCH * kTileN;              // [warps][32][kRec]
+  R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][TileShape<R>::N]
+  R* recs = tile + NCH * TileShape<R>::N;              // [warps][32][kRec]
   int* cells = reinterpret_cast<int*>(recs + kP2GWarps * 32 * kRec);
   __shared__ BlockHeader h;
   R* acc_g = (R*)b.acc;
@@ -734,13 +748,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
   R* wrec = recs + warp * 32 * kRec;
   int* wcell = cells + warp * 32;
   const int qi = lane >> 4, qj = (lane >> 2) & 3, qk = lane & 3;
-  const int col = tile_index(0, qj, qk);
+  const int col = tile_index<R>(0, qj, qk);
 
   __shared__ int s_item;
   ItemQueue q;
   q.fetch(b, &b.ctr->work_p2g, min(b.ctr->n_items, (uint32_t)b.cap_items));
   while (q.claim(b, &b.ctr->work_p2g, h, s_item)) {
-    for (int e = threadIdx.x; e < NCH * kTileN; e += blockDim.x) tile[e] = R(0);
+    for (int e = threadIdx.x; e < NCH * TileShape<R>::N; e += blockDim.x) tile[e] = R(0);
     __syncthreads();
     const SceneDev& sc = b.scenes[h.scene];
     const R dx = (R)sc.dx;
@@ -797,7 +811,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
         store_record(wrec + lane * kRec, v);
         const bool inside = (unsigned)tx <= 3u && (unsigned)ty <= 3u && (unsigned)tz <= 3u;
         if (!inside) flag(b, ST_OUT_OF_BOX);  // non-finite or mis-sorted: never index the tile with it
-        wcell[lane] = inside ? tile_index(tx, ty, tz) : -1;
+        wcell[lane] = inside ? tile_index<R>(tx, ty, tz) : -1;
       }
       __syncwarp();
       const int cnt = min(32, n - base);
@@ -813,7 +827,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
           for (int c = 0; c < NCH; ++c) {
             if (c == 0 && !kMass) continue;
             if (c >= 1 && c <= 3 && !kMom) continue;
-            atomicAdd(&tile[c * kTileN + at + col + qi + 2 * x], acc[x][c]);
+            atomicAdd(&tile[c * TileShape<R>::N + at + col + qi + 2 * x], acc[x][c]);
             acc[x][c] = R(0);
           }
       };
@@ -877,17 +891,17 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
     for (int e = threadIdx.x; e < 8 * 64; e += blockDim.x) {
       const int d = e >> 6, node = e & 63;
       int t;
-      if (!tile_of(d, node, t)) continue;
+      if (!tile_of<R>(d, node, t)) continue;
       const int32_t nb = h.nbr[d];
       if (nb < 0) continue;
       const int64_t g = (int64_t)nb * 64 + node;
       bool any = false;
 #pragma unroll
-      for (int ch = 0; ch < NCH; ++ch) any |= tile[ch * kTileN + t] != R(0);
+      for (int ch = 0; ch < NCH; ++ch) any |= tile[ch * TileShape<R>::N + t] != R(0);
       if (!any) continue;
 #pragma unroll
       for (int ch = 0; ch < NCH; ++ch) {
-        const R v = tile[ch * kTileN + t];
+        const R v = tile[ch * TileShape<R>::N + t];
         if (v != R(0)) atomicAdd(&acc_g[ch * plane + g], v);
       }
     }
@@ -1003,14 +1017,46 @@ __device__ __forceinline__ Sym3<R> next_force(const M3<R>& FE, const Plastic<R>&
   return assemble_force<R>(gram_rows(FE), pl.root, det3(FE), V0, (R)sc.mu0, (R)sc.lambda0, (R)hard);
 }
 
+// Node-major G2P tile: the channels of one node are adjacent, so a full-mode
+// gather reads each node with two 16-byte loads in float (6 channels padded to
+// 8) and three in double.
+template <typename R, int MODE>
+struct G2PTile {
+  static constexpr int NCH = G2PChannels<MODE>::n;
+  static constexpr int NS = NCH == 6 ? (sizeof(R) == 4 ? 8 : 6) : NCH;  // node stride
+  static constexpr int size() { return TileShape<R>::N * NS; }
+};
+
+template <typename R, int MODE>
+__device__ __forceinline__ void load_node(const R* tile, int t, R (&f)[G2PChannels<MODE>::n]) {
+  using T = G2PTile<R, MODE>;
+  const R* p = tile + t * T::NS;
+  if constexpr (T::NCH == 6 && sizeof(R) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    const float2 c = *reinterpret_cast<const float2*>(p + 4);
+    f[0] = a.x, f[1] = a.y, f[2] = a.z, f[3] = a.w, f[4] = c.x, f[5] = c.y;
+  } else if constexpr (T::NCH == 6) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double2 a = *reinterpret_cast<const double2*>(p + 2 * k);
+      f[2 * k] = a.x;
+      f[2 * k + 1] = a.y;
+    }
+  } else {
+#pragma unroll
+    for (int ch = 0; ch < T::NCH; ++ch) f[ch] = p[ch];
+  }
+}
+
 template <typename R, int MODE>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const BatchDev b) {
   constexpr int NCH = G2PChannels<MODE>::n;
+  constexpr int NS = G2PTile<R, MODE>::NS;
   constexpr bool kGrad = MODE == G2P_FULL || MODE == G2P_STRESS;
   constexpr bool kVel = MODE == G2P_FULL || MODE == G2P_VELOCITY;
   constexpr bool kDeferDouble = MODE == G2P_FULL && !std::is_same<R, double>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][kTileN]
+  R* tile = reinterpret_cast<R*>(smem_raw);  // [TileShape<R>::N][NS]
   __shared__ BlockHeader h;
   const R* vel = (const R*)b.vel;
   const R* acc = (const R*)b.acc;
@@ -1026,15 +1072,26 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
     for (int e = threadIdx.x; e < 8 * 64; e += blockDim.x) {
       const int d = e >> 6, node = e & 63;
       int t;
-      if (!tile_of(d, node, t)) continue;
+      if (!tile_of<R>(d, node, t)) continue;
       const int32_t nb = h.nbr[d];
       const int64_t g = (int64_t)(nb < 0 ? 0 : nb) * 64 + node;
+      R v[NCH];
 #pragma unroll
       for (int ch = 0; ch < NCH; ++ch) {
-        R v;
-        if constexpr (MODE == G2P_VOLUME) v = acc[g];
-        else v = vel[ch * plane + g];
-        tile[ch * kTileN + t] = nb < 0 ? R(0) : v;
+        if constexpr (MODE == G2P_VOLUME) v[ch] = acc[g];
+        else v[ch] = vel[ch * plane + g];
+        if (nb < 0) v[ch] = R(0);
+      }
+      R* dst = tile + t * NS;
+      if constexpr (NCH == 6 && sizeof(R) == 4) {
+        reinterpret_cast<float4*>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float2*>(dst)[2] = make_float2(v[4], v[5]);
+      } else if constexpr (NCH == 6) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) reinterpret_cast<double2*>(dst)[k] = make_double2(v[2 * k], v[2 * k + 1]);
+      } else {
+#pragma unroll
+        for (int ch = 0; ch < NCH; ++ch) dst[ch] = v[ch];
       }
     }
     __syncthreads();
@@ -1073,7 +1130,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               const R w = wx.w[a] * wy.w[c] * wz.w[e];
-              density += (tile[tile_index(tx + a, ty + c, tz + e)] * w) / (R)dx3;
+              density += (tile[tile_index<R>(tx + a, ty + c, tz + e) * NS] * w) / (R)dx3;
             }
         R* rw = (R*)sc.r[cur];
         rw[PVOL * sc.stride + i] = pv.at(PM, i) / density;
@@ -1099,12 +1156,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
             for (int ch = 0; ch < 3; ++ch) T[ch] = R(0);
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-              const int t = tile_index(tx + a, ty + c, tz + e);
+              R f[NCH];
+              load_node<R, MODE>(tile, tile_index<R>(tx + a, ty + c, tz + e), f);
 #pragma unroll
               for (int ch = 0; ch < NCH; ++ch) {
-                const R f = tile[ch * kTileN + t];
-                S[ch] += wz.w[e] * f;
-                if (kGrad && ch < 3) T[ch] += wz.dw[e] * f;
+                S[ch] += wz.w[e] * f[ch];
+                if (kGrad && ch < 3) T[ch] += wz.dw[e] * f[ch];
               }
             }
 #pragma unroll
@@ -1134,13 +1191,58 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
           }
         }
         const R dt = (R)sc.dt;
+        R vn[3];
+        if constexpr (kVel) {
+          // G2P (grid.cpp:321-324)
+          const R alpha = (R)sc.alpha;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const R vflip = pv.at(PV + a, i) + dflip[a];
+            vn[a] = (R(1) - alpha) * vpic[a] + alpha * vflip;
+          }
+        }
+        if constexpr (MODE == G2P_VELOCITY) {
+          R* rw = (R*)sc.r[cur];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) rw[(PV + a) * sc.stride + i] = vn[a];
+          continue;
+        }
+        const int64_t o = j - sc.begin;  // block-sorted slot in the other buffer
+        const int64_t st = sc.stride;
+        R V0 = R(0);
+        if constexpr (MODE == G2P_FULL) {
+          // particle_collisions (grid.cpp:327-333), position_update (grid.cpp:335-338);
+          // the kinematic part of the new state is written before the stress
+          // update so that its registers are free for the projection
+          for (int c = 0; c < sc.coll_count; ++c)
+            collide(b.colliders[sc.coll_begin + c], x[0], x[1], x[2], vn[0], vn[1], vn[2]);
+          R* rw = (R*)sc.r[cur ^ 1];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const R xn = x[a] + dt * vn[a];
+            rw[(PX + a) * st + o] = xn;
+            rw[(PV + a) * st + o] = vn[a];
+            if (isfinite((double)xn)) {
+              int cell;
+              const int bc = block_coord(xn, dx, cell);
+              bmin[a] = min(bmin[a], bc);
+              bmax[a] = max(bmax[a], bc);
+            } else {
+              flag(b, ST_NONFINITE);
+            }
+          }
+          V0 = pv.at(PVOL, i);
+          rw[PM * st + o] = pv.at(PM, i);
+          rw[PVOL * st + o] = V0;
+          sc.id[cur ^ 1][o] = pv.id[i];
+        }
+        // stress_update (grid.cpp:277-285)
         M3<R> FEn, trial;
         M3<double> FPn;
         Plastic<R> pl;
         bool needs_double = false;
         (void)trial;
-        if constexpr (kGrad) {
-          // stress_update (grid.cpp:277-285)
+        {
           M3<R> FE, L;
 #pragma unroll
           for (int e = 0; e < 9; ++e) {
@@ -1151,43 +1253,33 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
           L.a[4] += R(1);
           L.a[8] += R(1);
           FEn = mat_mul(L, FE);
-          if constexpr (kDeferDouble) {
-            // Mixed form: a projection that needs double is redone by k_fixup
-            // from the trial F_E, which is kept for it in the output slot.
-            trial = FEn;
-            const R lo = R(1) - (R)sc.theta_c, hi = R(1) + (R)sc.theta_s;
-            pl = plastic_projection(FEn, lo, hi);
-            needs_double = near_critical(pl.sigma, lo, hi, (R)kMixedTau, pl.clamped);
-          } else {
-            bool used_fp64 = false;
-            pl = project(FEn, sc, used_fp64);
-            if constexpr (!std::is_same<R, double>::value) {
-              const unsigned act = __activemask();
-              const unsigned fb = __ballot_sync(act, used_fp64);
-              if (fb && (threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&b.ctr->fp64_projections, (uint32_t)__popc(fb));
-            }
-          }
-#pragma unroll
-          for (int e = 0; e < 9; ++e) FPn.a[e] = pv.fp[e * pv.st + i];
-          if (pl.clamped) {
-            const Sym3<R>& Di = pl.Dinv;
-            M3<double> Dm;
-            const double d[9] = {(double)Di.xx, (double)Di.xy, (double)Di.xz, (double)Di.xy, (double)Di.yy,
-                                 (double)Di.yz, (double)Di.xz, (double)Di.yz, (double)Di.zz};
-#pragma unroll
-            for (int e = 0; e < 9; ++e) Dm.a[e] = d[e];
-            FPn = mat_mul(Dm, FPn);
+        }
+        if constexpr (kDeferDouble) {
+          // Mixed form: a projection that needs double is redone by k_fixup
+          // from the trial F_E, which is kept for it in the output slot.
+          trial = FEn;
+          const R lo = R(1) - (R)sc.theta_c, hi = R(1) + (R)sc.theta_s;
+          pl = plastic_projection(FEn, lo, hi);
+          needs_double = near_critical(pl.sigma, lo, hi, (R)kMixedTau, pl.clamped);
+        } else {
+          bool used_fp64 = false;
+          pl = project(FEn, sc, used_fp64);
+          if constexpr (!std::is_same<R, double>::value) {
+            const unsigned act = __activemask();
+            const unsigned fb = __ballot_sync(act, used_fp64);
+            if (fb && (threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&b.ctr->fp64_projections, (uint32_t)__popc(fb));
           }
         }
-        R vn[3];
-        if constexpr (kVel) {
-          // G2P (grid.cpp:321-324)
-          const R alpha = (R)sc.alpha;
 #pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const R vflip = pv.at(PV + a, i) + dflip[a];
-            vn[a] = (R(1) - alpha) * vpic[a] + alpha * vflip;
-          }
+        for (int e = 0; e < 9; ++e) FPn.a[e] = pv.fp[e * pv.st + i];
+        if (pl.clamped) {
+          const Sym3<R>& Di = pl.Dinv;
+          M3<double> Dm;
+          const double d[9] = {(double)Di.xx, (double)Di.xy, (double)Di.xz, (double)Di.xy, (double)Di.yy,
+                               (double)Di.yz, (double)Di.xz, (double)Di.yz, (double)Di.zz};
+#pragma unroll
+          for (int e = 0; e < 9; ++e) Dm.a[e] = d[e];
+          FPn = mat_mul(Dm, FPn);
         }
         if constexpr (MODE == G2P_STRESS) {
           R* rw = (R*)sc.r[cur];
@@ -1199,32 +1291,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
           }
           continue;
         }
-        if constexpr (MODE == G2P_VELOCITY) {
-          R* rw = (R*)sc.r[cur];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) rw[(PV + a) * sc.stride + i] = vn[a];
-          continue;
-        }
         if constexpr (MODE == G2P_FULL) {
-          // particle_collisions (grid.cpp:327-333), position_update (grid.cpp:335-338)
-          for (int c = 0; c < sc.coll_count; ++c)
-            collide(b.colliders[sc.coll_begin + c], x[0], x[1], x[2], vn[0], vn[1], vn[2]);
-          R xn[3];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) xn[a] = x[a] + dt * vn[a];
-          const R V0 = pv.at(PVOL, i);
           const Sym3<R> Mn = next_force(FEn, pl, FPn, sc, V0);
-          const int64_t o = j - sc.begin;  // block-sorted slot in the other buffer
           R* rw = (R*)sc.r[cur ^ 1];
           double* fw = sc.fp[cur ^ 1];
-          const int64_t st = sc.stride;
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            rw[(PX + a) * st + o] = xn[a];
-            rw[(PV + a) * st + o] = vn[a];
-          }
-          rw[PM * st + o] = pv.at(PM, i);
-          rw[PVOL * st + o] = V0;
 #pragma unroll
           for (int e = 0; e < 9; ++e) {
             rw[(PFE + e) * st + o] = needs_double ? trial.a[e] : FEn.a[e];
@@ -1251,18 +1321,6 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
           rw[(PFM + 3) * st + o] = Mn.xy;
           rw[(PFM + 4) * st + o] = Mn.xz;
           rw[(PFM + 5) * st + o] = Mn.yz;
-          sc.id[cur ^ 1][o] = pv.id[i];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            if (isfinite((double)xn[a])) {
-              int cell;
-              const int bc = block_coord(xn[a], dx, cell);
-              bmin[a] = min(bmin[a], bc);
-              bmax[a] = max(bmax[a], bc);
-            } else {
-              flag(b, ST_NONFINITE);
-            }
-          }
         }
       }
     }
@@ -1439,7 +1497,7 @@ void StepLaunch<R>::zero_grid(const BatchDev& b, cudaStream_t s) {
 }
 template <typename R, int MODE>
 static void launch_g2p(const BatchDev& b, cudaStream_t s) {
-  const size_t smem = sizeof(R) * G2PChannels<MODE>::n * kTileN;
+  const size_t smem = sizeof(R) * G2PTile<R, MODE>::size();
   static int grid = 0;
   if (!grid) {
     set_smem(k_g2p<R, MODE>, smem);
