@@ -394,13 +394,13 @@ def measured_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profile_traffic(workload: str, precision: str):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+def profile_traffic(workload: str, precision: str, kernel: str):
+    """Per-launch DRAM bytes (read + write) of `kernel` from the committed ncu summary."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
-        return t.get(f"{workload}/{precision}")
-    except Exception:
+        return t.get(f"{workload}/{precision}/{kernel}")
+    except (OSError, ValueError):
         return None
 
 
@@ -463,7 +463,7 @@ def run_ours(args, ws, rank, local):
     dom_ms = per["stress_update"] if dom == "g2p" else per["p2g"]
     peak, peak_src = measured_peak()
     achieved = ab[dom] / (dom_ms * 1e-3) / 1e9
-    traffic = profile_traffic(args.workload, args.precision)
+    traffic = profile_traffic(args.workload, args.precision, dom)
 
     # end to end through the drop-in entry point on pinned host records
     e2e = None

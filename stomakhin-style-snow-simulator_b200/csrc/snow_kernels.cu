@@ -1048,6 +1048,73 @@ __device__ __forceinline__ void load_node(const R* tile, int t, R (&f)[G2PChanne
   }
 }
 
+// Full-mode gather in float: a node's 6 channels as three pairs, accumulated
+// with the packed two-wide FMA of sm_100 (__ffma2_rn: two fmaf in one
+// instruction, same rounding), contracted z, then y, then x as in the generic
+// path.  Outputs: grad v (column-major), v_pic, and the FLIP term.
+__device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ void gather_f32(const float* tile, int t0, const AxisWeights<float>& wx,
+                                           const AxisWeights<float>& wy, const AxisWeights<float>& wz,
+                                           float gv[9], float vpic[3], float dflip[3]) {
+  constexpr int Y = TileShape<float>::Y, Z = TileShape<float>::Z;
+  float2 wz2[4], dwz2[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    wz2[e] = splat(wz.w[e]);
+    dwz2[e] = splat(wz.dw[e]);
+  }
+  const float2 zero = make_float2(0.f, 0.f);
+  float2 vp01 = zero, g01 = zero, gy01 = zero, gz01 = zero, df12 = zero;
+  float vp2 = 0.f, df0 = 0.f, g2 = 0.f, gy2 = 0.f, gz2 = 0.f;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    float2 SS01 = zero, SS23 = zero, SS45 = zero, SD01 = zero, TS01 = zero;
+    float SD2 = 0.f, TS2 = 0.f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float2 S01 = zero, S23 = zero, S45 = zero, T01 = zero;
+      float T2 = 0.f;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float* p = tile + (t0 + a + Y * c + Z * e) * 8;
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        const float2 f45 = *reinterpret_cast<const float2*>(p + 4);
+        const float2 f01 = make_float2(q.x, q.y), f23 = make_float2(q.z, q.w);
+        S01 = __ffma2_rn(wz2[e], f01, S01);
+        S23 = __ffma2_rn(wz2[e], f23, S23);
+        S45 = __ffma2_rn(wz2[e], f45, S45);
+        T01 = __ffma2_rn(dwz2[e], f01, T01);
+        T2 = fmaf(wz.dw[e], q.z, T2);
+      }
+      const float2 wy2 = splat(wy.w[c]), dwy2 = splat(wy.dw[c]);
+      SS01 = __ffma2_rn(wy2, S01, SS01);
+      SS23 = __ffma2_rn(wy2, S23, SS23);
+      SS45 = __ffma2_rn(wy2, S45, SS45);
+      SD01 = __ffma2_rn(dwy2, S01, SD01);
+      SD2 = fmaf(wy.dw[c], S23.x, SD2);
+      TS01 = __ffma2_rn(wy2, T01, TS01);
+      TS2 = fmaf(wy.w[c], T2, TS2);
+    }
+    const float2 wx2 = splat(wx.w[a]), dwx2 = splat(wx.dw[a]);
+    vp01 = __ffma2_rn(wx2, SS01, vp01);
+    vp2 = fmaf(wx.w[a], SS23.x, vp2);
+    df0 = fmaf(wx.w[a], SS23.y, df0);
+    df12 = __ffma2_rn(wx2, SS45, df12);
+    g01 = __ffma2_rn(dwx2, SS01, g01);
+    g2 = fmaf(wx.dw[a], SS23.x, g2);
+    gy01 = __ffma2_rn(wx2, SD01, gy01);
+    gy2 = fmaf(wx.w[a], SD2, gy2);
+    gz01 = __ffma2_rn(wx2, TS01, gz01);
+    gz2 = fmaf(wx.w[a], TS2, gz2);
+  }
+  vpic[0] = vp01.x, vpic[1] = vp01.y, vpic[2] = vp2;
+  dflip[0] = df0, dflip[1] = df12.x, dflip[2] = df12.y;
+  gv[0] = g01.x, gv[1] = g01.y, gv[2] = g2;
+  gv[3] = gy01.x, gv[4] = gy01.y, gv[5] = gy2;
+  gv[6] = gz01.x, gv[7] = gz01.y, gv[8] = gz2;
+}
+
 template <typename R, int MODE>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const BatchDev b) {
   constexpr int NCH = G2PChannels<MODE>::n;
@@ -1140,6 +1207,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
         // (grid.cpp:250-276, 295-319), contracted one axis at a time: z, then y, then x.
         R gv[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};  // column-major
         R vpic[3] = {R(0), R(0), R(0)}, dflip[3] = {R(0), R(0), R(0)};
+        if constexpr (std::is_same<R, float>::value && NCH == 6) {
+          gather_f32(tile, tile_index<R>(tx, ty, tz), wx, wy, wz, gv, vpic, dflip);
+        } else {
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
           R SS[NCH], SD[3], TS[3];
@@ -1189,6 +1259,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
               gv[6 + r] += wx.w[a] * TS[r];
             }
           }
+        }
         }
         const R dt = (R)sc.dt;
         R vn[3];
