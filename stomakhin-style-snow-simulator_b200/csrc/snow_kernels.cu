@@ -700,8 +700,7 @@ constexpr int rec_stride() {
 
 template <typename R, int MODE>
 constexpr size_t p2g_smem() {
-  return sizeof(R) * (P2GChannels<R, MODE>::n * TileShape<R>::N + kP2GWarps * 32 * rec_stride<R>()) +
-         sizeof(int) * kP2GWarps * 32;
+  return sizeof(R) * (P2GChannels<R, MODE>::n * TileShape<R>::N + kP2GWarps * 32 * rec_stride<R>());
 }
 
 // Stores a 34-field record with 16-byte stores.
@@ -740,13 +739,11 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][TileShape<R>::N]
   R* recs = tile + NCH * TileShape<R>::N;              // [warps][32][kRec]
-  int* cells = reinterpret_cast<int*>(recs + kP2GWarps * 32 * kRec);
   __shared__ BlockHeader h;
   R* acc_g = (R*)b.acc;
   const int64_t plane = (int64_t)b.cap_blocks * 64;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   R* wrec = recs + warp * 32 * kRec;
-  int* wcell = cells + warp * 32;
   const int qi = lane >> 4, qj = (lane >> 2) & 3, qk = lane & 3;
   const int col = tile_index<R>(0, qj, qk);
 
@@ -763,6 +760,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
     const int n = h.end - h.start;
     for (int base = warp * 32; base < n; base += kP2GWarps * 32) {
       const int p = base + lane;
+      int my_cell = -1;
       if (p < n) {
         const int64_t i = vals[h.start + p];
         const R x0 = pv.at(PX, i), x1 = pv.at(PX + 1, i), x2 = pv.at(PX + 2, i);
@@ -811,7 +809,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
         store_record(wrec + lane * kRec, v);
         const bool inside = (unsigned)tx <= 3u && (unsigned)ty <= 3u && (unsigned)tz <= 3u;
         if (!inside) flag(b, ST_OUT_OF_BOX);  // non-finite or mis-sorted: never index the tile with it
-        wcell[lane] = inside ? tile_index<R>(tx, ty, tz) : -1;
+        my_cell = inside ? tile_index<R>(tx, ty, tz) : -1;
       }
       __syncwarp();
       const int cnt = min(32, n - base);
@@ -831,14 +829,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
             acc[x][c] = R(0);
           }
       };
-      int cur = -1;
-      for (int qq = 0; qq < cnt; ++qq) {
-        const int cell = wcell[qq];  // uniform across the warp
-        if (cell != cur) {
-          if (cur >= 0) flush(cur);
-          cur = cell;
-        }
-        if (cell < 0) continue;
+      // Walk the runs of equal cells (the particles arrive cell-sorted): the
+      // run boundaries come from one ballot, so the inner loop carries no
+      // per-particle cell test.
+      auto add = [&](int qq) {
         const R* rr = wrec + qq * kRec;
         using R2 = typename Vec<R>::two;
         const R2 py = *reinterpret_cast<const R2*>(rr + RW_Y + 2 * qj);
@@ -882,8 +876,23 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
             acc[x][6] += dwx * U[2] + wxv * V[2];
           }
         }
+      };
+      const int prev = __shfl_up_sync(0xffffffffu, my_cell, 1);
+      unsigned starts = __ballot_sync(0xffffffffu, lane < cnt && (lane == 0 || my_cell != prev));
+      while (starts) {
+        const int s0 = __ffs(starts) - 1;
+        starts &= starts - 1;
+        const int e0 = starts ? __ffs(starts) - 1 : cnt;
+        const int cell = __shfl_sync(0xffffffffu, my_cell, s0);
+        if (cell < 0) continue;  // particles outside the tile (flagged above)
+        int qq = s0;
+        for (; qq + 1 < e0; qq += 2) {
+          add(qq);
+          add(qq + 1);
+        }
+        if (qq < e0) add(qq);
+        flush(cell);
       }
-      if (cur >= 0) flush(cur);
       __syncwarp();
     }
     __syncthreads();
