@@ -1057,6 +1057,32 @@ __device__ __forceinline__ void load_node(const R* tile, int t, R (&f)[G2PChanne
   }
 }
 
+// Asynchronous global -> shared copies (cp.async): issued per thread, waited
+// for by the same thread, so they need no barrier.
+__device__ __forceinline__ void cp_async(void* sdst, const void* gsrc, int bytes_4_or_8) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  if (bytes_4_or_8 == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Full-mode G2P: the particle state the update reads after the gather (F_E,
+// F_P, v, m, V_p0, id) is copied into per-thread shared slots as soon as the
+// particle's index is known, so its load latency overlaps the gather.
+constexpr int kG2PThreads = 256;
+template <typename R>
+struct G2PSlots {
+  double fp[9][kG2PThreads];
+  R fe[9][kG2PThreads];
+  R v[3][kG2PThreads];
+  R m[kG2PThreads];
+  R v0[kG2PThreads];
+  int32_t id[kG2PThreads];
+};
+
 // Full-mode gather in float: a node's 6 channels as three pairs, accumulated
 // with the packed two-wide FMA of sm_100 (__ffma2_rn: two fmaf in one
 // instruction, same rounding), contracted z, then y, then x as in the generic
@@ -1133,6 +1159,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
   constexpr bool kDeferDouble = MODE == G2P_FULL && !std::is_same<R, double>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile = reinterpret_cast<R*>(smem_raw);  // [TileShape<R>::N][NS]
+  G2PSlots<R>* slot = reinterpret_cast<G2PSlots<R>*>(smem_raw + sizeof(R) * G2PTile<R, MODE>::size());
+  const int me = threadIdx.x;
   __shared__ BlockHeader h;
   const R* vel = (const R*)b.vel;
   const R* acc = (const R*)b.acc;
@@ -1185,6 +1213,21 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
       const int j = h.start + k;
       const int64_t i = vals[j];
+      if constexpr (MODE == G2P_FULL) {
+        cp_async_wait_all();  // this thread's slot is free again
+        constexpr int rb = (int)sizeof(R);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+          cp_async(&slot->fe[e][me], pv.r + (PFE + e) * pv.st + i, rb);
+          cp_async(&slot->fp[e][me], pv.fp + e * pv.st + i, 8);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) cp_async(&slot->v[a][me], pv.r + (PV + a) * pv.st + i, rb);
+        cp_async(&slot->m[me], pv.r + PM * pv.st + i, rb);
+        cp_async(&slot->v0[me], pv.r + PVOL * pv.st + i, rb);
+        cp_async(&slot->id[me], pv.id + i, 4);
+        cp_async_commit();
+      }
       R x[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) x[a] = pv.at(PX + a, i);
@@ -1271,13 +1314,14 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
         }
         }
         const R dt = (R)sc.dt;
+        if constexpr (MODE == G2P_FULL) cp_async_wait_all();
         R vn[3];
         if constexpr (kVel) {
           // G2P (grid.cpp:321-324)
           const R alpha = (R)sc.alpha;
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
-            const R vflip = pv.at(PV + a, i) + dflip[a];
+            const R vflip = (MODE == G2P_FULL ? slot->v[a][me] : pv.at(PV + a, i)) + dflip[a];
             vn[a] = (R(1) - alpha) * vpic[a] + alpha * vflip;
           }
         }
@@ -1311,10 +1355,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
               flag(b, ST_NONFINITE);
             }
           }
-          V0 = pv.at(PVOL, i);
-          rw[PM * st + o] = pv.at(PM, i);
+          V0 = slot->v0[me];
+          rw[PM * st + o] = slot->m[me];
           rw[PVOL * st + o] = V0;
-          sc.id[cur ^ 1][o] = pv.id[i];
+          sc.id[cur ^ 1][o] = slot->id[me];
         }
         // stress_update (grid.cpp:277-285)
         M3<R> FEn, trial;
@@ -1326,7 +1370,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
           M3<R> FE, L;
 #pragma unroll
           for (int e = 0; e < 9; ++e) {
-            FE.a[e] = pv.at(PFE + e, i);
+            FE.a[e] = MODE == G2P_FULL ? slot->fe[e][me] : pv.at(PFE + e, i);
             L.a[e] = dt * gv[e];
           }
           L.a[0] += R(1);
@@ -1351,7 +1395,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
           }
         }
 #pragma unroll
-        for (int e = 0; e < 9; ++e) FPn.a[e] = pv.fp[e * pv.st + i];
+        for (int e = 0; e < 9; ++e) FPn.a[e] = MODE == G2P_FULL ? slot->fp[e][me] : pv.fp[e * pv.st + i];
         if (pl.clamped) {
           const Sym3<R>& Di = pl.Dinv;
           M3<double> Dm;
@@ -1405,6 +1449,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
       }
     }
   }
+  if constexpr (MODE == G2P_FULL) cp_async_wait_all();
   if (MODE == G2P_FULL && last_scene >= 0) flush_box(b.scenes[last_scene], bmin, bmax);
 }
 
@@ -1577,7 +1622,7 @@ void StepLaunch<R>::zero_grid(const BatchDev& b, cudaStream_t s) {
 }
 template <typename R, int MODE>
 static void launch_g2p(const BatchDev& b, cudaStream_t s) {
-  const size_t smem = sizeof(R) * G2PTile<R, MODE>::size();
+  const size_t smem = sizeof(R) * G2PTile<R, MODE>::size() + (MODE == G2P_FULL ? sizeof(G2PSlots<R>) : 0);
   static int grid = 0;
   if (!grid) {
     set_smem(k_g2p<R, MODE>, smem);
