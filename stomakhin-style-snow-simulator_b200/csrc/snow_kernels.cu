@@ -270,6 +270,9 @@ __global__ void __launch_bounds__(256) k_keys(const BatchDev b) {
     if (!ok) flag(b, ST_OUT_OF_BOX);
     const uint32_t bk = block_key(sc, blk[0], blk[1], blk[2]);
     key = (bk << 6) | (uint32_t)(cell[0] + 4 * cell[1] + 16 * cell[2]);
+    // boxes beyond the 32-bit key range: the step only reports the error, so
+    // every particle gets key 0 (a valid key) and no index goes astray
+    if (b.ctr->status & ST_KEY_OVERFLOW) key = 0;
     b.keys[0][t] = key;
     b.vals[0][t] = (uint32_t)i;
   }
@@ -1396,15 +1399,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
         }
 #pragma unroll
         for (int e = 0; e < 9; ++e) FPn.a[e] = MODE == G2P_FULL ? slot->fp[e][me] : pv.fp[e * pv.st + i];
-        if (pl.clamped) {
-          const Sym3<R>& Di = pl.Dinv;
-          M3<double> Dm;
-          const double d[9] = {(double)Di.xx, (double)Di.xy, (double)Di.xz, (double)Di.xy, (double)Di.yy,
-                               (double)Di.yz, (double)Di.xz, (double)Di.yz, (double)Di.zz};
-#pragma unroll
-          for (int e = 0; e < 9; ++e) Dm.a[e] = d[e];
-          FPn = mat_mul(Dm, FPn);
-        }
+        if (pl.clamped) sym_mul_inplace(pl.Dinv, FPn);
         if constexpr (MODE == G2P_STRESS) {
           R* rw = (R*)sc.r[cur];
           double* fw = sc.fp[cur];
@@ -1473,14 +1468,7 @@ __global__ void __launch_bounds__(256) k_fixup(const BatchDev b) {
       FP.a[k] = fp_old[k * st + i];
     }
     const Plastic<double> pl = plastic_projection(F, 1.0 - sc.theta_c, 1.0 + sc.theta_s);
-    if (pl.clamped) {
-      const Sym3<double>& Di = pl.Dinv;
-      M3<double> Dm;
-      const double d[9] = {Di.xx, Di.xy, Di.xz, Di.xy, Di.yy, Di.yz, Di.xz, Di.yz, Di.zz};
-#pragma unroll
-      for (int k = 0; k < 9; ++k) Dm.a[k] = d[k];
-      FP = mat_mul(Dm, FP);
-    }
+    if (pl.clamped) sym_mul_inplace(pl.Dinv, FP);
     const double hard = exp(sc.xi * (1.0 - det3(FP)));
     const double V0 = (double)rw[PVOL * st + o];
     const Sym3<double> M = pl.regular

@@ -72,6 +72,20 @@ struct Sym3 {
   T xx, yy, zz, xy, xz, yz;
 };
 
+// F <- D F for a symmetric D, column by column in place (the same sums as
+// mat_mul with D written out, with a third of the live registers).
+template <typename T>
+SNOW_HD void sym_mul_inplace(const Sym3<T>& D, M3<double>& F) {
+  const double xx = D.xx, yy = D.yy, zz = D.zz, xy = D.xy, xz = D.xz, yz = D.yz;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double a = F(0, c), b = F(1, c), d = F(2, c);
+    F(0, c) = xx * a + xy * b + xz * d;
+    F(1, c) = xy * a + yy * b + yz * d;
+    F(2, c) = xz * a + yz * b + zz * d;
+  }
+}
+
 // Eigen-decomposition S = Q diag(lam) Q^T of a symmetric 3x3 by cyclic Jacobi
 // rotations (Golub & Van Loan, Matrix Computations, 4th ed., Alg. 8.5.2 with
 // the stable rotation of Alg. 8.5.1).  Converges quadratically; the sweep loop

@@ -1,0 +1,106 @@
+"""Edge cases of the GPU step: empty and single-particle scenes, a particle
+whose position is not finite, and scenes too far apart for the block keys.
+
+An empty scene next to a normal one leaves the normal one exactly as alone
+(FP64, 1e-12: only the order of atomic sums differs); a one-particle scene
+matches the oracle to the FP64 parity bound (1e-10); the error cases end the
+call with the matching status code instead of a wrong result.
+"""
+import numpy as np
+import pytest
+
+from oracle_lib import errors
+
+pytestmark = pytest.mark.gpu
+
+
+def _cube(seed=2, n_side=6, lo=(0.3, 0.3, 0.3)):
+    from snow_b200 import scenes
+
+    rec = scenes.cube(n_side, lo=lo, velocity=(0.2, -1.0, 0.1), seed=seed)
+    return scenes.Scene(rec, dx=0.02, dt=1e-4, steps=5, material=scenes.Material(),
+                        planes=[((0, 0.05, 0), (0, 1, 0), 0.2)])
+
+
+def test_empty_scene_beside_a_normal_one(snow):
+    sc = _cube()
+    rec = snow.setup(sc.particles.copy(), sc.dx)
+    alone = snow.Batch(snow.SNOW_FP64)
+    a = alone.add_scene(rec, sc.params(), sc.planes)
+    alone.step(5)
+    want = alone.download(a)
+    alone.close()
+
+    b = snow.Batch(snow.SNOW_FP64)
+    e0 = b.add_scene(np.zeros((0, 26)), sc.params(), sc.planes)
+    s1 = b.add_scene(rec, sc.params(), sc.planes)
+    e2 = b.add_scene(np.zeros((0, 26)), sc.params(), sc.planes)
+    b.step(5)
+    got = b.download(s1)
+    assert b.download(e0).shape == (0, 26) and b.download(e2).shape == (0, 26)
+    b.close()
+    assert max(errors(got, want).values()) < 1e-12
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_single_particle(snow, oracle, prec):
+    sc = _cube(n_side=1)
+    rec = oracle.setup(sc.particles, sc.dx)
+    want, _ = oracle.step(rec, sc.params(), sc.plane_array(), 10)
+    b = snow.Batch(prec)
+    sid = b.add_scene(rec, sc.params(), sc.planes)
+    b.step(10)
+    got = b.download(sid)
+    b.close()
+    e = errors(got, want)
+    tol = 1e-10 if prec == 0 else 1e-4
+    assert max(e["x"], e["F_E"]) < tol, e
+
+
+def test_nonfinite_position_is_reported(snow):
+    sc = _cube()
+    rec = snow.setup(sc.particles.copy(), sc.dx)
+    rec[7, 1] = np.nan
+    b = snow.Batch(snow.SNOW_FP64)
+    b.add_scene(rec, sc.params(), sc.planes)
+    with pytest.raises(snow.SnowError) as err:
+        b.step(2)
+    assert err.value.code == -4  # SNOW_E_NONFINITE
+    b.close()
+
+
+def test_long_thin_scene_is_stepped(snow, oracle):
+    """A particle 100 m away along x only: a long box (~1.3e4 blocks), still within the keys."""
+    sc = _cube(n_side=2)
+    rec = oracle.setup(sc.particles, sc.dx)
+    rec[-1, 0] += 100.0
+    want, _ = oracle.step(rec, sc.params(), sc.plane_array(), 3)
+    b = snow.Batch(snow.SNOW_FP64)
+    sid = b.add_scene(rec, sc.params(), sc.planes)
+    b.step(3)
+    got = b.download(sid)
+    b.close()
+    assert max(errors(got, want).values()) < 1e-10
+
+
+def test_scene_beyond_key_range_is_reported(snow):
+    sc = _cube(n_side=2)
+    rec = snow.setup(sc.particles.copy(), sc.dx)
+    rec[-1, 0:3] += 100.0  # one particle 100 m away on every axis: ~2e9 blocks in the scene's box
+    b = snow.Batch(snow.SNOW_FP64)
+    b.add_scene(rec, sc.params(), sc.planes)
+    with pytest.raises(snow.SnowError) as err:
+        b.step(1)
+    assert err.value.code == -5  # SNOW_E_KEYRANGE
+    b.close()
+
+
+def test_zero_steps_leave_state_alone(snow):
+    sc = _cube()
+    rec = snow.setup(sc.particles.copy(), sc.dx)
+    b = snow.Batch(snow.SNOW_FP64)
+    sid = b.add_scene(rec, sc.params(), sc.planes)
+    b.step(0)
+    got = b.download(sid)
+    b.close()
+    assert np.array_equal(got, rec)
