@@ -98,6 +98,7 @@ struct Counters {
   uint32_t n_items;     // (block, chunk) work items of the particle kernels
   uint32_t fp64_projections;  // mixed form: plastic projections redone in double
   uint32_t bin_ticket;  // next tile of the dense-bin scan
+  uint32_t last_blocks, last_fp64;  // n_blocks and fp64_projections of the previous step
 };
 
 struct BatchDev {
@@ -194,6 +195,8 @@ struct StepLaunch {
   static void g2p(const BatchDev& b, int mode, cudaStream_t s);
   static void zero_grid(const BatchDev& b, cudaStream_t s);
   static void finish(const BatchDev& b, cudaStream_t s);
+  // finish, then keyspace for the next step, in one launch
+  static void finish_and_keyspace(const BatchDev& b, cudaStream_t s);
   static void bbox_init(const BatchDev& b, cudaStream_t s);
   static void prepare_force(const BatchDev& b, cudaStream_t s);
   static void fixup(const BatchDev& b, cudaStream_t s);

@@ -526,6 +526,7 @@ BatchDev Batch::dev(SceneDev* scenes, int num_scenes, int64_t total) const {
 // buffer moved (step() compares the launch arguments).
 void Batch::prepare(cudaStream_t s) {
   if (!(dirty_ || boxes_dirty_ || params_dirty_)) return;
+  keyspace_ready_ = false;  // the boxes are measured afresh below
   total_ = 0;
   table_.clear();
   coll_.clear();
@@ -588,7 +589,8 @@ void Batch::launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev) {
     if (ev) cudaEventRecord(ev[k], s);
   };
   mark(0);
-  StepLaunch<R>::keyspace(b, s, false);
+  // the key boxes of this step were prepared by the previous step's last
+  // launch (or by step() before the first one)
   StepLaunch<R>::keys(b, s);
   radix_sort(b, s);
   StepLaunch<R>::blocks(b, s);
@@ -599,7 +601,7 @@ void Batch::launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev) {
   mark(3);
   StepLaunch<R>::g2p(b, G2P_FULL, s);
   StepLaunch<R>::fixup(b, s);
-  StepLaunch<R>::finish(b, s);
+  StepLaunch<R>::finish_and_keyspace(b, s);
   mark(4);
 }
 
@@ -620,6 +622,14 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
       StepLaunch<float>::prepare_force(b, s);
     check_cuda(cudaGetLastError(), "prepare force");
     force_dirty_ = false;
+  }
+  if (!keyspace_ready_) {
+    // key boxes of the first step; every step ends by preparing the next one's
+    if (prec_ == SNOW_FP64)
+      StepLaunch<double>::keyspace(b, s, false);
+    else
+      StepLaunch<float>::keyspace(b, s, false);
+    keyspace_ready_ = true;
   }
   auto one = [&](cudaEvent_t* ev) {
     if (prec_ == SNOW_FP64)
@@ -680,7 +690,7 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
   check_cuda(cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, s), "status");
   check_cuda(cudaStreamSynchronize(s), "step");
   last_status_ = h_ctr_->status;
-  last_blocks_ = (int64_t)h_ctr_->n_blocks;
+  last_blocks_ = (int64_t)h_ctr_->last_blocks;
   last_key_blocks_ = (int64_t)h_ctr_->key_blocks;
   // Keep 2x headroom: grow the grid and the bins before the next call if the
   // last step came close.
@@ -695,6 +705,7 @@ void Batch::check_status() {
   cudaMemset(&d_ctr_->status, 0, sizeof(uint32_t));
   bins_dirty_ = true;  // a step that stopped early may leave counts behind
   boxes_dirty_ = true;
+  keyspace_ready_ = false;
   if (st & ST_BIN_OVERFLOW)
     throw Error(SNOW_E_CAPACITY, "scene key boxes outgrew the dense bins (" + std::to_string(cap_bins_) +
                                      "); the step result is not valid");
@@ -711,6 +722,7 @@ void Batch::check_status() {
 
 // setup() for one scene: a private one-scene view over the batch's buffers.
 void Batch::setup(int32_t id, double dx, cudaStream_t s) {
+  keyspace_ready_ = false;  // setup's own steps reuse the counters
   if (!(dx > 0.0)) throw Error(SNOW_E_ARG, "grid_spacing must be positive");
   Scene* sc = find(id);
   if (sc->n == 0) return;

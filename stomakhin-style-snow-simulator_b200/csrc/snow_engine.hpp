@@ -63,7 +63,7 @@ class Batch {
   }
   uint32_t last_status() const { return last_status_; }
   int64_t last_blocks() const { return last_blocks_; }
-  int64_t last_fp64_projections() const { return prec_ == SNOW_MIXED ? (int64_t)h_ctr_->fp64_projections : 0; }
+  int64_t last_fp64_projections() const { return prec_ == SNOW_MIXED ? (int64_t)h_ctr_->last_fp64 : 0; }
   int64_t capacity_blocks() const { return cap_blocks_; }
   // Particles per P2G/G2P work item (a power of two, 32..1024).
   void set_chunk(int chunk) {
@@ -132,6 +132,7 @@ class Batch {
   bool dirty_ = true, boxes_dirty_ = true, params_dirty_ = false;
   bool use_graphs_ = true;
   bool force_dirty_ = true;  // particles' force matrices must be recomputed
+  bool keyspace_ready_ = false;  // the device holds the next step's key boxes
   int64_t total_ = 0;
   int num_dev_scenes_ = 0;
 

@@ -149,9 +149,14 @@ __global__ void __launch_bounds__(256) k_bbox_init(const BatchDev b) {
 }
 
 // ------------------------------------------------------------------ keyspace
+// kSwap: also swap every scene's particle buffers first (the end of a step:
+// the same launch then prepares the next step's keys).
+template <bool kSwap>
 __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
   __shared__ unsigned long long s_carry;
   __shared__ unsigned long long s_warp[8];
+  if (kSwap)
+    for (int s = threadIdx.x; s < b.num_scenes; s += blockDim.x) b.scenes[s].cur ^= 1;
   if (threadIdx.x == 0) s_carry = 0;
   __syncthreads();
   for (int base = 0; base < b.num_scenes; base += 256) {
@@ -214,6 +219,8 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
       bits += kb;
     }
     Counters* c = b.ctr;
+    c->last_blocks = c->n_blocks;  // what the host reads after the last step
+    c->last_fp64 = c->fp64_projections;
     c->sort_bits = bits;
     c->key_blocks = (uint32_t)min(total, (unsigned long long)UINT32_MAX);
     if (b.dense && total * 64 > (unsigned long long)b.cap_bins) atomicOr(&c->status, ST_BIN_OVERFLOW);
@@ -229,6 +236,19 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
 // Dense bins hold every key of this step's key boxes.
 __device__ __forceinline__ bool bins_fit(const BatchDev& b) {
   return (int64_t)b.ctr->key_blocks * 64 <= b.cap_bins;
+}
+
+// Runs of equal keys among a warp's consecutive lanes (particles arrive
+// nearly sorted, so a warp holds a few long runs): the lane where this lane's
+// run starts and the run's length.  Equal keys in separate runs stay separate
+// runs, which keeps counts and positions consistent.
+__device__ __forceinline__ void key_run(uint32_t key, int lane, int& first, int& len) {
+  const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+  const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || key != prev);
+  const unsigned upto = (2u << lane) - 1u;  // lanes 0..lane (all ones for lane 31)
+  first = 31 - __clz(starts & upto);
+  const unsigned after = starts & ~upto;
+  len = (after ? __ffs(after) - 1 : 32) - first;
 }
 
 // Sort key of every particle (and its index within its scene).  With dense
@@ -277,9 +297,11 @@ __global__ void __launch_bounds__(256) k_keys(const BatchDev b) {
     b.vals[0][t] = (uint32_t)i;
   }
   if (!dense) return;
-  const unsigned peers = __match_any_sync(0xffffffffu, key);
-  if (valid && (threadIdx.x & 31) == __ffs(peers) - 1) {
-    atomicAdd(&b.bins[key], (uint32_t)__popc(peers));
+  const int lane = threadIdx.x & 31;
+  int first, len;
+  key_run(key, lane, first, len);
+  if (valid && lane == first) {
+    atomicAdd(&b.bins[key], (uint32_t)len);
     b.occ[key >> 6] = 1;
   }
 }
@@ -499,7 +521,7 @@ __global__ void __launch_bounds__(256) k_bins(const BatchDev b) {
 }
 
 // Counting-sort scatter (the order of particles with equal keys is that of
-// the warps' atomics; within a warp it follows the input), the occupancy
+// the runs' atomics; within a run it follows the input), the occupancy
 // bytes cleared for the next step, and the neighbour ids of every work item.
 __global__ void __launch_bounds__(256) k_scatter(const BatchDev b) {
   if (!bins_fit(b)) return;
@@ -507,15 +529,15 @@ __global__ void __launch_bounds__(256) k_scatter(const BatchDev b) {
   const int lane = threadIdx.x & 31;
   const bool valid = t < b.total;
   const uint32_t key = valid ? b.keys[0][t] : 0xFFFFFFFFu;
-  const unsigned peers = __match_any_sync(0xffffffffu, key);
-  const int leader = __ffs(peers) - 1;
+  int first, len;
+  key_run(key, lane, first, len);
   uint32_t base = 0;
-  if (valid && lane == leader) {
-    base = atomicAdd(&b.bin_off[key], (uint32_t)__popc(peers));
+  if (valid && lane == first) {
+    base = atomicAdd(&b.bin_off[key], (uint32_t)len);
     b.occ[key >> 6] = 0;
   }
-  base = __shfl_sync(0xffffffffu, base, leader);
-  const uint32_t pos = base + __popc(peers & ((1u << lane) - 1u));
+  base = __shfl_sync(0xffffffffu, base, first);
+  const uint32_t pos = base + (uint32_t)(lane - first);
   if (valid) {
     if (pos < b.total)
       b.vals[1][pos] = b.vals[0][t];
@@ -1553,7 +1575,7 @@ void StepLaunch<R>::bbox_init(const BatchDev& b, cudaStream_t s) {
 }
 template <typename R>
 void StepLaunch<R>::keyspace(const BatchDev& b, cudaStream_t s, bool) {
-  k_keyspace<<<1, 256, 0, s>>>(b);
+  k_keyspace<false><<<1, 256, 0, s>>>(b);
 }
 template <typename R>
 void StepLaunch<R>::keys(const BatchDev& b, cudaStream_t s) {
@@ -1641,6 +1663,10 @@ void StepLaunch<R>::prepare_force(const BatchDev& b, cudaStream_t s) {
 template <typename R>
 void StepLaunch<R>::finish(const BatchDev& b, cudaStream_t s) {
   k_finish<<<1, 256, 0, s>>>(b);
+}
+template <typename R>
+void StepLaunch<R>::finish_and_keyspace(const BatchDev& b, cudaStream_t s) {
+  k_keyspace<true><<<1, 256, 0, s>>>(b);
 }
 
 template struct StepLaunch<double>;
