@@ -159,6 +159,7 @@ Batch::Batch(int precision) : prec_(precision) {
 }
 
 Batch::~Batch() {
+  if (pending_) cudaStreamSynchronize(pending_stream_);
   drop_graph();
   for (auto& s : scenes_) free_scene(*s);
   dfree(d_scenes_);
@@ -337,6 +338,7 @@ void Batch::set_colliders(Scene& sc, const snow_collider* c, int n) {
 }
 
 void Batch::remove_scene(int32_t id) {
+  step_complete();
   for (size_t k = 0; k < scenes_.size(); ++k)
     if (scenes_[k]->sid == id) {
       cudaDeviceSynchronize();
@@ -376,6 +378,7 @@ void Batch::set_params(int32_t id, const snow_step_params* params, const snow_co
 }
 
 void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s) {
+  step_complete();
   Scene* sc = find(id);
   if (n != sc->n) throw Error(SNOW_E_ARG, "upload: particle count differs from the scene's");
   if (n == 0) return;
@@ -394,6 +397,7 @@ void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s)
 }
 
 void Batch::download(int32_t id, double* records, int64_t n, cudaStream_t s) {
+  step_complete();
   Scene* sc = find(id);
   if (n != sc->n) throw Error(SNOW_E_ARG, "download: particle count differs from the scene's");
   if (n == 0) return;
@@ -606,7 +610,36 @@ void Batch::launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev) {
 }
 
 void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
+  step_launch(n_steps, timings, s);
+  step_complete();
+}
+
+// Moves scene `id` of `from` (same precision) into this batch without copying
+// its particles; returns its id here.  The server sets scenes up in a separate
+// batch while this one steps, then moves them in.
+int32_t Batch::adopt_scene(Batch& from, int32_t id) {
+  step_complete();
+  if (from.prec_ != prec_) throw Error(SNOW_E_ARG, "adopt_scene: precisions differ");
+  for (size_t k = 0; k < from.scenes_.size(); ++k)
+    if (from.scenes_[k]->sid == id) {
+      std::unique_ptr<Scene> sc = std::move(from.scenes_[k]);
+      from.scenes_.erase(from.scenes_.begin() + k);
+      from.dirty_ = true;
+      sc->sid = next_id_++;
+      const int32_t sid = sc->sid;
+      scenes_.push_back(std::move(sc));
+      dirty_ = true;
+      force_dirty_ = true;
+      return sid;
+    }
+  throw Error(SNOW_E_STATE, "unknown scene id " + std::to_string(id));
+}
+
+// Launches n_steps steps on stream s without waiting for them; step_complete()
+// waits and checks their status.
+void Batch::step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s) {
   if (n_steps < 0) throw Error(SNOW_E_ARG, "negative step count");
+  if (pending_) step_complete();
   if (n_steps == 0 || scenes_.empty()) return;
   // The legacy NULL stream cannot be captured into a graph: run on the batch's
   // own (blocking) stream instead, which orders itself with NULL-stream work.
@@ -688,7 +721,14 @@ void Batch::step(int n_steps, snow_step_timings* timings, cudaStream_t s) {
   check_cuda(cudaGetLastError(), "step launch");
   for (auto& sc : scenes_) sc->cur ^= (n_steps & 1);
   check_cuda(cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, s), "status");
-  check_cuda(cudaStreamSynchronize(s), "step");
+  pending_ = true;
+  pending_stream_ = s;
+}
+
+void Batch::step_complete() {
+  if (!pending_) return;
+  pending_ = false;
+  check_cuda(cudaStreamSynchronize(pending_stream_), "step");
   last_status_ = h_ctr_->status;
   last_blocks_ = (int64_t)h_ctr_->last_blocks;
   last_key_blocks_ = (int64_t)h_ctr_->key_blocks;
@@ -722,6 +762,7 @@ void Batch::check_status() {
 
 // setup() for one scene: a private one-scene view over the batch's buffers.
 void Batch::setup(int32_t id, double dx, cudaStream_t s) {
+  step_complete();
   keyspace_ready_ = false;  // setup's own steps reuse the counters
   if (!(dx > 0.0)) throw Error(SNOW_E_ARG, "grid_spacing must be positive");
   Scene* sc = find(id);

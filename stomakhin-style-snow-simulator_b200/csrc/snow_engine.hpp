@@ -49,6 +49,9 @@ class Batch {
   void download(int32_t id, double* records, int64_t n, cudaStream_t s);
   void setup(int32_t id, double dx, cudaStream_t s);
   void step(int n_steps, snow_step_timings* timings, cudaStream_t s);
+  void step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s);
+  void step_complete();
+  int32_t adopt_scene(Batch& from, int32_t id);
   int autotune(int trial_steps, double* best_ms, cudaStream_t s);
 
   int scene_count() const { return (int)scenes_.size(); }
@@ -133,6 +136,8 @@ class Batch {
   bool use_graphs_ = true;
   bool force_dirty_ = true;  // particles' force matrices must be recomputed
   bool keyspace_ready_ = false;  // the device holds the next step's key boxes
+  bool pending_ = false;  // steps launched, status not read yet
+  cudaStream_t pending_stream_ = nullptr;
   int64_t total_ = 0;
   int num_dev_scenes_ = 0;
 

@@ -6,7 +6,8 @@
 // passes and the device-memory budget and scene slots allow.  Admitted scenes
 // stay resident; every tick advances all of them together by the same number
 // of steps (one launch per kernel for the whole batch, replayed from a CUDA
-// graph), at most until the next scene finishes.  A finished scene is copied
+// graph), at most until the next scene finishes; requests that arrive are
+// uploaded and set up on a second stream while a tick runs.  A finished scene is copied
 // back, removed, and its latency (arrival to result) recorded.  Scenes do not
 // interact, so each result is the one the scene would get alone.
 #include <algorithm>
@@ -46,8 +47,18 @@ struct Request {
 class Server {
  public:
   Server(int precision, int64_t budget, int max_scenes, int max_tick_steps)
-      : batch_(precision), prec_(precision), budget_(budget), max_scenes_(max_scenes),
+      : batch_(precision), admit_(precision), prec_(precision), budget_(budget), max_scenes_(max_scenes),
         max_tick_(max_tick_steps) {}
+  ~Server() {
+    try {
+      batch_.step_complete();
+    } catch (...) {
+    }
+    if (main_s_) cudaStreamDestroy(main_s_);
+    if (admit_s_stream_) cudaStreamDestroy(admit_s_stream_);
+  }
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
 
   int64_t submit(const double* rec, int64_t n, const snow_step_params* p, const snow_collider* c, int nc,
                  int64_t steps, double arrival) {
@@ -75,19 +86,33 @@ class Server {
     return n * per_particle + grid + (1 << 16);
   }
 
+  // One tick: launch the live scenes' steps, set up newly arrived requests in
+  // a second batch on a second stream while those steps run, wait for the
+  // steps, retire finished scenes, then move the new ones into the live batch
+  // (without copying their particles) for the next tick.
   void run(cudaStream_t s) {
+    if (!s) s = main_stream();
     std::vector<Request*> order;
     for (auto& r : reqs_)
       if (r->finished < 0 && !r->rejected) order.push_back(r.get());
     std::stable_sort(order.begin(), order.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
     std::deque<Request*> pending(order.begin(), order.end());
-    std::vector<Request*> live;
+    std::vector<Request*> live, arriving;
     int64_t used = 0;
     const auto t0 = clock_t_::now();
     auto now = [&] { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
     while (!pending.empty() || !live.empty()) {
-      // admit every arrived request that fits, in arrival order
+      // launch this tick (the steps run while the host admits below)
+      int64_t k = 0;
       double t_phase = now();
+      if (!live.empty()) {
+        k = max_tick_;
+        for (Request* r : live) k = std::min(k, r->remaining);
+        batch_.step_launch((int)k, nullptr, s);
+      }
+      step_s_ += now() - t_phase;
+      // admit every arrived request that fits, in arrival order
+      t_phase = now();
       while (!pending.empty() && pending.front()->arrival <= now()) {
         Request* r = pending.front();
         if (r->bytes > budget_) {  // can never fit
@@ -96,44 +121,46 @@ class Server {
           ++rejected_;
           continue;
         }
-        if (used + r->bytes > budget_ || (int)live.size() >= max_scenes_) break;
+        if (used + r->bytes > budget_ || (int)(live.size() + arriving.size()) >= max_scenes_) break;
         pending.pop_front();
         const int64_t n = (int64_t)r->records.size() / 26;
-        r->scene = batch_.add_scene(r->records.data(), n, &r->params, r->colliders.data(),
-                                    (int)r->colliders.size(), s);
-        batch_.setup(r->scene, r->params.grid_spacing, s);
+        r->scene = admit_.add_scene(r->records.data(), n, &r->params, r->colliders.data(),
+                                    (int)r->colliders.size(), admit_stream());
+        admit_.setup(r->scene, r->params.grid_spacing, admit_stream());
         r->remaining = r->steps;
         r->admitted = now();
         used += r->bytes;
-        live.push_back(r);
-        peak_scenes_ = std::max<int64_t>(peak_scenes_, (int64_t)live.size());
+        arriving.push_back(r);
+        peak_scenes_ = std::max<int64_t>(peak_scenes_, (int64_t)(live.size() + arriving.size()));
         peak_bytes_ = std::max(peak_bytes_, used);
       }
       admit_s_ += now() - t_phase;
-      // retire scenes with nothing left to do (zero-step requests)
-      t_phase = now();
-      retire(live, used, now, s, true);
-      retire_s_ += now() - t_phase;
-      if (live.empty()) {
-        if (!pending.empty()) {
-          const double wait = pending.front()->arrival - now();
-          if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
+      // complete the tick
+      if (k > 0) {
+        t_phase = now();
+        batch_.step_complete();
+        step_s_ += now() - t_phase;
+        ++ticks_;
+        for (Request* r : live) {
+          r->remaining -= k;
+          particle_steps_ += k * ((int64_t)r->records.size() / 26);
         }
-        continue;
-      }
-      int64_t k = max_tick_;
-      for (Request* r : live) k = std::min(k, r->remaining);
-      t_phase = now();
-      batch_.step((int)k, nullptr, s);
-      step_s_ += now() - t_phase;
-      ++ticks_;
-      for (Request* r : live) {
-        r->remaining -= k;
-        particle_steps_ += k * ((int64_t)r->records.size() / 26);
       }
       t_phase = now();
-      retire(live, used, now, s, false);
+      retire(live, used, now, s);
       retire_s_ += now() - t_phase;
+      for (Request* r : arriving) {
+        r->scene = batch_.adopt_scene(admit_, r->scene);
+        live.push_back(r);
+      }
+      arriving.clear();
+      t_phase = now();
+      retire(live, used, now, s);  // zero-step requests
+      retire_s_ += now() - t_phase;
+      if (live.empty() && !pending.empty()) {
+        const double wait = pending.front()->arrival - now();
+        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
+      }
     }
     wall_ += now();
   }
@@ -173,10 +200,10 @@ class Server {
 
  private:
   template <typename Now>
-  void retire(std::vector<Request*>& live, int64_t& used, Now&& now, cudaStream_t s, bool only_zero) {
+  void retire(std::vector<Request*>& live, int64_t& used, Now&& now, cudaStream_t s) {
     for (size_t i = 0; i < live.size();) {
       Request* r = live[i];
-      if (r->remaining > 0 || (only_zero && r->steps != 0)) {
+      if (r->remaining > 0) {
         ++i;
         continue;
       }
@@ -189,7 +216,18 @@ class Server {
     }
   }
 
+  cudaStream_t main_stream() {
+    if (!main_s_) check_cuda(cudaStreamCreateWithFlags(&main_s_, cudaStreamNonBlocking), "cudaStreamCreate");
+    return main_s_;
+  }
+  cudaStream_t admit_stream() {
+    if (!admit_s_stream_) check_cuda(cudaStreamCreateWithFlags(&admit_s_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    return admit_s_stream_;
+  }
+
   Batch batch_;
+  Batch admit_;  // new scenes are set up here while batch_ steps
+  cudaStream_t main_s_ = nullptr, admit_s_stream_ = nullptr;
   int prec_;
   int64_t budget_;
   int max_scenes_;
