@@ -311,7 +311,7 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
         bsteps = max(20, steps // 4)
         ms_b = timed_steps(b, bsteps, sp, torch)
         brates[name] = {"value": nb * bsteps / (ms_b * 1e-3), "ms_per_step": ms_b / bsteps,
-                        "work_item": chunk}
+                        "work_item": chunk, "sort": b.sort_mode()}
         b.close()
     berr = {}
     a = snow_b200.Batch(snow_b200.SNOW_FP64)
@@ -341,7 +341,7 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
                         "mixed_vs_fp64": brates["mixed"]["value"] / brates["fp64"]["value"],
                         "mixed_vs_plain_fp64_headline": brates["mixed"]["value"] / fp64_rate,
                         "mixed_error_vs_fp64_step10_first16": worst,
-                        "graph": "CUDA graph per step", "autotuned": "work-item size"}
+                        "graph": "CUDA graph per step", "autotuned": "work-item size and particle ordering"}
     # -- served: Poisson stream, mixed form
     reqs = scenes.served_requests(count=48, rate=200.0)
     srv = snow_b200.Server(snow_b200.SNOW_MIXED, budget_bytes=150 * 10**9, max_steps_per_tick=16)
@@ -633,7 +633,7 @@ def run_batch(args, ws, rank, local):
         "data": "synthetic: 256 seeded box/sphere scenes, log-uniform 1k..64k particles",
         "config": {"workload": "batch-256-scenes", "scenes": len(allsc), "particles": total,
                    "precision": args.precision, "parallelism": f"scene shards x{ws}" if ws > 1 else "single GPU",
-                   "rank0_scenes": len(mine), "work_item": chunk,
+                   "rank0_scenes": len(mine), "work_item": chunk, "sort": batch.sort_mode(),
                    "l2": "particle state > 126 MB L2 (no flush needed)", "graph": "CUDA graph per step"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src, "alg_bytes_per_launch": ab[dom],

@@ -159,11 +159,18 @@ int snow_gpu_batch_set_dense(snow_gpu_batch* batch, int enable);
 /* Kernels launched by one replay of the batch's captured step graph (0 until
  * a multi-step call captured it).  No reference counterpart. */
 int snow_gpu_batch_graph_kernels(snow_gpu_batch* batch);
+/* Particle ordering in use: 1 counting sort over dense key bins, 0 radix sort
+ * (set by set_dense, the autotuner, or the size of the key boxes).  No
+ * reference counterpart. */
+int snow_gpu_batch_sort_mode(snow_gpu_batch* batch);
 
 /* Autotuner: times `trial_steps` steps of the batch for each work-item size
- * (particles per P2G/G2P CTA work item: 64 ... 1024) on a snapshot of the
- * current state, restores the state, keeps the fastest size and reports it in
- * *chosen (and its ms per step in *ms_per_step).  No reference counterpart. */
+ * (particles per P2G/G2P CTA work item: 64 ... 1024) and each particle
+ * ordering (counting sort over dense key bins, or the radix sort with the
+ * block hash table, unless set_dense(0) ruled the former out) on a snapshot of
+ * the current state, restores the state, keeps the fastest pair and reports
+ * the size in *chosen (and its ms per step in *ms_per_step).  No reference
+ * counterpart. */
 int snow_gpu_batch_autotune(snow_gpu_batch* batch, int trial_steps, int* chosen, double* ms_per_step,
                             void* stream);
 

@@ -847,13 +847,18 @@ int Batch::autotune(int trial_steps, double* best_ms, cudaStream_t s) {
     force_dirty_ = true;
   };
   const int candidates[] = {64, 128, 256, 512, 1024};
+  const bool dense_allowed = want_dense_;
   int best = chunk_;
+  bool best_dense = want_dense_;
   double best_t = 1e300;
   cudaEvent_t e0, e1;
   check_cuda(cudaEventCreate(&e0), "event");
   check_cuda(cudaEventCreate(&e1), "event");
+  for (int m = 0; m < (dense_allowed ? 2 : 1); ++m)
   for (int c : candidates) {
+    const bool dense = dense_allowed && m == 0;
     set_chunk(c);
+    set_dense(dense);
     restore();
     step(2, nullptr, s);
     check_cuda(cudaEventRecord(e0, s), "event");
@@ -865,11 +870,13 @@ int Batch::autotune(int trial_steps, double* best_ms, cudaStream_t s) {
     if (ms < best_t) {
       best_t = ms;
       best = c;
+      best_dense = dense;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   set_chunk(best);
+  set_dense(best_dense);
   restore();
   check_cuda(cudaStreamSynchronize(s), "restore");
   for (auto& sn : snaps) dfree(sn.buf);
@@ -1050,6 +1057,9 @@ int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk) {
     SNOW_BATCH_OR_FAIL;
     batch->impl->set_chunk(chunk);
   });
+}
+int snow_gpu_batch_sort_mode(snow_gpu_batch* batch) {
+  return batch && batch->impl ? (batch->impl->dense() ? 1 : 0) : SNOW_E_ARG;
 }
 int snow_gpu_batch_graph_kernels(snow_gpu_batch* batch) {
   return batch && batch->impl ? batch->impl->graph_kernels() : SNOW_E_ARG;

@@ -125,6 +125,7 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_batch_set_chunk": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_set_dense": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_graph_kernels": (ctypes.c_int, [vp]),
+        "snow_gpu_batch_sort_mode": (ctypes.c_int, [vp]),
         "snow_gpu_setup": (ctypes.c_int, [_dp, i64, d]),
         "snow_gpu_step": (ctypes.c_int, [_dp, i64, ctypes.POINTER(StepParams), ctypes.POINTER(Collider),
                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(StepTimings)]),
@@ -262,6 +263,10 @@ class Batch:
 
     def set_graphs(self, enable: bool) -> None:
         _check(lib().snow_gpu_batch_set_graphs(self._h, int(bool(enable))))
+
+    def sort_mode(self) -> str:
+        """Particle ordering in use: "dense" (counting sort over key bins) or "radix"."""
+        return "dense" if lib().snow_gpu_batch_sort_mode(self._h) == 1 else "radix"
 
     def graph_kernels(self) -> int:
         """Kernel launches in one replay of the captured step graph (0 before capture)."""
