@@ -1,8 +1,9 @@
 // Colliders (reference include/snow/collision.hpp).  CollisionBody keeps the
 // reference's std::function members so that existing code compiles; bodies
-// made by make_plane hold the named functors below, from which the GPU step
-// recovers the plane (any other callable is rejected with
-// std::invalid_argument: a std::function cannot run on the device).
+// made by make_plane (and snow::make_moving_plane, snow::make_sphere) hold the
+// named functors below, from which the GPU step recovers the body (any other
+// callable is rejected with std::invalid_argument: a std::function cannot run
+// on the device).
 #pragma once
 
 #include <functional>
@@ -36,6 +37,26 @@ struct ConstantVelocity
     Eigen::Vector3d value;
     Eigen::Vector3d operator()(const Eigen::Vector3d&) const { return value; }
 };
+// phi(x) = |x - center| - radius of a solid sphere, and its outward normal.
+struct SphereDistance
+{
+    Eigen::Vector3d center;
+    double radius;
+    double operator()(const Eigen::Vector3d& x) const { return (x - center).norm() - radius; }
+};
+struct SphereNormal
+{
+    Eigen::Vector3d center;
+    Eigen::Vector3d operator()(const Eigen::Vector3d& x) const { return (x - center).normalized(); }
+};
+
+// Not in the reference (which takes any CollisionBody): bodies the GPU step
+// can run besides make_plane -- a plane moving with a constant velocity and a
+// solid sphere, resting or moving.
+CollisionBody make_moving_plane(const Eigen::Vector3d& point, const Eigen::Vector3d& normal,
+                                const Eigen::Vector3d& velocity, double friction);
+CollisionBody make_sphere(const Eigen::Vector3d& center, double radius, double friction,
+                          const Eigen::Vector3d& velocity = Eigen::Vector3d::Zero());
 }  // namespace snow
 
 CollisionBody make_plane(const Eigen::Vector3d& point, const Eigen::Vector3d& normal, double friction);

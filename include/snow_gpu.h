@@ -58,11 +58,14 @@ enum {
 };
 
 /* Collider kinds. */
-enum { SNOW_COLLIDER_PLANE = 0 };
+enum { SNOW_COLLIDER_PLANE = 0, SNOW_COLLIDER_SPHERE = 1 };
 
-/* A collider (CollisionBody, include/snow/collision.hpp:6-12).  A plane is
- * the half-space phi(x) = normal . (x - point) <= 0 with unit `normal`; the
- * collider moves with constant `velocity` (zero for make_plane). */
+/* A collider (CollisionBody, include/snow/collision.hpp:6-12; the reference
+ * takes any phi / normal / velocity functions and defines make_plane,
+ * src/collision.cpp:5-27).  A plane is the half-space
+ * phi(x) = normal . (x - point) <= 0 with unit `normal`; a sphere (kind 1) is
+ * the solid ball |x - point| <= param[0] with normal (x - point)/|x - point|.
+ * Either moves with constant `velocity` (zero for make_plane). */
 typedef struct snow_collider {
   int32_t kind;
   int32_t reserved;

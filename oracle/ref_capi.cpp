@@ -43,6 +43,30 @@ std::vector<CollisionBody> planes(const double* q, int n) {
     b.push_back(make_plane({q[0], q[1], q[2]}, {q[3], q[4], q[5]}, q[6]));
   return b;
 }
+// Bodies as n x 12 rows: kind, point[3], normal[3], velocity[3], friction,
+// radius.  A resting plane is the reference's own make_plane; a moving plane
+// and a solid sphere are CollisionBody values with their phi / normal /
+// velocity functions written out, as a user of the reference would.
+std::vector<CollisionBody> bodies(const double* q, int n) {
+  std::vector<CollisionBody> b;
+  for (int i = 0; i < n; ++i, q += 12) {
+    const Eigen::Vector3d p{q[1], q[2], q[3]}, nrm{q[4], q[5], q[6]}, v{q[7], q[8], q[9]};
+    const double mu = q[10], r = q[11];
+    if (q[0] == 1.0) {
+      b.push_back(CollisionBody{[p, r](const Eigen::Vector3d& x) { return (x - p).norm() - r; },
+                                [p](const Eigen::Vector3d& x) { return Eigen::Vector3d((x - p).normalized()); },
+                                [v](const Eigen::Vector3d&) { return v; }, mu});
+    } else if (v[0] == 0.0 && v[1] == 0.0 && v[2] == 0.0) {
+      b.push_back(make_plane(p, nrm, mu));
+    } else {
+      const Eigen::Vector3d u = nrm.normalized();
+      b.push_back(CollisionBody{[p, u](const Eigen::Vector3d& x) { return u.dot(x - p); },
+                                [u](const Eigen::Vector3d&) { return u; },
+                                [v](const Eigen::Vector3d&) { return v; }, mu});
+    }
+  }
+  return b;
+}
 thread_local std::string g_err;
 }  // namespace
 
@@ -55,10 +79,9 @@ void ref_setup(double* rec, int64_t n, double dx) {
 }
 
 // params: gravity[3], dt, dx, mu0, lambda0, xi, theta_c, theta_s, alpha
-void ref_step(double* rec, int64_t n, const double* p, const double* plane_data, int n_planes,
-              int steps, double* stage_ms) {
+static void run(double* rec, int64_t n, const double* p, const std::vector<CollisionBody>& bodies, int steps,
+                double* stage_ms) {
   auto v = to_vec(rec, n);
-  auto bodies = planes(plane_data, n_planes);
   std::vector<ParticleStencil> stencils(v.size());
   StepTimings t;
   const auto t0 = std::chrono::steady_clock::now();
@@ -74,6 +97,15 @@ void ref_step(double* rec, int64_t n, const double* p, const double* plane_data,
     std::memcpy(stage_ms, ms, sizeof ms);
   }
   from_vec(v, rec);
+}
+
+void ref_step(double* rec, int64_t n, const double* p, const double* plane_data, int n_planes,
+              int steps, double* stage_ms) {
+  run(rec, n, p, planes(plane_data, n_planes), steps, stage_ms);
+}
+void ref_step_bodies(double* rec, int64_t n, const double* p, const double* body_rows, int n_bodies,
+                     int steps, double* stage_ms) {
+  run(rec, n, p, bodies(body_rows, n_bodies), steps, stage_ms);
 }
 
 // Two calls: with out == nullptr returns the particle count, else fills `out`

@@ -273,17 +273,33 @@ struct StencilEntry {
 };
 using Stencil = std::array<StencilEntry, 64>;
 
-// Analytic plane collider: make_plane (src/collision.cpp:5-27) stores the unit
-// normal; phi(x) = n.(x - p); collider velocity is zero.
+// Analytic colliders standing for the reference's CollisionBody (phi, normal,
+// velocity functions and a friction coefficient, include/snow/collision.hpp):
+// make_plane (src/collision.cpp:5-27) stores the unit normal, phi(x) = n.(x - p)
+// and zero velocity; the same plane may move with a constant velocity; a solid
+// sphere has phi(x) = |x - c| - r and normal (x - c)/|x - c|.
 struct Plane {
-  Vec3 point, normal;  // normal already normalised
-  double friction;
+  int kind = 0;        // 0 plane, 1 sphere
+  Vec3 point, normal;  // plane: point, unit normal; sphere: centre in `point`
+  double friction = 0.0;
+  Vec3 velocity{0.0, 0.0, 0.0};
+  double radius = 0.0;
 };
-inline Plane make_plane(const Vec3& p, const Vec3& n, double mu) {
+inline Vec3 unit(const Vec3& n) {
   const double len = norm(n);
-  Vec3 u = len > 0.0 ? n / len : n;  // Eigen normalized() leaves a zero vector as is
-  return {p, u, mu};
+  return len > 0.0 ? n / len : n;  // Eigen normalized() leaves a zero vector as is
 }
+inline Plane make_plane(const Vec3& p, const Vec3& n, double mu) {
+  Plane b;
+  b.point = p;
+  b.normal = unit(n);
+  b.friction = mu;
+  return b;
+}
+inline double body_phi(const Plane& b, const Vec3& x) {
+  return b.kind == 1 ? norm(x - b.point) - b.radius : dot(b.normal, x - b.point);
+}
+inline Vec3 body_normal(const Plane& b, const Vec3& x) { return b.kind == 1 ? unit(x - b.point) : b.normal; }
 
 // ------------------------------------------------------------------ kernels
 // N(a, b): cubic B-spline of |a - b| (grid.cpp:24-40).
@@ -399,10 +415,10 @@ void grid_velocity(Grid& grid, const Vec3& g, double dt) {
 
 // collision_helper (grid.cpp:206-231): Coulomb friction against a collider.
 Vec3 collide(const Vec3& x, const Vec3& v, const Plane& b) {
-  const double phi = dot(b.normal, x - b.point);
+  const double phi = body_phi(b, x);
   if (phi <= 0) {
-    const Vec3& n = b.normal;
-    const Vec3 vc{0.0, 0.0, 0.0};
+    const Vec3 n = body_normal(b, x);
+    const Vec3 vc = b.velocity;
     const Vec3 vrel = v - vc;
     const double vn = dot(vrel, n);
     if (vn < 0) {
@@ -570,6 +586,19 @@ std::vector<Plane> to_planes(const double* planes, int n) {
   }
   return b;
 }
+// bodies: n x 12 doubles = kind, point[3], normal[3], velocity[3], friction, radius
+std::vector<Plane> to_bodies(const double* rows, int n) {
+  std::vector<Plane> b;
+  for (int i = 0; i < n; ++i) {
+    const double* q = rows + 12 * i;
+    Plane c = make_plane(Vec3{q[1], q[2], q[3]}, Vec3{q[4], q[5], q[6]}, q[10]);
+    c.kind = (int)q[0];
+    c.velocity = Vec3{q[7], q[8], q[9]};
+    c.radius = q[11];
+    b.push_back(c);
+  }
+  return b;
+}
 struct GridBox {
   Grid g;
 };
@@ -586,12 +615,11 @@ void oracle_setup(double* rec, int64_t n, double dx) {
 }
 
 // params: gravity[3], dt, dx, mu0, lambda0, xi, theta_c, theta_s, alpha (11 doubles)
-void oracle_step(double* rec, int64_t n, const double* params, const double* planes, int n_planes,
-                 int steps, double* stage_ms) {
+static void run_steps(double* rec, int64_t n, const double* params, const std::vector<Plane>& b, int steps,
+                      double* stage_ms) {
   auto v = to_vec(rec, n);
   StepParams p;
   std::memcpy(&p, params, sizeof(StepParams));
-  auto b = to_planes(planes, n_planes);
   std::vector<Stencil> st(v.size());
   double ms[10] = {0};
   const auto t0 = std::chrono::steady_clock::now();
@@ -602,6 +630,16 @@ void oracle_step(double* rec, int64_t n, const double* params, const double* pla
     stage_ms[10] = wall;
   }
   from_vec(v, rec);
+}
+
+void oracle_step(double* rec, int64_t n, const double* params, const double* planes, int n_planes,
+                 int steps, double* stage_ms) {
+  run_steps(rec, n, params, to_planes(planes, n_planes), steps, stage_ms);
+}
+// The same with general bodies (rows as in to_bodies).
+void oracle_step_bodies(double* rec, int64_t n, const double* params, const double* bodies, int n_bodies,
+                        int steps, double* stage_ms) {
+  run_steps(rec, n, params, to_bodies(bodies, n_bodies), steps, stage_ms);
 }
 
 double oracle_N(double a, double b) { return N(a, b); }

@@ -321,8 +321,10 @@ void Batch::set_colliders(Scene& sc, const snow_collider* c, int n) {
   if (n < 0 || (n > 0 && !c)) throw Error(SNOW_E_ARG, "bad collider array");
   sc.colliders.clear();
   for (int i = 0; i < n; ++i) {
-    if (c[i].kind != SNOW_COLLIDER_PLANE)
+    if (c[i].kind != SNOW_COLLIDER_PLANE && c[i].kind != SNOW_COLLIDER_SPHERE)
       throw Error(SNOW_E_ARG, "unsupported collider kind " + std::to_string(c[i].kind));
+    if (c[i].kind == SNOW_COLLIDER_SPHERE && !(c[i].param[0] > 0.0 && std::isfinite(c[i].param[0])))
+      throw Error(SNOW_E_ARG, "sphere collider needs a positive finite radius in param[0]");
     Collider d{};
     d.kind = c[i].kind;
     for (int a = 0; a < 3; ++a) {

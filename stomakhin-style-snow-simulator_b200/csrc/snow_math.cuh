@@ -347,16 +347,30 @@ struct Collider {
   double normal[3];
   double velocity[3];
   double friction;
-  double param[2];  // reserved for other shapes
+  double param[2];  // sphere: param[0] = radius
 };
+enum : int32_t { COLLIDER_PLANE = 0, COLLIDER_SPHERE = 1 };
 
 // collision_helper (grid.cpp:206-231): Coulomb friction, stick when
 // |v_t| <= -mu v_n, else slide.
+// Bodies: a plane phi(x) = n . (x - p) with unit normal n (make_plane,
+// src/collision.cpp:5-27), or a solid sphere phi(x) = |x - c| - r with normal
+// (x - c) / |x - c| (zero at the centre, as Eigen's normalized() leaves it);
+// either moves with the constant velocity v_c.
 template <typename T>
 SNOW_HD void collide(const Collider& b, T x, T y, T z, T& vx, T& vy, T& vz) {
-  const T nx = T(b.normal[0]), ny = T(b.normal[1]), nz = T(b.normal[2]);
-  const T phi = nx * (x - T(b.point[0])) + ny * (y - T(b.point[1])) + nz * (z - T(b.point[2]));
-  if (!(phi <= T(0))) return;
+  T nx, ny, nz;
+  if (b.kind == COLLIDER_SPHERE) {
+    const T ex = x - T(b.point[0]), ey = y - T(b.point[1]), ez = z - T(b.point[2]);
+    const T len = sqrt(ex * ex + ey * ey + ez * ez);
+    if (!(len - T(b.param[0]) <= T(0))) return;
+    const T inv = len > T(0) ? T(1) / len : T(0);
+    nx = ex * inv, ny = ey * inv, nz = ez * inv;
+  } else {
+    nx = T(b.normal[0]), ny = T(b.normal[1]), nz = T(b.normal[2]);
+    const T phi = nx * (x - T(b.point[0])) + ny * (y - T(b.point[1])) + nz * (z - T(b.point[2]));
+    if (!(phi <= T(0))) return;
+  }
   const T cx = T(b.velocity[0]), cy = T(b.velocity[1]), cz = T(b.velocity[2]);
   const T rx = vx - cx, ry = vy - cy, rz = vz - cz;
   const T vn = rx * nx + ry * ny + rz * nz;

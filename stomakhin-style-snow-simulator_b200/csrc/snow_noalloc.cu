@@ -157,7 +157,9 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
     if (!params || !(params->grid_spacing > 0.0)) throw Error(SNOW_E_ARG, "bad step parameters");
     if (n_steps < 0) throw Error(SNOW_E_ARG, "negative step count");
     for (int c = 0; c < n_colliders; ++c)
-      if (colliders[c].kind != SNOW_COLLIDER_PLANE) throw Error(SNOW_E_ARG, "unsupported collider kind");
+      if ((colliders[c].kind != SNOW_COLLIDER_PLANE && colliders[c].kind != SNOW_COLLIDER_SPHERE) ||
+          (colliders[c].kind == SNOW_COLLIDER_SPHERE && !(colliders[c].param[0] > 0.0)))
+        throw Error(SNOW_E_ARG, "unsupported collider");
     if (n == 0 || n_steps == 0) return SNOW_OK;
 
     unsigned char* A = arena_for_current_device();

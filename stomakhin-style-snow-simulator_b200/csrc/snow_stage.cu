@@ -289,8 +289,12 @@ std::vector<Collider> to_colliders(const snow_collider* c, int nc) {
   if (nc < 0 || (nc > 0 && !c)) throw Error(SNOW_E_ARG, "bad collider array");
   std::vector<Collider> out((size_t)nc);
   if (nc) std::memcpy(out.data(), c, sizeof(Collider) * nc);
-  for (auto& x : out)
-    if (x.kind != SNOW_COLLIDER_PLANE) throw Error(SNOW_E_ARG, "unsupported collider kind");
+  for (auto& x : out) {
+    if (x.kind != SNOW_COLLIDER_PLANE && x.kind != SNOW_COLLIDER_SPHERE)
+      throw Error(SNOW_E_ARG, "unsupported collider kind");
+    if (x.kind == SNOW_COLLIDER_SPHERE && !(x.param[0] > 0.0))
+      throw Error(SNOW_E_ARG, "sphere collider needs a positive radius in param[0]");
+  }
   return out;
 }
 

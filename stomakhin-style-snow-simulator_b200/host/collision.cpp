@@ -8,3 +8,20 @@ CollisionBody make_plane(const Eigen::Vector3d& point, const Eigen::Vector3d& no
     return CollisionBody{snow::PlaneDistance{point, unit_normal}, snow::PlaneNormal{unit_normal},
                          snow::ConstantVelocity{Eigen::Vector3d::Zero()}, friction};
 }
+
+namespace snow
+{
+CollisionBody make_moving_plane(const Eigen::Vector3d& point, const Eigen::Vector3d& normal,
+                                const Eigen::Vector3d& velocity, double friction)
+{
+    const Eigen::Vector3d unit_normal = normal.normalized();
+    return CollisionBody{PlaneDistance{point, unit_normal}, PlaneNormal{unit_normal}, ConstantVelocity{velocity},
+                         friction};
+}
+
+CollisionBody make_sphere(const Eigen::Vector3d& center, double radius, double friction,
+                          const Eigen::Vector3d& velocity)
+{
+    return CollisionBody{SphereDistance{center, radius}, SphereNormal{center}, ConstantVelocity{velocity}, friction};
+}
+}  // namespace snow

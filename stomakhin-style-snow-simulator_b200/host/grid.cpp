@@ -320,21 +320,34 @@ std::vector<snow_collider> to_colliders(const std::vector<CollisionBody>& bodies
     std::vector<snow_collider> out;
     for (const CollisionBody& b : bodies)
     {
+        const auto* vel = b.velocity.target<snow::ConstantVelocity>();
         const auto* d = b.phi.target<snow::PlaneDistance>();
         const auto* nrm = b.normal.target<snow::PlaneNormal>();
-        const auto* vel = b.velocity.target<snow::ConstantVelocity>();
-        if (!d || !nrm || !vel || d->unit_normal != nrm->unit_normal)
-            throw std::invalid_argument(
-                "collider is not a make_plane body: the GPU step runs plane colliders only "
-                "(a std::function cannot execute on the device)");
+        const auto* sd = b.phi.target<snow::SphereDistance>();
+        const auto* sn = b.normal.target<snow::SphereNormal>();
         snow_collider c{};
-        c.kind = SNOW_COLLIDER_PLANE;
-        for (int a = 0; a < 3; ++a)
+        if (vel && d && nrm && d->unit_normal == nrm->unit_normal)
         {
-            c.point[a] = d->point[a];
-            c.normal[a] = d->unit_normal[a];
-            c.velocity[a] = vel->value[a];
+            c.kind = SNOW_COLLIDER_PLANE;
+            for (int a = 0; a < 3; ++a)
+            {
+                c.point[a] = d->point[a];
+                c.normal[a] = d->unit_normal[a];
+            }
         }
+        else if (vel && sd && sn && sd->center == sn->center && sd->radius > 0.0)
+        {
+            c.kind = SNOW_COLLIDER_SPHERE;
+            for (int a = 0; a < 3; ++a) c.point[a] = sd->center[a];
+            c.param[0] = sd->radius;
+        }
+        else
+        {
+            throw std::invalid_argument(
+                "collider is not a make_plane, snow::make_moving_plane or snow::make_sphere body "
+                "(a std::function cannot execute on the device)");
+        }
+        for (int a = 0; a < 3; ++a) c.velocity[a] = vel->value[a];
         c.friction = b.friction;
         out.push_back(c);
     }

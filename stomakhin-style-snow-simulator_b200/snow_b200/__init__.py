@@ -20,6 +20,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.environ.get("SNOW_B200_LIB") or os.path.join(PKG_DIR, "libsnow_b200.so")
 
 SNOW_FP64, SNOW_MIXED = 0, 1
+SNOW_COLLIDER_PLANE, SNOW_COLLIDER_SPHERE = 0, 1
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "grid capacity exceeded",
           -4: "non-finite particle state", -5: "key range exceeded", -6: "invalid state"}
 
@@ -187,14 +188,44 @@ def make_plane(point, normal, friction: float) -> Collider:
     return c
 
 
+def sphere(center, radius: float, friction: float, velocity=(0.0, 0.0, 0.0)) -> "Collider":
+    """A solid sphere collider (phi = |x - center| - radius), moving with `velocity`."""
+    c = Collider()
+    c.kind = SNOW_COLLIDER_SPHERE
+    for a in range(3):
+        c.point[a] = float(center[a])
+        c.velocity[a] = float(velocity[a])
+    c.friction = float(friction)
+    c.param[0] = float(radius)
+    return c
+
+
+def moving_plane(point, normal, friction: float, velocity) -> "Collider":
+    """make_plane with a constant velocity."""
+    c = make_plane(point, normal, friction)
+    for a in range(3):
+        c.velocity[a] = float(velocity[a])
+    return c
+
+
+def body_rows(cols) -> np.ndarray:
+    """(k, 12) rows (kind, point, normal, velocity, friction, radius) of Collider values,
+    the form the oracle and the reference build take."""
+    out = np.zeros((len(cols), 12))
+    for i, c in enumerate(cols):
+        out[i] = [c.kind, *c.point, *c.normal, *c.velocity, c.friction, c.param[0]]
+    return out
+
+
 def colliders(planes) -> ctypes.Array:
-    """A ctypes array of plane colliders from (point, normal, friction) triples
-    or from a (k, 7) array of point[3], normal[3], friction rows."""
+    """A ctypes array of colliders from (point, normal, friction) plane triples,
+    Collider values (see sphere, moving_plane), or a (k, 7) array of point[3],
+    normal[3], friction plane rows."""
     if isinstance(planes, np.ndarray):
         planes = [(r[:3], r[3:6], r[6]) for r in planes.reshape(-1, 7)]
     arr = (Collider * max(1, len(planes)))()
-    for i, (p, n, mu) in enumerate(planes):
-        arr[i] = make_plane(p, n, mu)
+    for i, item in enumerate(planes):
+        arr[i] = item if isinstance(item, Collider) else make_plane(*item)
     return arr
 
 

@@ -271,6 +271,19 @@ int main()
              }
              expect(threw, "std::invalid_argument for a std::function collider");
          }},
+        {"sphere and moving-plane bodies run on the device", [] {
+             // a particle falling onto a resting sphere stops moving into it; one
+             // under a rising plane is carried up with the plane's velocity
+             std::vector<Particle> a{Particle({0.5, 0.5801, 0.5}, {0, -1, 0}, 1, 1e-6),
+                                     Particle({0.2, 0.0995, 0.2}, {0, 0, 0}, 1, 1e-6)};
+             std::vector<ParticleStencil> st(2);
+             StepTimings t;
+             std::vector<CollisionBody> bodies{snow::make_sphere({0.5, 0.5, 0.5}, 0.08, 0.0),
+                                               snow::make_moving_plane({0, 0.1, 0}, {0, 3, 0}, {0, 0.5, 0}, 1.0)};
+             step(a, bodies, st, {0, 0, 0}, 1e-4, 0.02, 1, 1, 1, 0.02, 0.01, 0.95, t);
+             expect(a[0].v_p[1] > -1.0 + 1e-6, "sphere pushes back the falling particle");
+             expect(a[1].v_p[1] > 0.0, "the rising plane lifts the particle");
+         }},
         {"CSV import, its errors, and frame export", [] {
              namespace fs = std::filesystem;
              const fs::path dir = fs::temp_directory_path() / "snow_gpu_io_test";

@@ -33,14 +33,26 @@ class _StepLib:
         self.L = ctypes.CDLL(path)
         f = getattr(self.L, self.prefix + "_setup")
         f.argtypes, f.restype = [_dp, ctypes.c_int64, ctypes.c_double], None
-        f = getattr(self.L, self.prefix + "_step")
-        f.argtypes = [_dp, ctypes.c_int64, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp]
-        f.restype = None
+        for name in ("_step", "_step_bodies"):
+            f = getattr(self.L, self.prefix + name)
+            f.argtypes = [_dp, ctypes.c_int64, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp]
+            f.restype = None
 
     def setup(self, rec: np.ndarray, dx: float) -> np.ndarray:
         out = np.ascontiguousarray(rec, dtype=np.float64).copy()
         getattr(self.L, self.prefix + "_setup")(_p(out), out.shape[0], float(dx))
         return out
+
+    def step_bodies(self, rec: np.ndarray, params, bodies, steps: int = 1):
+        """Like step() with general colliders: (k, 12) rows of kind (0 plane, 1 sphere),
+        point[3], normal[3], velocity[3], friction, radius."""
+        out = np.ascontiguousarray(rec, dtype=np.float64).copy()
+        prm = np.ascontiguousarray(params, dtype=np.float64)
+        b = np.ascontiguousarray(np.asarray(bodies, dtype=np.float64).reshape(-1, 12))
+        ms = np.zeros(11)
+        getattr(self.L, self.prefix + "_step_bodies")(_p(out), out.shape[0], _p(prm), _p(b), b.shape[0],
+                                                      int(steps), _p(ms))
+        return out, ms
 
     def step(self, rec: np.ndarray, params, planes, steps: int = 1):
         """Returns (new records, milliseconds[11]: ten stages, then the step loop's wall time)."""
