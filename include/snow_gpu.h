@@ -130,6 +130,12 @@ int snow_gpu_batch_upload(snow_gpu_batch* batch, int32_t scene_id, const double*
 /* Copies a scene's particles back in their original order. */
 int snow_gpu_batch_download(snow_gpu_batch* batch, int32_t scene_id, double* records, int64_t n,
                             void* stream);
+/* A device copy of a scene's particle state (one per scene, replaced by the
+ * next call), and putting it back so the scene continues from there: for
+ * pre-empting or retrying served work.  No reference counterpart (the
+ * reference keeps no state between steps). */
+int snow_gpu_batch_snapshot(snow_gpu_batch* batch, int32_t scene_id, void* stream);
+int snow_gpu_batch_restore(snow_gpu_batch* batch, int32_t scene_id, void* stream);
 /* setup() for one scene: V_p0 = m_p / (sum_i m_i w_ip / dx^3) from a mass-only P2G. */
 int snow_gpu_batch_setup(snow_gpu_batch* batch, int32_t scene_id, double grid_spacing,
                          void* stream);

@@ -188,6 +188,30 @@ void Batch::free_scene(Scene& s) {
     dfree(s.fp[k]);
     dfree(s.id[k]);
   }
+  dfree(s.snap);
+}
+
+void Batch::snapshot(int32_t id, cudaStream_t s) {
+  step_complete();
+  Scene* sc = find(id);
+  const size_t rb = (size_t)sc->stride * kRealPlanes * rsize_, fb = (size_t)sc->stride * kFPPlanes * sizeof(double),
+               ib = (size_t)sc->stride * sizeof(int32_t);
+  if (!sc->snap) sc->snap = dalloc<unsigned char>(rb + fb + ib);
+  check_cuda(cudaMemcpyAsync(sc->snap, sc->r[sc->cur], rb, cudaMemcpyDeviceToDevice, s), "snapshot");
+  check_cuda(cudaMemcpyAsync(sc->snap + rb, sc->fp[sc->cur], fb, cudaMemcpyDeviceToDevice, s), "snapshot");
+  check_cuda(cudaMemcpyAsync(sc->snap + rb + fb, sc->id[sc->cur], ib, cudaMemcpyDeviceToDevice, s), "snapshot");
+}
+
+void Batch::restore(int32_t id, cudaStream_t s) {
+  step_complete();
+  Scene* sc = find(id);
+  if (!sc->snap) throw Error(SNOW_E_STATE, "restore: scene " + std::to_string(id) + " has no snapshot");
+  const size_t rb = (size_t)sc->stride * kRealPlanes * rsize_, fb = (size_t)sc->stride * kFPPlanes * sizeof(double),
+               ib = (size_t)sc->stride * sizeof(int32_t);
+  check_cuda(cudaMemcpyAsync(sc->r[sc->cur], sc->snap, rb, cudaMemcpyDeviceToDevice, s), "restore");
+  check_cuda(cudaMemcpyAsync(sc->fp[sc->cur], sc->snap + rb, fb, cudaMemcpyDeviceToDevice, s), "restore");
+  check_cuda(cudaMemcpyAsync(sc->id[sc->cur], sc->snap + rb + fb, ib, cudaMemcpyDeviceToDevice, s), "restore");
+  boxes_dirty_ = true;  // the particles moved back
 }
 
 void Batch::free_particle_buffers() {
@@ -346,6 +370,7 @@ void Batch::remove_scene(int32_t id) {
       cudaDeviceSynchronize();
       // keep the buffers for a later scene (serving admits and retires scenes
       // continuously); the cache holds at most kSceneCacheBytes
+      dfree(scenes_[k]->snap);
       Scene c;
       c.stride = scenes_[k]->stride;
       for (int b = 0; b < 2; ++b) {
@@ -1012,6 +1037,18 @@ int snow_gpu_batch_download(snow_gpu_batch* batch, int32_t scene_id, double* rec
   return guarded([&] {
     SNOW_BATCH_OR_FAIL;
     batch->impl->download(scene_id, records, n, as_stream(stream));
+  });
+}
+int snow_gpu_batch_snapshot(snow_gpu_batch* batch, int32_t scene_id, void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->snapshot(scene_id, as_stream(stream));
+  });
+}
+int snow_gpu_batch_restore(snow_gpu_batch* batch, int32_t scene_id, void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->restore(scene_id, as_stream(stream));
   });
 }
 int snow_gpu_batch_setup(snow_gpu_batch* batch, int32_t scene_id, double grid_spacing, void* stream) {

@@ -32,6 +32,7 @@ struct Scene {
   int32_t* id[2] = {nullptr, nullptr};
   snow_step_params params{};
   std::vector<Collider> colliders;
+  unsigned char* snap = nullptr;  // snapshot of the particle state (snapshot())
 };
 
 class Batch {
@@ -52,6 +53,10 @@ class Batch {
   void step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s);
   void step_complete();
   int32_t adopt_scene(Batch& from, int32_t id);
+  // A device copy of a scene's particle state, and putting it back (the
+  // scene then continues from there).  One snapshot per scene.
+  void snapshot(int32_t id, cudaStream_t s);
+  void restore(int32_t id, cudaStream_t s);
   int autotune(int trial_steps, double* best_ms, cudaStream_t s);
 
   int scene_count() const { return (int)scenes_.size(); }

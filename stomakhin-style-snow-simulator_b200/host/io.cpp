@@ -10,10 +10,12 @@
 #include <fstream>
 #include <iomanip>
 #include <iterator>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
 #include <string_view>
+#include <thread>
 #include <vector>
 
 #include "snow/export.hpp"
@@ -164,6 +166,29 @@ std::vector<Particle> import_particles(const std::string& filename_group, const 
     return assemble_particles(seeds, groups);
 }
 
+namespace
+{
+// output/frame_<frame>.csv with header "x,y,z" and rows (x, -z, y), default
+// stream formatting (export.cpp:10-22).
+void write_frame(const double* rec, std::size_t n, int frame_no)
+{
+    std::ostringstream name;
+    name << "output/frame_" << std::setw(6) << std::setfill('0') << frame_no << ".csv";
+    std::ofstream file{name.str()};
+    std::ostringstream out;
+    out << "x,y,z\n";
+    for (std::size_t i = 0; i < n; ++i)
+    {
+        const double* p = rec + SNOW_RECORD_DOUBLES * i;
+        out << p[0] << "," << p[2] * -1 << "," << p[1] << "\n";
+    }
+    file << out.str();
+}
+
+std::mutex g_export_mu;
+std::vector<std::thread> g_exports;
+}  // namespace
+
 void export_particles(const std::vector<Particle>& particles, int frame_no)
 {
     // A vector kept on the GPU by resident stepping is read back first.
@@ -174,15 +199,28 @@ void export_particles(const std::vector<Particle>& particles, int frame_no)
         fresh.resize(particles.size() * SNOW_RECORD_DOUBLES);
         if (snow_host_resident_copy(particles, fresh.data())) rec = fresh.data();
     }
-    std::ostringstream name;
-    name << "output/frame_" << std::setw(6) << std::setfill('0') << frame_no << ".csv";
-    std::ofstream file{name.str()};
-    std::ostringstream out;
-    out << "x,y,z\n";
-    for (std::size_t i = 0; i < particles.size(); ++i)
-    {
-        const double* p = rec + SNOW_RECORD_DOUBLES * i;
-        out << p[0] << "," << p[2] * -1 << "," << p[1] << "\n";
-    }
-    file << out.str();
+    write_frame(rec, particles.size(), frame_no);
 }
+
+namespace snow::gpu
+{
+void export_particles_async(const std::vector<Particle>& particles, int frame_no)
+{
+    std::vector<double> state(particles.size() * SNOW_RECORD_DOUBLES);
+    if (!particles.empty() && !snow_host_resident_copy(particles, state.data()))
+        std::memcpy(state.data(), particles.data(), state.size() * sizeof(double));
+    const std::size_t n = particles.size();
+    std::lock_guard<std::mutex> lock(g_export_mu);
+    g_exports.emplace_back([state = std::move(state), n, frame_no] { write_frame(state.data(), n, frame_no); });
+}
+
+void wait_exports()
+{
+    std::vector<std::thread> jobs;
+    {
+        std::lock_guard<std::mutex> lock(g_export_mu);
+        jobs.swap(g_exports);
+    }
+    for (auto& t : jobs) t.join();
+}
+}  // namespace snow::gpu

@@ -127,6 +127,8 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_batch_set_dense": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_graph_kernels": (ctypes.c_int, [vp]),
         "snow_gpu_batch_sort_mode": (ctypes.c_int, [vp]),
+        "snow_gpu_batch_snapshot": (ctypes.c_int, [vp, ctypes.c_int32, vp]),
+        "snow_gpu_batch_restore": (ctypes.c_int, [vp, ctypes.c_int32, vp]),
         "snow_gpu_setup": (ctypes.c_int, [_dp, i64, d]),
         "snow_gpu_step": (ctypes.c_int, [_dp, i64, ctypes.POINTER(StepParams), ctypes.POINTER(Collider),
                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(StepTimings)]),
@@ -282,6 +284,14 @@ class Batch:
             out = np.empty((n, 26), dtype=np.float64)
         _check(lib().snow_gpu_batch_download(self._h, sid, _ptr(out), n, ctypes.c_void_p(stream)))
         return out
+
+    def snapshot(self, sid: int, stream: int | None = None) -> None:
+        """Keeps a device copy of the scene's particle state."""
+        _check(lib().snow_gpu_batch_snapshot(self._h, sid, ctypes.c_void_p(stream)))
+
+    def restore(self, sid: int, stream: int | None = None) -> None:
+        """Puts the scene back to its last snapshot."""
+        _check(lib().snow_gpu_batch_restore(self._h, sid, ctypes.c_void_p(stream)))
 
     def setup(self, sid: int, dx: float, stream: int | None = None) -> None:
         _check(lib().snow_gpu_batch_setup(self._h, sid, float(dx), ctypes.c_void_p(stream)))

@@ -317,11 +317,19 @@ int main()
              const fs::path cwd = fs::current_path();
              fs::current_path(dir);
              export_particles(parts, 7);
+             std::vector<Particle> copy = parts;
+             snow::gpu::export_particles_async(copy, 8);
+             copy[0].x_p[0] = 99.0;  // the asynchronous export copied the state already
+             snow::gpu::wait_exports();
              fs::current_path(cwd);
-             std::ifstream out(dir / "output" / "frame_000007.csv");
-             std::stringstream ss;
-             ss << out.rdbuf();
-             expect(ss.str() == "x,y,z\n-0.1,-0.05,1\n0.2,-0.4,0.3\n", "export axes and format");
+             auto slurp = [&](const char* f) {
+                 std::ifstream in(dir / "output" / f);
+                 std::stringstream ss;
+                 ss << in.rdbuf();
+                 return ss.str();
+             };
+             expect(slurp("frame_000007.csv") == "x,y,z\n-0.1,-0.05,1\n0.2,-0.4,0.3\n", "export axes and format");
+             expect(slurp("frame_000008.csv") == slurp("frame_000007.csv"), "asynchronous export writes the same file");
          }},
     };
     int n = 0;

@@ -104,3 +104,31 @@ def test_zero_steps_leave_state_alone(snow):
     got = b.download(sid)
     b.close()
     assert np.array_equal(got, rec)
+
+
+def test_snapshot_and_restore(snow):
+    """A scene put back to its snapshot continues exactly as it did from there."""
+    sc = _cube()
+    rec = snow.setup(sc.particles.copy(), sc.dx)
+    b = snow.Batch(snow.SNOW_FP64)
+    other = b.add_scene(_cube(seed=5, lo=(0.6, 0.3, 0.6)).particles, sc.params(), sc.planes)
+    sid = b.add_scene(rec, sc.params(), sc.planes)
+    b.step(2)
+    before = b.download(sid)
+    b.snapshot(sid)
+    b.step(5)
+    first = b.download(sid)
+    b.restore(sid)
+    assert np.array_equal(b.download(sid), before)
+    b.step(5)
+    again = b.download(sid)
+    b.close()
+    assert max(errors(again, first).values()) < 1e-12
+    with pytest.raises(snow.SnowError):
+        b2 = snow.Batch(snow.SNOW_FP64)
+        try:
+            s2 = b2.add_scene(rec, sc.params(), sc.planes)
+            b2.restore(s2)
+        finally:
+            b2.close()
+    assert other >= 0
