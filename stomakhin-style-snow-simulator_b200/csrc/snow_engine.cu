@@ -367,9 +367,10 @@ void Batch::remove_scene(int32_t id) {
   step_complete();
   for (size_t k = 0; k < scenes_.size(); ++k)
     if (scenes_[k]->sid == id) {
-      cudaDeviceSynchronize();
-      // keep the buffers for a later scene (serving admits and retires scenes
-      // continuously); the cache holds at most kSceneCacheBytes
+      // Keep the buffers for a later scene (serving admits and retires scenes
+      // continuously); the cache holds at most kSceneCacheBytes.  This batch
+      // has no work in flight (step_complete above; copies are synchronous),
+      // so no device-wide wait is needed.
       dfree(scenes_[k]->snap);
       Scene c;
       c.stride = scenes_[k]->stride;

@@ -53,6 +53,13 @@ class Batch {
   void step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s);
   void step_complete();
   int32_t adopt_scene(Batch& from, int32_t id);
+  // Hands the cached buffers of removed scenes to another batch.
+  void give_cache(Batch& to) {
+    for (auto& c : cache_) to.cache_.push_back(c);
+    to.cached_bytes_ += cached_bytes_;
+    cache_.clear();
+    cached_bytes_ = 0;
+  }
   // A device copy of a scene's particle state, and putting it back (the
   // scene then continues from there).  One snapshot per scene.
   void snapshot(int32_t id, cudaStream_t s);

@@ -7,7 +7,8 @@
 // stay resident; every tick advances all of them together by the same number
 // of steps (one launch per kernel for the whole batch, replayed from a CUDA
 // graph), at most until the next scene finishes; requests that arrive are
-// uploaded and set up on a second stream while a tick runs.  A finished scene is copied
+// uploaded and set up, and finished scenes copied back, on other streams
+// while a tick runs.  A finished scene is copied
 // back, removed, and its latency (arrival to result) recorded.  Scenes do not
 // interact, so each result is the one the scene would get alone.
 #include <algorithm>
@@ -40,6 +41,7 @@ struct Request {
   double admitted = -1.0, finished = -1.0;
   int64_t bytes = 0;
   bool rejected = false;
+  bool pinned = false;  // records page-locked with cudaHostRegister
 };
 
 }  // namespace
@@ -47,15 +49,18 @@ struct Request {
 class Server {
  public:
   Server(int precision, int64_t budget, int max_scenes, int max_tick_steps)
-      : batch_(precision), admit_(precision), prec_(precision), budget_(budget), max_scenes_(max_scenes),
+      : batch_(precision), admit_(precision), retired_(precision), prec_(precision), budget_(budget), max_scenes_(max_scenes),
         max_tick_(max_tick_steps) {}
   ~Server() {
     try {
       batch_.step_complete();
     } catch (...) {
     }
+    for (auto& r : reqs_)
+      if (r->pinned) cudaHostUnregister(r->records.data());
     if (main_s_) cudaStreamDestroy(main_s_);
     if (admit_s_stream_) cudaStreamDestroy(admit_s_stream_);
+    if (retire_s_stream_) cudaStreamDestroy(retire_s_stream_);
   }
   Server(const Server&) = delete;
   Server& operator=(const Server&) = delete;
@@ -67,6 +72,13 @@ class Server {
     auto r = std::make_unique<Request>();
     r->id = (int64_t)reqs_.size();
     r->records.assign(rec, rec + n * 26);
+    // page-lock the request's records so uploads and result copies run as
+    // direct DMA (without it they go through the batch's staging chunks)
+    if (n > 0 && cudaHostRegister(r->records.data(), r->records.size() * sizeof(double), cudaHostRegisterDefault) ==
+                     cudaSuccess)
+      r->pinned = true;
+    else
+      cudaGetLastError();
     r->params = *p;
     r->colliders.assign(c, c + nc);
     r->steps = steps;
@@ -97,11 +109,11 @@ class Server {
       if (r->finished < 0 && !r->rejected) order.push_back(r.get());
     std::stable_sort(order.begin(), order.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
     std::deque<Request*> pending(order.begin(), order.end());
-    std::vector<Request*> live, arriving;
+    std::vector<Request*> live, arriving, leaving;
     int64_t used = 0;
     const auto t0 = clock_t_::now();
     auto now = [&] { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
-    while (!pending.empty() || !live.empty()) {
+    while (!pending.empty() || !live.empty() || !leaving.empty()) {
       // launch this tick (the steps run while the host admits below)
       int64_t k = 0;
       double t_phase = now();
@@ -135,6 +147,10 @@ class Server {
         peak_bytes_ = std::max(peak_bytes_, used);
       }
       admit_s_ += now() - t_phase;
+      // results of the scenes that finished last tick, copied back while this tick runs
+      t_phase = now();
+      drain(leaving, used, now);
+      retire_s_ += now() - t_phase;
       // complete the tick
       if (k > 0) {
         t_phase = now();
@@ -146,22 +162,30 @@ class Server {
           particle_steps_ += k * ((int64_t)r->records.size() / 26);
         }
       }
-      t_phase = now();
-      retire(live, used, now, s);
-      retire_s_ += now() - t_phase;
       for (Request* r : arriving) {
         r->scene = batch_.adopt_scene(admit_, r->scene);
         live.push_back(r);
       }
       arriving.clear();
-      t_phase = now();
-      retire(live, used, now, s);  // zero-step requests
-      retire_s_ += now() - t_phase;
-      if (live.empty() && !pending.empty()) {
+      // finished scenes leave the live batch without a copy
+      for (size_t i = 0; i < live.size();) {
+        Request* r = live[i];
+        if (r->remaining > 0) {
+          ++i;
+          continue;
+        }
+        r->scene = retired_.adopt_scene(batch_, r->scene);
+        leaving.push_back(r);
+        live.erase(live.begin() + i);
+      }
+      if (live.empty() && !pending.empty() && leaving.empty()) {
         const double wait = pending.front()->arrival - now();
         if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
       }
     }
+    const double t_phase = now();
+    drain(leaving, used, now);
+    retire_s_ += now() - t_phase;
     wall_ += now();
   }
 
@@ -199,35 +223,48 @@ class Server {
   }
 
  private:
+  // Copies finished scenes back from the retired batch (on its own stream) and
+  // releases them; their buffers go back to the admission batch for reuse.
   template <typename Now>
-  void retire(std::vector<Request*>& live, int64_t& used, Now&& now, cudaStream_t s) {
-    for (size_t i = 0; i < live.size();) {
-      Request* r = live[i];
-      if (r->remaining > 0) {
-        ++i;
-        continue;
-      }
+  void drain(std::vector<Request*>& leaving, int64_t& used, Now&& now) {
+    for (Request* r : leaving) {
       const int64_t n = (int64_t)r->records.size() / 26;
-      batch_.download(r->scene, r->records.data(), n, s);
-      batch_.remove_scene(r->scene);
+      retired_.download(r->scene, r->records.data(), n, retire_stream());
+      retired_.remove_scene(r->scene);
       r->finished = now();
       used -= r->bytes;
-      live.erase(live.begin() + i);
     }
+    if (!leaving.empty()) retired_.give_cache(admit_);
+    leaving.clear();
   }
 
   cudaStream_t main_stream() {
     if (!main_s_) check_cuda(cudaStreamCreateWithFlags(&main_s_, cudaStreamNonBlocking), "cudaStreamCreate");
     return main_s_;
   }
+  // Admission and result copies run beside the live batch's tick at the
+  // highest stream priority, so their short kernels start at the tick's next
+  // kernel boundary instead of after the whole tick.
+  static cudaStream_t side_stream() {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    cudaStream_t st = nullptr;
+    check_cuda(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
+    return st;
+  }
+  cudaStream_t retire_stream() {
+    if (!retire_s_stream_) retire_s_stream_ = side_stream();
+    return retire_s_stream_;
+  }
   cudaStream_t admit_stream() {
-    if (!admit_s_stream_) check_cuda(cudaStreamCreateWithFlags(&admit_s_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!admit_s_stream_) admit_s_stream_ = side_stream();
     return admit_s_stream_;
   }
 
   Batch batch_;
-  Batch admit_;  // new scenes are set up here while batch_ steps
-  cudaStream_t main_s_ = nullptr, admit_s_stream_ = nullptr;
+  Batch admit_;    // new scenes are set up here while batch_ steps
+  Batch retired_;  // finished scenes are copied back from here while batch_ steps
+  cudaStream_t main_s_ = nullptr, admit_s_stream_ = nullptr, retire_s_stream_ = nullptr;
   int prec_;
   int64_t budget_;
   int max_scenes_;
