@@ -345,18 +345,23 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
                         "graph": "CUDA graph per step", "autotuned": "work-item size and particle ordering"}
     # -- served: Poisson stream, mixed form
     reqs = scenes.served_requests(count=48, rate=200.0)
-    srv = snow_b200.Server(snow_b200.SNOW_MIXED, budget_bytes=150 * 10**9, max_steps_per_tick=16)
-    for sc, n, t in reqs:
-        srv.submit(sc, n, t)
-    srv.run(stream=sp)
-    st = srv.stats()
-    srv.close()
+    runs = []
+    for _ in range(3):  # the host's share varies from run to run: report the median run
+        srv = snow_b200.Server(snow_b200.SNOW_MIXED, budget_bytes=150 * 10**9, max_steps_per_tick=16)
+        for sc, n, t in reqs:
+            srv.submit(sc, n, t)
+        srv.run(stream=sp)
+        runs.append(srv.stats())
+        srv.close()
+    runs.sort(key=lambda r: r["particle_steps_per_s"])
+    st = runs[len(runs) // 2]
     plain_s = plain_fp64_rate(snow_b200, torch, sp, [(sc, n, min(n, 40)) for sc, n, _ in reqs])
     forms["served"] = {"requests": len(reqs), "arrival_rate_per_s": 200.0, "budget_bytes": 150 * 10**9,
                        "plain_fp64_one_request_at_a_time": plain_s,
                        "plain_fp64_sample": "each request's scene alone, min(steps, 40) timed steps "
                                             "scaled to its requested steps",
                        "served_vs_plain_fp64_same_requests": st["particle_steps_per_s"] / plain_s,
+                       "runs_particle_steps_per_s": [r["particle_steps_per_s"] for r in runs],
                        "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"],
                        "mean_latency_s": st["mean_s"], "particle_steps_per_s": st["particle_steps_per_s"],
                        "served_vs_plain_fp64_headline": st["particle_steps_per_s"] / fp64_rate,
