@@ -6,7 +6,7 @@ dt = 2e-5, plain FP64 path -- the configuration the headline metric is quoted
 on.  A "step" is one explicit MPM timestep over the whole scene.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tori|cube|snowball] [--precision fp64|mixed]
+                    [--workload tori|cube|snowball|batch] [--precision fp64|mixed]
 
 * value        particle-steps/s with the scene resident in HBM, device time of
                K CUDA-graph-replayed steps (CUDA events on the launching stream),
