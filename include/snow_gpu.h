@@ -210,6 +210,17 @@ int snow_gpu_server_run(snow_gpu_server* server, void* stream);
 int snow_gpu_server_result(snow_gpu_server* server, int64_t request_id, double* records, int64_t n,
                            double* latency_s);
 int snow_gpu_server_stats(snow_gpu_server* server, snow_server_stats* stats);
+/* One tick of the last run(): host times on the server's clock (launch of the
+ * tick's steps, and the moment the host saw them complete), the device span of
+ * the steps (CUDA events on the run's stream, seconds after the first tick's
+ * start event), steps, live scenes and particles, and the scenes admitted into
+ * and retired from the live batch after it.  *count = ticks recorded; at most
+ * `capacity` are copied. */
+typedef struct snow_server_tick {
+  double host_start_s, host_end_s, device_start_s, device_end_s;
+  int64_t steps, scenes, particles, admitted, retired;
+} snow_server_tick;
+int snow_gpu_server_ticks(snow_gpu_server* server, snow_server_tick* out, int64_t capacity, int64_t* count);
 
 /* ---- one scene: setup() / step() of the reference ------------------------ */
 /* setup() on host records: records[i].V_p0 is overwritten. */

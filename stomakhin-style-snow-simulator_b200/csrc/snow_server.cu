@@ -58,6 +58,8 @@ class Server {
     }
     for (auto& r : reqs_)
       if (r->pinned) cudaHostUnregister(r->records.data());
+    for (cudaEvent_t e : {ev_base_, ev_start_, ev_end_})
+      if (e) cudaEventDestroy(e);
     if (main_s_) cudaStreamDestroy(main_s_);
     if (admit_s_stream_) cudaStreamDestroy(admit_s_stream_);
     if (retire_s_stream_) cudaStreamDestroy(retire_s_stream_);
@@ -111,16 +113,31 @@ class Server {
     std::deque<Request*> pending(order.begin(), order.end());
     std::vector<Request*> live, arriving, leaving;
     int64_t used = 0;
+    ticks_log_.clear();
+    bool base_recorded = false;
+    for (cudaEvent_t* e : {&ev_base_, &ev_start_, &ev_end_})
+      if (!*e) check_cuda(cudaEventCreate(e), "cudaEventCreate");
     const auto t0 = clock_t_::now();
     auto now = [&] { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
     while (!pending.empty() || !live.empty() || !leaving.empty()) {
       // launch this tick (the steps run while the host admits below)
       int64_t k = 0;
       double t_phase = now();
+      snow_server_tick tick{};
+      tick.host_start_s = t_phase;
       if (!live.empty()) {
         k = max_tick_;
-        for (Request* r : live) k = std::min(k, r->remaining);
+        for (Request* r : live) {
+          k = std::min(k, r->remaining);
+          tick.particles += (int64_t)r->records.size() / 26;
+        }
+        if (!base_recorded) {
+          check_cuda(cudaEventRecord(ev_base_, s), "cudaEventRecord");
+          base_recorded = true;
+        }
+        check_cuda(cudaEventRecord(ev_start_, s), "cudaEventRecord");
         batch_.step_launch((int)k, nullptr, s);
+        check_cuda(cudaEventRecord(ev_end_, s), "cudaEventRecord");
       }
       step_s_ += now() - t_phase;
       // admit every arrived request that fits, in arrival order
@@ -161,6 +178,16 @@ class Server {
           r->remaining -= k;
           particle_steps_ += k * ((int64_t)r->records.size() / 26);
         }
+        float a = 0.f, b = 0.f;
+        check_cuda(cudaEventSynchronize(ev_end_), "cudaEventSynchronize");
+        check_cuda(cudaEventElapsedTime(&a, ev_base_, ev_start_), "cudaEventElapsedTime");
+        check_cuda(cudaEventElapsedTime(&b, ev_base_, ev_end_), "cudaEventElapsedTime");
+        tick.host_end_s = now();
+        tick.device_start_s = a * 1e-3;
+        tick.device_end_s = b * 1e-3;
+        tick.steps = k;
+        tick.scenes = (int64_t)live.size();
+        tick.admitted = (int64_t)arriving.size();
       }
       for (Request* r : arriving) {
         r->scene = batch_.adopt_scene(admit_, r->scene);
@@ -178,6 +205,10 @@ class Server {
         leaving.push_back(r);
         live.erase(live.begin() + i);
       }
+      if (k > 0) {
+        tick.retired = (int64_t)leaving.size();
+        ticks_log_.push_back(tick);
+      }
       if (live.empty() && !pending.empty() && leaving.empty()) {
         const double wait = pending.front()->arrival - now();
         if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
@@ -188,6 +219,8 @@ class Server {
     retire_s_ += now() - t_phase;
     wall_ += now();
   }
+
+  const std::vector<snow_server_tick>& ticks() const { return ticks_log_; }
 
   const Request& req(int64_t id) const {
     if (id < 0 || id >= (int64_t)reqs_.size()) throw Error(SNOW_E_ARG, "unknown request id");
@@ -265,6 +298,8 @@ class Server {
   Batch admit_;    // new scenes are set up here while batch_ steps
   Batch retired_;  // finished scenes are copied back from here while batch_ steps
   cudaStream_t main_s_ = nullptr, admit_s_stream_ = nullptr, retire_s_stream_ = nullptr;
+  cudaEvent_t ev_base_ = nullptr, ev_start_ = nullptr, ev_end_ = nullptr;
+  std::vector<snow_server_tick> ticks_log_;
   int prec_;
   int64_t budget_;
   int max_scenes_;
@@ -353,6 +388,15 @@ int snow_gpu_server_stats(snow_gpu_server* server, snow_server_stats* stats) {
   return guarded([&] {
     if (!server || !stats) throw snow::Error(SNOW_E_ARG, "NULL argument");
     server->impl->stats(stats);
+  });
+}
+
+int snow_gpu_server_ticks(snow_gpu_server* server, snow_server_tick* out, int64_t capacity, int64_t* count) {
+  return guarded([&] {
+    if (!server || !count || capacity < 0 || (capacity > 0 && !out)) throw snow::Error(SNOW_E_ARG, "bad argument");
+    const auto& t = server->impl->ticks();
+    *count = (int64_t)t.size();
+    std::copy_n(t.begin(), std::min<int64_t>(capacity, (int64_t)t.size()), out);
   });
 }
 

@@ -73,6 +73,14 @@ class ServerStats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class ServerTick(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("host_start_s", "host_end_s", "device_start_s", "device_end_s")] + \
+               [(n, ctypes.c_int64) for n in ("steps", "scenes", "particles", "admitted", "retired")]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class SnowError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -123,6 +131,7 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_server_run": (ctypes.c_int, [vp, vp]),
         "snow_gpu_server_result": (ctypes.c_int, [vp, i64, _dp, i64, _dp]),
         "snow_gpu_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
+        "snow_gpu_server_ticks": (ctypes.c_int, [vp, ctypes.POINTER(ServerTick), i64, _i64p]),
         "snow_gpu_batch_set_chunk": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_set_dense": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_graph_kernels": (ctypes.c_int, [vp]),
@@ -496,3 +505,11 @@ class Server:
         st = ServerStats()
         _check(lib().snow_gpu_server_stats(self._h, ctypes.byref(st)))
         return st.as_dict()
+
+    def ticks(self) -> list[dict]:
+        """Per-tick trace of the last run() (snow_gpu_server_ticks)."""
+        n = ctypes.c_int64()
+        _check(lib().snow_gpu_server_ticks(self._h, None, 0, ctypes.byref(n)))
+        buf = (ServerTick * max(1, n.value))()
+        _check(lib().snow_gpu_server_ticks(self._h, buf, n.value, ctypes.byref(n)))
+        return [buf[i].as_dict() for i in range(n.value)]

@@ -46,6 +46,16 @@ def test_served_results_match_alone(snow, prec, tol):
         assert lat > 0
         e = errors(got, _alone(snow, prec, sc, steps))
         assert max(e.values()) < tol, (sc.name, e)
+    # the tick trace accounts for every particle-step, in order on both clocks
+    ticks = srv.ticks()
+    assert len(ticks) == st["ticks"]
+    assert sum(t["steps"] * t["particles"] for t in ticks) == st["particle_steps"]
+    assert 0 <= sum(t["admitted"] for t in ticks) < len(reqs)
+    assert sum(t["retired"] for t in ticks) == len(reqs)
+    for a, b in zip(ticks, ticks[1:]):
+        assert a["device_end_s"] <= b["device_start_s"] and a["host_end_s"] <= b["host_start_s"]
+    assert all(0 <= t["device_start_s"] <= t["device_end_s"] for t in ticks)
+    assert all(1 <= t["steps"] <= 8 and t["scenes"] >= 1 for t in ticks)
     srv.close()
 
 
