@@ -102,11 +102,12 @@ void Batch::ensure_pinned() {
   }
 }
 
-void Batch::copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+void Batch::copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s, bool wait) {
   if (page_locked(src)) {
-    // the caller may reuse its buffer once the call returns
+    // the caller may reuse its buffer once the call returns (wait), or once
+    // the stream has passed the copy
     check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "upload copy");
-    check_cuda(cudaStreamSynchronize(s), "upload sync");
+    if (wait) check_cuda(cudaStreamSynchronize(s), "upload sync");
     return;
   }
   ensure_pinned();
@@ -121,10 +122,10 @@ void Batch::copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   }
 }
 
-void Batch::copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+void Batch::copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s, bool wait) {
   if (page_locked(dst)) {
     check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "download copy");
-    check_cuda(cudaStreamSynchronize(s), "download sync");
+    if (wait) check_cuda(cudaStreamSynchronize(s), "download sync");
     return;
   }
   ensure_pinned();
@@ -301,7 +302,7 @@ static void validate_params(const snow_step_params* p) {
 }
 
 int32_t Batch::add_scene(const double* records, int64_t n, const snow_step_params* params,
-                         const snow_collider* colliders, int n_colliders, cudaStream_t s) {
+                         const snow_collider* colliders, int n_colliders, cudaStream_t s, bool wait) {
   if (n < 0 || (n > 0 && !records)) throw Error(SNOW_E_ARG, "bad particle array");
   if (n > INT32_MAX) throw Error(SNOW_E_ARG, "at most 2^31-1 particles per scene");
   validate_params(params);
@@ -337,7 +338,7 @@ int32_t Batch::add_scene(const double* records, int64_t n, const snow_step_param
   Scene* raw = sc.get();
   scenes_.push_back(std::move(sc));
   dirty_ = true;
-  upload(raw->sid, records, n, s);
+  upload(raw->sid, records, n, s, wait);
   return raw->sid;
 }
 
@@ -368,9 +369,10 @@ void Batch::remove_scene(int32_t id) {
   for (size_t k = 0; k < scenes_.size(); ++k)
     if (scenes_[k]->sid == id) {
       // Keep the buffers for a later scene (serving admits and retires scenes
-      // continuously); the cache holds at most kSceneCacheBytes.  This batch
-      // has no work in flight (step_complete above; copies are synchronous),
-      // so no device-wide wait is needed.
+      // continuously); the cache holds at most cache_limit_ bytes.  This
+      // batch has no work in flight (step_complete above; a copy left in
+      // flight by wait = false has passed, by the caller's contract), so no
+      // device-wide wait is needed.
       dfree(scenes_[k]->snap);
       Scene c;
       c.stride = scenes_[k]->stride;
@@ -384,7 +386,7 @@ void Batch::remove_scene(int32_t id) {
       }
       cache_.push_back(c);
       cached_bytes_ += scene_bytes(c.stride);
-      while (cached_bytes_ > kSceneCacheBytes && !cache_.empty()) {
+      while (cached_bytes_ > cache_limit_ && !cache_.empty()) {
         cached_bytes_ -= scene_bytes(cache_.front().stride);
         free_scene(cache_.front());
         cache_.erase(cache_.begin());
@@ -405,13 +407,13 @@ void Batch::set_params(int32_t id, const snow_step_params* params, const snow_co
   force_dirty_ = true;
 }
 
-void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s) {
+void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s, bool wait) {
   step_complete();
   Scene* sc = find(id);
   if (n != sc->n) throw Error(SNOW_E_ARG, "upload: particle count differs from the scene's");
   if (n == 0) return;
   ensure_staging(n);
-  copy_in(staging_, records, (size_t)n * 26 * sizeof(double), s);
+  copy_in(staging_, records, (size_t)n * 26 * sizeof(double), s, wait);
   const unsigned g = (unsigned)((n + 255) / 256);
   if (prec_ == SNOW_FP64)
     k_records_to_planes<double><<<g, 256, 0, s>>>(staging_, n, (double*)sc->r[sc->cur],
@@ -424,7 +426,7 @@ void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s)
   force_dirty_ = true;
 }
 
-void Batch::download(int32_t id, double* records, int64_t n, cudaStream_t s) {
+void Batch::download(int32_t id, double* records, int64_t n, cudaStream_t s, bool wait) {
   step_complete();
   Scene* sc = find(id);
   if (n != sc->n) throw Error(SNOW_E_ARG, "download: particle count differs from the scene's");
@@ -438,7 +440,7 @@ void Batch::download(int32_t id, double* records, int64_t n, cudaStream_t s) {
     k_planes_to_records<float><<<g, 256, 0, s>>>(staging_, n, (const float*)sc->r[sc->cur],
                                                   sc->fp[sc->cur], sc->id[sc->cur], sc->stride);
   check_cuda(cudaGetLastError(), "download kernel");
-  copy_out(records, staging_, (size_t)n * 26 * sizeof(double), s);
+  copy_out(records, staging_, (size_t)n * 26 * sizeof(double), s, wait);
 }
 
 SceneDev Batch::scene_dev(const Scene& sc, int64_t begin) const {
@@ -468,6 +470,26 @@ SceneDev Batch::scene_dev(const Scene& sc, int64_t begin) const {
     d.nb_hi[a] = INT_MIN;
   }
   return d;
+}
+
+void Batch::reserve(int64_t particles, int64_t staging, int scenes, int colliders) {
+  if (particles < 0 || staging < 0 || scenes < 0 || colliders < 0) throw Error(SNOW_E_ARG, "negative reservation");
+  step_complete();
+  ensure_particle_buffers(particles);
+  if (staging > 0) ensure_staging(staging);
+  if (!d_tmp_scene_) d_tmp_scene_ = dalloc<SceneDev>(1);
+  if (scenes > d_scenes_cap_) {
+    dfree(d_scenes_);
+    d_scenes_cap_ = scenes;
+    d_scenes_ = dalloc<SceneDev>(d_scenes_cap_);
+    dirty_ = true;  // the tables are written again before the next step
+  }
+  if (colliders > d_coll_cap_) {
+    dfree(d_coll_);
+    d_coll_cap_ = colliders;
+    d_coll_ = dalloc<Collider>(d_coll_cap_);
+    dirty_ = true;
+  }
 }
 
 void Batch::ensure_particle_buffers(int64_t total) {
@@ -714,33 +736,49 @@ void Batch::step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s)
     for (auto& e : ev) cudaEventDestroy(e);
   } else if (use_graphs_) {
     int k = 0;
-    if (gexec_ && std::memcmp(&graph_args_, &b, sizeof b) != 0) drop_graph();  // a buffer moved
     if (!gexec_) {
       // first step eagerly (initialises per-kernel launch settings), then capture
       one(nullptr);
       check_cuda(cudaGetLastError(), "step launch");
       ++k;
-      if (k < n_steps) {
-        cudaGraph_t g;
-        check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
-        one(nullptr);
-        check_cuda(cudaStreamEndCapture(s, &g), "capture end");
-        {
-          size_t nodes = 0;
-          check_cuda(cudaGraphGetNodes(g, nullptr, &nodes), "graph nodes");
-          std::vector<cudaGraphNode_t> list(nodes);
-          check_cuda(cudaGraphGetNodes(g, list.data(), &nodes), "graph nodes");
-          graph_kernels_ = 0;
-          for (cudaGraphNode_t nd : list) {
-            cudaGraphNodeType type;
-            check_cuda(cudaGraphNodeGetType(nd, &type), "graph node type");
-            if (type == cudaGraphNodeTypeKernel) ++graph_kernels_;
-          }
+    }
+    if (k < n_steps && (!gexec_ || std::memcmp(&graph_args_, &b, sizeof b) != 0)) {
+      cudaGraph_t g;
+      check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+      one(nullptr);
+      check_cuda(cudaStreamEndCapture(s, &g), "capture end");
+      {
+        size_t nodes = 0;
+        check_cuda(cudaGraphGetNodes(g, nullptr, &nodes), "graph nodes");
+        std::vector<cudaGraphNode_t> list(nodes);
+        check_cuda(cudaGraphGetNodes(g, list.data(), &nodes), "graph nodes");
+        graph_kernels_ = 0;
+        for (cudaGraphNode_t nd : list) {
+          cudaGraphNodeType type;
+          check_cuda(cudaGraphNodeGetType(nd, &type), "graph node type");
+          if (type == cudaGraphNodeTypeKernel) ++graph_kernels_;
         }
-        check_cuda(cudaGraphInstantiate(&gexec_, g, 0), "graph instantiate");
-        cudaGraphDestroy(g);
-        graph_args_ = b;
       }
+      // A buffer moved or the scenes changed: when the step launches the same
+      // kernels, only their arguments and grids differ and the executable
+      // graph is updated in place; otherwise it is instantiated anew.
+      bool updated = false;
+      if (gexec_) {
+        cudaGraphExecUpdateResultInfo info{};
+        updated = cudaGraphExecUpdate(gexec_, g, &info) == cudaSuccess;
+        if (!updated) {
+          cudaGetLastError();
+          drop_graph();
+        }
+      }
+      if (!updated) {
+        const cudaError_t e = cudaGraphInstantiate(&gexec_, g, 0);
+        cudaGraphDestroy(g);
+        check_cuda(e, "graph instantiate");
+      } else {
+        cudaGraphDestroy(g);
+      }
+      graph_args_ = b;
     }
     for (; k < n_steps; ++k) check_cuda(cudaGraphLaunch(gexec_, s), "graph launch");
   } else {
@@ -789,7 +827,7 @@ void Batch::check_status() {
 }
 
 // setup() for one scene: a private one-scene view over the batch's buffers.
-void Batch::setup(int32_t id, double dx, cudaStream_t s) {
+void Batch::setup(int32_t id, double dx, cudaStream_t s, int64_t box_blocks, bool wait) {
   step_complete();
   keyspace_ready_ = false;  // setup's own steps reuse the counters
   if (!(dx > 0.0)) throw Error(SNOW_E_ARG, "grid_spacing must be positive");
@@ -807,11 +845,16 @@ void Batch::setup(int32_t id, double dx, cudaStream_t s) {
       StepLaunch<double>::bbox_init(b0, s);
     else
       StepLaunch<float>::bbox_init(b0, s);
-    check_cuda(cudaMemcpyAsync(&d, d_tmp_scene_, sizeof d, cudaMemcpyDeviceToHost, s), "box");
-    check_cuda(cudaStreamSynchronize(s), "sync");
-    int64_t vol = 1;
-    for (int a = 0; a < 3; ++a) vol *= (int64_t)(d.nb_hi[a] - d.nb_lo[a] + 4);
-    ensure_grid(std::min<int64_t>(vol + 1024, 8 * sc->n + 1024));
+    int64_t vol = box_blocks;
+    if (vol < 0) {
+      check_cuda(cudaMemcpyAsync(&d, d_tmp_scene_, sizeof d, cudaMemcpyDeviceToHost, s), "box");
+      check_cuda(cudaStreamSynchronize(s), "sync");
+      vol = 1;
+      for (int a = 0; a < 3; ++a) vol *= (int64_t)(d.nb_hi[a] - d.nb_lo[a] + 4);
+    }
+    // 2x headroom, as for steps: a batch that sets up scenes one after
+    // another regrows (and frees) its grid only when the box doubles
+    ensure_grid(std::min<int64_t>(2 * vol + 1024, 8 * sc->n + 1024));
     size_dense(vol, s);
   }
   const BatchDev b = dev(d_tmp_scene_, 1, sc->n);
@@ -831,10 +874,42 @@ void Batch::setup(int32_t id, double dx, cudaStream_t s) {
     run(float{});
   check_cuda(cudaGetLastError(), "setup launch");
   check_cuda(cudaMemcpyAsync(h_ctr_, d_ctr_, sizeof(Counters), cudaMemcpyDeviceToHost, s), "status");
-  check_cuda(cudaStreamSynchronize(s), "setup");
-  last_status_ = h_ctr_->status;
   force_dirty_ = true;  // V_p0 changed
+  if (!wait) return;
+  check_cuda(cudaStreamSynchronize(s), "setup");
+  collect_status();
+}
+
+// Status flags accumulate in the counters until read here, so one read covers
+// every setup left in flight before it.
+void Batch::collect_status() {
+  last_status_ = h_ctr_->status;
   check_status();
+}
+
+void Batch::reserve_grid(int64_t blocks, int64_t key_blocks, cudaStream_t s) {
+  if (blocks < 0 || key_blocks < 0) throw Error(SNOW_E_ARG, "negative reservation");
+  step_complete();
+  if (blocks > 0) ensure_grid(blocks);
+  if (key_blocks > 0) size_dense(key_blocks, s);
+}
+
+void Batch::reserve_scenes(const std::vector<int64_t>& sizes, int64_t max_bytes) {
+  int64_t bytes = 0;
+  for (int64_t n : sizes) {
+    Scene c;
+    c.stride = pad32(std::max<int64_t>(n, 1));
+    if (bytes + scene_bytes(c.stride) > max_bytes) break;
+    for (int k = 0; k < 2; ++k) {
+      c.r[k] = dalloc<unsigned char>((size_t)c.stride * kRealPlanes * rsize_);
+      c.fp[k] = dalloc<double>((size_t)c.stride * kFPPlanes);
+      c.id[k] = dalloc<int32_t>((size_t)c.stride);
+    }
+    bytes += scene_bytes(c.stride);
+    cache_.push_back(c);
+    cached_bytes_ += scene_bytes(c.stride);
+  }
+  cache_limit_ = std::max(cache_limit_, cached_bytes_);
 }
 
 // Work-item-size autotuner.  Each candidate runs from the same snapshot of the

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -42,21 +43,40 @@ class Batch {
   Batch(const Batch&) = delete;
   Batch& operator=(const Batch&) = delete;
 
+  // wait = false (page-locked records only): the copies are left in flight on
+  // stream s; the caller keeps `records` untouched, and the scene in this
+  // batch, until s has passed them.
   int32_t add_scene(const double* records, int64_t n, const snow_step_params* params,
-                    const snow_collider* colliders, int n_colliders, cudaStream_t s);
+                    const snow_collider* colliders, int n_colliders, cudaStream_t s, bool wait = true);
   void remove_scene(int32_t id);
   void set_params(int32_t id, const snow_step_params* params, const snow_collider* c, int n);
-  void upload(int32_t id, const double* records, int64_t n, cudaStream_t s);
-  void download(int32_t id, double* records, int64_t n, cudaStream_t s);
-  void setup(int32_t id, double dx, cudaStream_t s);
+  void upload(int32_t id, const double* records, int64_t n, cudaStream_t s, bool wait = true);
+  void download(int32_t id, double* records, int64_t n, cudaStream_t s, bool wait = true);
+  // box_blocks >= 0: an upper bound on the scene's block box at dx (in 4^3
+  // blocks, halo included) known to the caller, which sizes the grid without
+  // reading the box back.  wait = false: the setup is left in flight on s and
+  // its status is read by collect_status() once s has passed it.
+  void setup(int32_t id, double dx, cudaStream_t s, int64_t box_blocks = -1, bool wait = true);
+  void collect_status();
+  // Grid blocks and key blocks to size the grid and the dense bins for now.
+  void reserve_grid(int64_t blocks, int64_t key_blocks, cudaStream_t s);
+  // Allocates particle buffers for scenes of these sizes into the cache of
+  // removed scenes' buffers, up to `max_bytes`.
+  void reserve_scenes(const std::vector<int64_t>& sizes, int64_t max_bytes);
   void step(int n_steps, snow_step_timings* timings, cudaStream_t s);
   void step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s);
   void step_complete();
   int32_t adopt_scene(Batch& from, int32_t id);
+  // Sizes the particle-indexed step buffers for `particles` in total, the
+  // host-transfer staging for scenes of up to `staging` particles and the
+  // device scene and collider tables, so that membership changes within those
+  // sizes allocate and free nothing (a cudaFree waits for the whole device).
+  void reserve(int64_t particles, int64_t staging, int scenes = 0, int colliders = 0);
   // Hands the cached buffers of removed scenes to another batch.
   void give_cache(Batch& to) {
     for (auto& c : cache_) to.cache_.push_back(c);
     to.cached_bytes_ += cached_bytes_;
+    to.cache_limit_ = std::max(to.cache_limit_, cache_limit_);
     cache_.clear();
     cached_bytes_ = 0;
   }
@@ -124,8 +144,8 @@ class Batch {
   void drop_graph();
   void ensure_staging(int64_t n);
   void ensure_pinned();
-  void copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s);
-  void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);
+  void copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s, bool wait);
+  void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s, bool wait);
   int64_t scene_bytes(int64_t stride) const {
     return 2 * stride * (kRealPlanes * (int64_t)rsize_ + kFPPlanes * 8 + 4);
   }
@@ -195,6 +215,7 @@ class Batch {
   cudaEvent_t pinned_ev_[2] = {nullptr, nullptr};
   // particle buffers of removed scenes, reused by later scenes
   static constexpr int64_t kSceneCacheBytes = int64_t(8) << 30;
+  int64_t cache_limit_ = kSceneCacheBytes;  // raised by reserve_scenes()
   std::vector<Scene> cache_;
   int64_t cached_bytes_ = 0;
 

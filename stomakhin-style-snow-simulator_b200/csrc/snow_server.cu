@@ -42,7 +42,32 @@ struct Request {
   int64_t bytes = 0;
   bool rejected = false;
   bool pinned = false;  // records page-locked with cudaHostRegister
+  int64_t box_blocks = 0;       // upper bound on the block box at the grid spacing
+  cudaEvent_t done = nullptr;   // the admission's setup, then the result copy, has passed
 };
+
+// Upper bound on a scene's block box at spacing dx (4^3-node blocks, halo and
+// one block of rounding slack per side included): the step's own measure is
+// prod(hi - lo + 4) over the block coordinates of the stencil bases.
+int64_t host_box_blocks(const double* rec, int64_t n, double dx) {
+  if (n == 0) return 0;
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) lo[a] = hi[a] = rec[a];
+  for (int64_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) {
+      const double x = rec[26 * i + a];
+      if (!std::isfinite(x)) throw Error(SNOW_E_NONFINITE, "request has a non-finite particle position");
+      lo[a] = std::min(lo[a], x);
+      hi[a] = std::max(hi[a], x);
+    }
+  int64_t v = 1;
+  for (int a = 0; a < 3; ++a) {
+    const double bl = std::floor(std::floor(lo[a] / dx) - 1.0) / 4.0, bh = std::floor(std::floor(hi[a] / dx) - 1.0) / 4.0;
+    if (!(std::fabs(bl) < 2e9 && std::fabs(bh) < 2e9)) throw Error(SNOW_E_KEYRANGE, "request extent out of range");
+    v *= (int64_t)(std::floor(bh) - std::floor(bl)) + 6;
+  }
+  return v;
+}
 
 }  // namespace
 
@@ -56,8 +81,10 @@ class Server {
       batch_.step_complete();
     } catch (...) {
     }
-    for (auto& r : reqs_)
+    for (auto& r : reqs_) {
       if (r->pinned) cudaHostUnregister(r->records.data());
+      if (r->done) cudaEventDestroy(r->done);
+    }
     for (cudaEvent_t e : {ev_base_, ev_start_, ev_end_})
       if (e) cudaEventDestroy(e);
     if (main_s_) cudaStreamDestroy(main_s_);
@@ -71,8 +98,12 @@ class Server {
                  int64_t steps, double arrival) {
     if (n < 0 || (n > 0 && !rec) || steps < 0 || !p || nc < 0 || (nc > 0 && !c))
       throw Error(SNOW_E_ARG, "bad request");
+    if (!(p->grid_spacing > 0.0) || !std::isfinite(p->grid_spacing))
+      throw Error(SNOW_E_ARG, "grid_spacing must be positive and finite");
+    const int64_t box = host_box_blocks(rec, n, p->grid_spacing);
     auto r = std::make_unique<Request>();
     r->id = (int64_t)reqs_.size();
+    r->box_blocks = box;
     r->records.assign(rec, rec + n * 26);
     // page-lock the request's records so uploads and result copies run as
     // direct DMA (without it they go through the batch's staging chunks)
@@ -93,36 +124,45 @@ class Server {
   // Device bytes a scene of n particles holds: two particle buffers, sort
   // buffers, and its share of the grid (about one 4x4x4 block per 32
   // particles, with the grid's 2x headroom).
+  int64_t per_particle_bytes() const {
+    const int64_t real = prec_ == SNOW_FP64 ? 8 : 4;
+    return 2 * (kRealPlanes * real + kFPPlanes * 8 + 4) + 16 + 26 * 8 / 4;
+  }
   int64_t footprint(int64_t n) const {
     const int64_t real = prec_ == SNOW_FP64 ? 8 : 4;
-    const int64_t per_particle = 2 * (kRealPlanes * real + kFPPlanes * 8 + 4) + 16 + 26 * 8 / 4;
     const int64_t grid = 2 * ((n + 31) / 32) * 64 * (kAccCh + kVelCh) * real;
-    return n * per_particle + grid + (1 << 16);
+    return n * per_particle_bytes() + grid + (1 << 16);
   }
 
-  // One tick: launch the live scenes' steps, set up newly arrived requests in
-  // a second batch on a second stream while those steps run, wait for the
-  // steps, retire finished scenes, then move the new ones into the live batch
-  // (without copying their particles) for the next tick.
+  // The loop allocates nothing: streams, events and every buffer that scales
+  // with the requests are made before it (a cudaMalloc or cudaFree inside it
+  // can wait for the tick in flight).  Each pass launches a tick of steps for
+  // the live scenes, then, while it runs, issues the setup of newly arrived
+  // requests in a second batch on a second stream and the result copies of
+  // finished scenes on a third, without waiting for either; after the tick it
+  // moves the set-up scenes whose work has passed into the live batch
+  // (without copying their particles), finished scenes out of it, and
+  // releases scenes whose results have arrived.
   void run(cudaStream_t s) {
+    const auto t0 = clock_t_::now();
+    auto now = [&] { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
     if (!s) s = main_stream();
     std::vector<Request*> order;
     for (auto& r : reqs_)
       if (r->finished < 0 && !r->rejected) order.push_back(r.get());
     std::stable_sort(order.begin(), order.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
     std::deque<Request*> pending(order.begin(), order.end());
-    std::vector<Request*> live, arriving, leaving;
+    std::vector<Request*> live, admitting, leaving;
     int64_t used = 0;
     ticks_log_.clear();
     bool base_recorded = false;
-    for (cudaEvent_t* e : {&ev_base_, &ev_start_, &ev_end_})
-      if (!*e) check_cuda(cudaEventCreate(e), "cudaEventCreate");
-    const auto t0 = clock_t_::now();
-    auto now = [&] { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
-    while (!pending.empty() || !live.empty() || !leaving.empty()) {
-      // launch this tick (the steps run while the host admits below)
+    double t_phase = now();
+    reserve(order, s);
+    admit_s_ += now() - t_phase;
+    while (!pending.empty() || !live.empty() || !admitting.empty() || !leaving.empty()) {
+      // launch this tick (the steps run while the host admits and retires below)
       int64_t k = 0;
-      double t_phase = now();
+      t_phase = now();
       snow_server_tick tick{};
       tick.host_start_s = t_phase;
       if (!live.empty()) {
@@ -140,7 +180,7 @@ class Server {
         check_cuda(cudaEventRecord(ev_end_, s), "cudaEventRecord");
       }
       step_s_ += now() - t_phase;
-      // admit every arrived request that fits, in arrival order
+      // issue the setup of every arrived request that fits, in arrival order
       t_phase = now();
       while (!pending.empty() && pending.front()->arrival <= now()) {
         Request* r = pending.front();
@@ -150,23 +190,24 @@ class Server {
           ++rejected_;
           continue;
         }
-        if (used + r->bytes > budget_ || (int)(live.size() + arriving.size()) >= max_scenes_) break;
+        if (used + r->bytes > budget_ || (int)(live.size() + admitting.size()) >= max_scenes_) break;
         pending.pop_front();
         const int64_t n = (int64_t)r->records.size() / 26;
         r->scene = admit_.add_scene(r->records.data(), n, &r->params, r->colliders.data(),
-                                    (int)r->colliders.size(), admit_stream());
-        admit_.setup(r->scene, r->params.grid_spacing, admit_stream());
+                                    (int)r->colliders.size(), admit_stream(), /*wait=*/!r->pinned);
+        admit_.setup(r->scene, r->params.grid_spacing, admit_stream(), r->box_blocks, /*wait=*/false);
+        check_cuda(cudaEventRecord(r->done, admit_stream()), "cudaEventRecord");
         r->remaining = r->steps;
         r->admitted = now();
         used += r->bytes;
-        arriving.push_back(r);
-        peak_scenes_ = std::max<int64_t>(peak_scenes_, (int64_t)(live.size() + arriving.size()));
+        admitting.push_back(r);
+        peak_scenes_ = std::max<int64_t>(peak_scenes_, (int64_t)(live.size() + admitting.size()));
         peak_bytes_ = std::max(peak_bytes_, used);
       }
       admit_s_ += now() - t_phase;
-      // results of the scenes that finished last tick, copied back while this tick runs
+      // release the scenes whose results have arrived
       t_phase = now();
-      drain(leaving, used, now);
+      collect_results(leaving, used, now, false);
       retire_s_ += now() - t_phase;
       // complete the tick
       if (k > 0) {
@@ -187,14 +228,31 @@ class Server {
         tick.device_end_s = b * 1e-3;
         tick.steps = k;
         tick.scenes = (int64_t)live.size();
-        tick.admitted = (int64_t)arriving.size();
       }
-      for (Request* r : arriving) {
+      if (live.empty() && !admitting.empty())  // nothing to step: wait for the first setup
+        check_cuda(cudaEventSynchronize(admitting.front()->done), "cudaEventSynchronize");
+      // set-up scenes join the live batch
+      t_phase = now();
+      bool joined = false;
+      for (size_t i = 0; i < admitting.size();) {
+        Request* r = admitting[i];
+        const cudaError_t q = cudaEventQuery(r->done);
+        if (q == cudaErrorNotReady) {
+          ++i;
+          continue;
+        }
+        check_cuda(q, "admission");
+        if (!joined) admit_.collect_status();  // flags of every setup that has passed
+        joined = true;
         r->scene = batch_.adopt_scene(admit_, r->scene);
         live.push_back(r);
+        admitting.erase(admitting.begin() + i);
+        ++tick.admitted;
       }
-      arriving.clear();
-      // finished scenes leave the live batch without a copy
+      admit_s_ += now() - t_phase;
+      // finished scenes leave the live batch without a copy; their results are
+      // copied back on the retire stream while the next tick runs
+      t_phase = now();
       for (size_t i = 0; i < live.size();) {
         Request* r = live[i];
         if (r->remaining > 0) {
@@ -202,21 +260,24 @@ class Server {
           continue;
         }
         r->scene = retired_.adopt_scene(batch_, r->scene);
+        retired_.download(r->scene, r->records.data(), (int64_t)r->records.size() / 26, retire_stream(),
+                          /*wait=*/!r->pinned);
+        check_cuda(cudaEventRecord(r->done, retire_stream()), "cudaEventRecord");
         leaving.push_back(r);
         live.erase(live.begin() + i);
+        ++tick.retired;
       }
-      if (k > 0) {
-        tick.retired = (int64_t)leaving.size();
-        ticks_log_.push_back(tick);
+      if (live.empty() && admitting.empty()) {
+        // nothing runs: finish the copies back, or wait for the next arrival
+        collect_results(leaving, used, now, true);
+        if (!pending.empty()) {
+          const double wait = pending.front()->arrival - now();
+          if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
+        }
       }
-      if (live.empty() && !pending.empty() && leaving.empty()) {
-        const double wait = pending.front()->arrival - now();
-        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
-      }
+      retire_s_ += now() - t_phase;
+      if (k > 0) ticks_log_.push_back(tick);
     }
-    const double t_phase = now();
-    drain(leaving, used, now);
-    retire_s_ += now() - t_phase;
     wall_ += now();
   }
 
@@ -256,19 +317,63 @@ class Server {
   }
 
  private:
-  // Copies finished scenes back from the retired batch (on its own stream) and
-  // releases them; their buffers go back to the admission batch for reuse.
+  // Releases the finished scenes whose result copies have passed (all of
+  // them, waiting, when `wait`); their buffers go back to the admission batch
+  // for reuse.
   template <typename Now>
-  void drain(std::vector<Request*>& leaving, int64_t& used, Now&& now) {
-    for (Request* r : leaving) {
-      const int64_t n = (int64_t)r->records.size() / 26;
-      retired_.download(r->scene, r->records.data(), n, retire_stream());
+  void collect_results(std::vector<Request*>& leaving, int64_t& used, Now&& now, bool wait) {
+    bool any = false;
+    for (size_t i = 0; i < leaving.size();) {
+      Request* r = leaving[i];
+      if (wait) check_cuda(cudaEventSynchronize(r->done), "cudaEventSynchronize");
+      const cudaError_t q = cudaEventQuery(r->done);
+      if (q == cudaErrorNotReady) {
+        ++i;
+        continue;
+      }
+      check_cuda(q, "result copy");
       retired_.remove_scene(r->scene);
       r->finished = now();
       used -= r->bytes;
+      leaving.erase(leaving.begin() + i);
+      any = true;
     }
-    if (!leaving.empty()) retired_.give_cache(admit_);
-    leaving.clear();
+    if (any) retired_.give_cache(admit_);
+  }
+
+  // Everything the loop needs, made before it: streams, events, and buffers
+  // sized for the requests (the live batch's particle buffers, grid and key
+  // bins for all admissible requests at once; the admission batch's for the
+  // largest; the particle buffers of every request that fits the budget).
+  void reserve(const std::vector<Request*>& order, cudaStream_t s) {
+    admit_stream();
+    retire_stream();
+    for (cudaEvent_t* e : {&ev_base_, &ev_start_, &ev_end_})
+      if (!*e) check_cuda(cudaEventCreate(e), "cudaEventCreate");
+    int64_t live_n = 0, scene_max = 0, box_sum = 0, box_max = 0, grid_max = 0, colliders = 0;
+    std::vector<int64_t> sizes;
+    for (Request* r : order) {
+      if (!r->done) check_cuda(cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming), "cudaEventCreate");
+      if (r->bytes > budget_) continue;
+      const int64_t n = (int64_t)r->records.size() / 26;
+      live_n += n;
+      scene_max = std::max(scene_max, n);
+      box_sum += r->box_blocks;
+      box_max = std::max(box_max, r->box_blocks);
+      grid_max = std::max(grid_max, std::min<int64_t>(2 * r->box_blocks + 1024, 8 * n + 1024));
+      sizes.push_back(n);
+      colliders += (int64_t)r->colliders.size();
+    }
+    live_n = std::min(live_n, budget_ / per_particle_bytes());
+    const int slots = (int)std::min<int64_t>((int64_t)sizes.size(), max_scenes_);
+    batch_.reserve(live_n, 0, slots, (int)std::min<int64_t>(colliders, INT32_MAX));
+    batch_.reserve_grid(std::min<int64_t>(2 * box_sum + 1024, std::max<int64_t>(8 * live_n + 64, 1024)), box_sum, s);
+    admit_.reserve(scene_max, scene_max);
+    admit_.reserve_grid(grid_max, box_max, admit_stream());
+    admit_.reserve_scenes(sizes, budget_);
+    retired_.reserve(0, scene_max);
+    check_cuda(cudaStreamSynchronize(s), "reserve");
+    check_cuda(cudaStreamSynchronize(admit_stream()), "reserve");
   }
 
   cudaStream_t main_stream() {
