@@ -185,10 +185,17 @@ Batch::~Batch() {
 
 void Batch::free_scene(Scene& s) {
   for (int k = 0; k < 2; ++k) {
-    dfree(s.r[k]);
-    dfree(s.fp[k]);
-    dfree(s.id[k]);
+    if (s.slab) {
+      s.r[k] = nullptr;
+      s.fp[k] = nullptr;
+      s.id[k] = nullptr;
+    } else {
+      dfree(s.r[k]);
+      dfree(s.fp[k]);
+      dfree(s.id[k]);
+    }
   }
+  s.slab.reset();
   dfree(s.snap);
 }
 
@@ -325,6 +332,7 @@ int32_t Batch::add_scene(const double* records, int64_t n, const snow_step_param
       sc->fp[k] = c.fp[k];
       sc->id[k] = c.id[k];
     }
+    sc->slab = std::move(c.slab);
     cache_.erase(cache_.begin() + best);
   } else {
     for (int k = 0; k < 2; ++k) {
@@ -384,6 +392,7 @@ void Batch::remove_scene(int32_t id) {
         scenes_[k]->fp[b] = nullptr;
         scenes_[k]->id[b] = nullptr;
       }
+      c.slab = std::move(scenes_[k]->slab);
       cache_.push_back(c);
       cached_bytes_ += scene_bytes(c.stride);
       while (cached_bytes_ > cache_limit_ && !cache_.empty()) {
@@ -895,19 +904,35 @@ void Batch::reserve_grid(int64_t blocks, int64_t key_blocks, cudaStream_t s) {
 }
 
 void Batch::reserve_scenes(const std::vector<int64_t>& sizes, int64_t max_bytes) {
+  const auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  std::vector<int64_t> strides;
+  size_t total = 0;
   int64_t bytes = 0;
   for (int64_t n : sizes) {
+    const int64_t st = pad32(std::max<int64_t>(n, 1));
+    if (bytes + scene_bytes(st) > max_bytes) break;
+    bytes += scene_bytes(st);
+    strides.push_back(st);
+    total += 2 * (al((size_t)st * kRealPlanes * rsize_) + al((size_t)st * kFPPlanes * 8) + al((size_t)st * 4));
+  }
+  if (strides.empty()) return;
+  unsigned char* base = dalloc<unsigned char>(total);
+  std::shared_ptr<void> slab(base, [](void* p) { cudaFree(p); });
+  size_t off = 0;
+  for (int64_t st : strides) {
     Scene c;
-    c.stride = pad32(std::max<int64_t>(n, 1));
-    if (bytes + scene_bytes(c.stride) > max_bytes) break;
+    c.stride = st;
     for (int k = 0; k < 2; ++k) {
-      c.r[k] = dalloc<unsigned char>((size_t)c.stride * kRealPlanes * rsize_);
-      c.fp[k] = dalloc<double>((size_t)c.stride * kFPPlanes);
-      c.id[k] = dalloc<int32_t>((size_t)c.stride);
+      c.r[k] = base + off;
+      off += al((size_t)st * kRealPlanes * rsize_);
+      c.fp[k] = reinterpret_cast<double*>(base + off);
+      off += al((size_t)st * kFPPlanes * 8);
+      c.id[k] = reinterpret_cast<int32_t*>(base + off);
+      off += al((size_t)st * 4);
     }
-    bytes += scene_bytes(c.stride);
+    c.slab = slab;
     cache_.push_back(c);
-    cached_bytes_ += scene_bytes(c.stride);
+    cached_bytes_ += scene_bytes(st);
   }
   cache_limit_ = std::max(cache_limit_, cached_bytes_);
 }

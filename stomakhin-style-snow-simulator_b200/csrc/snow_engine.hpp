@@ -34,6 +34,9 @@ struct Scene {
   snow_step_params params{};
   std::vector<Collider> colliders;
   unsigned char* snap = nullptr;  // snapshot of the particle state (snapshot())
+  // Set when r/fp/id are carved from one shared allocation (reserve_scenes),
+  // which is freed when its last piece is dropped; else each is its own.
+  std::shared_ptr<void> slab;
 };
 
 class Batch {
@@ -61,7 +64,7 @@ class Batch {
   // Grid blocks and key blocks to size the grid and the dense bins for now.
   void reserve_grid(int64_t blocks, int64_t key_blocks, cudaStream_t s);
   // Allocates particle buffers for scenes of these sizes into the cache of
-  // removed scenes' buffers, up to `max_bytes`.
+  // removed scenes' buffers, up to `max_bytes`, carved from one allocation.
   void reserve_scenes(const std::vector<int64_t>& sizes, int64_t max_bytes);
   void step(int n_steps, snow_step_timings* timings, cudaStream_t s);
   void step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s);
