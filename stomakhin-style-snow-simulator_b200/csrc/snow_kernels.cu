@@ -711,11 +711,16 @@ struct P2GChannels {
   static constexpr int n = MODE == P2G_MASS ? 1 : (MODE == P2G_MASS_MOMENTUM ? 4 : 7);
 };
 
-// Per-particle record staged in shared memory for the scatter: interleaved
-// (weight, slope) pairs per axis and stencil offset, then m, m v, and the
-// symmetric force matrix.  Record strides (36 floats, 34 doubles) make the
-// 16-byte record stores of a warp conflict-free.
-enum : int { RW_X = 0, RW_Y = 8, RW_Z = 16, R_M = 24, R_MV = 25, R_F = 28, kRecFields = 34 };
+// Per-particle record staged in shared memory for the scatter: the stencil
+// weights and slopes per axis, then m, m v, and the symmetric force matrix.
+// y and z hold (weight, slope) pairs per stencil offset.  In double, x does
+// too and the force matrix is (xx, yy, zz, xy, xz, yz).  In float the record
+// is laid out for the packed two-wide arithmetic of the scatter: x holds
+// (w_q, w_q+2, dw_q, dw_q+2) for q = 0, 1 (the two nodes of a lane) and the
+// force matrix is (xx, xy, xy, yy, xz, yz, zz, 0), whose pairs are the rows
+// M e_x, M e_y, M e_z as the scatter combines them.  Record strides (36
+// floats, 34 doubles) make the 16-byte record stores of a warp conflict-free.
+enum : int { RW_X = 0, RW_Y = 8, RW_Z = 16, R_M = 24, R_MV = 25, R_F = 28 };
 constexpr int kP2GWarps = 8;
 
 template <typename R>
@@ -728,16 +733,111 @@ constexpr size_t p2g_smem() {
   return sizeof(R) * (P2GChannels<R, MODE>::n * TileShape<R>::N + kP2GWarps * 32 * rec_stride<R>());
 }
 
-// Stores a 34-field record with 16-byte stores.
-__device__ __forceinline__ void store_record(float* rr, const float (&v)[kRecFields]) {
+// Stores a record (36 floats, 34 doubles) with 16-byte stores.
+__device__ __forceinline__ void store_record(float* rr, const float (&v)[36]) {
 #pragma unroll
-  for (int k = 0; k < 8; ++k)
+  for (int k = 0; k < 9; ++k)
     reinterpret_cast<float4*>(rr)[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
-  reinterpret_cast<float2*>(rr)[16] = make_float2(v[32], v[33]);
 }
-__device__ __forceinline__ void store_record(double* rr, const double (&v)[kRecFields]) {
+__device__ __forceinline__ void store_record(double* rr, const double (&v)[34]) {
 #pragma unroll
   for (int k = 0; k < 17; ++k) reinterpret_cast<double2*>(rr)[k] = make_double2(v[2 * k], v[2 * k + 1]);
+}
+
+__device__ __forceinline__ float2 splat2(float a) { return make_float2(a, a); }
+
+// The record walk of the scatter below in float, with the packed two-wide
+// arithmetic of sm_100 (__ffma2_rn / __fmul2_rn: two fmaf / fmul in one
+// instruction, same rounding).  Per lane and particle: {A, B, C} from the y and
+// z weights, P = A (m, m v) and U = A M e_x, V = B M e_y + C M e_z as channel
+// pairs, then for each of the lane's two x nodes (w, dw): (m, m v) += w P and
+// f += dw U + w V.
+template <int MODE>
+__device__ __forceinline__ void p2g_walk_f32(const float* wrec, float* tile, int my_cell, int cnt, int lane, int qi,
+                                             int qj, int qk, int col) {
+  constexpr int N = TileShape<float>::N, kRec = rec_stride<float>();
+  constexpr bool kMom = MODE == P2G_FULL || MODE == P2G_PRE || MODE == P2G_MASS_MOMENTUM;
+  constexpr bool kForce = MODE == P2G_FULL || MODE == P2G_PRE || MODE == P2G_FORCE;
+  constexpr bool kMass = MODE != P2G_FORCE;
+  const float2 zero = make_float2(0.f, 0.f);
+  float2 am01[2] = {zero, zero}, am23[2] = {zero, zero}, af01[2] = {zero, zero};
+  float af2[2] = {0.f, 0.f};
+  auto add = [&](int qq) {
+    const float* rr = wrec + qq * kRec;
+    const float2 py = *reinterpret_cast<const float2*>(rr + RW_Y + 2 * qj);
+    const float2 pz = *reinterpret_cast<const float2*>(rr + RW_Z + 2 * qk);
+    const float4 xw = *reinterpret_cast<const float4*>(rr + RW_X + 4 * qi);
+    const float A = py.x * pz.x;
+    const float2 A2 = splat2(A);
+    float2 P01 = zero, P23 = zero;
+    if constexpr (kMass || kMom) {
+      const float4 mm = *reinterpret_cast<const float4*>(rr + R_M);  // m, m v
+      P01 = __fmul2_rn(A2, make_float2(mm.x, mm.y));
+      P23 = __fmul2_rn(A2, make_float2(mm.z, mm.w));
+    }
+    float2 U01 = zero, V01 = zero;
+    float U2 = 0.f, V2 = 0.f;
+    if constexpr (kForce) {
+      const float4 f0 = *reinterpret_cast<const float4*>(rr + R_F);      // xx, xy | xy, yy
+      const float4 f1 = *reinterpret_cast<const float4*>(rr + R_F + 4);  // xz, yz | zz, -
+      const float B = py.y * pz.x, C = py.x * pz.y;
+      U01 = __fmul2_rn(A2, make_float2(f0.x, f0.y));
+      U2 = A * f1.x;
+      V01 = __ffma2_rn(splat2(C), make_float2(f1.x, f1.y), __fmul2_rn(splat2(B), make_float2(f0.z, f0.w)));
+      V2 = fmaf(C, f1.z, B * f1.y);
+    }
+    const float w[2] = {xw.x, xw.y}, dw[2] = {xw.z, xw.w};
+#pragma unroll
+    for (int x = 0; x < 2; ++x) {
+      const float2 w2 = splat2(w[x]);
+      if constexpr (kMass || kMom) {
+        am01[x] = __ffma2_rn(w2, P01, am01[x]);
+        am23[x] = __ffma2_rn(w2, P23, am23[x]);
+      }
+      if constexpr (kForce) {
+        af01[x] = __ffma2_rn(splat2(dw[x]), U01, __ffma2_rn(w2, V01, af01[x]));
+        af2[x] = fmaf(dw[x], U2, fmaf(w[x], V2, af2[x]));
+      }
+    }
+  };
+  auto flush = [&](int at) {
+#pragma unroll
+    for (int x = 0; x < 2; ++x) {
+      float* t = tile + at + col + qi + 2 * x;
+      if constexpr (kMass) atomicAdd(t, am01[x].x);
+      if constexpr (kMom) {
+        atomicAdd(t + N, am01[x].y);
+        atomicAdd(t + 2 * N, am23[x].x);
+        atomicAdd(t + 3 * N, am23[x].y);
+      }
+      if constexpr (kForce) {
+        atomicAdd(t + 4 * N, af01[x].x);
+        atomicAdd(t + 5 * N, af01[x].y);
+        atomicAdd(t + 6 * N, af2[x]);
+      }
+      am01[x] = am23[x] = af01[x] = zero;
+      af2[x] = 0.f;
+    }
+  };
+  // Walk the runs of equal cells (the particles arrive cell-sorted): the run
+  // boundaries come from one ballot, so the inner loop carries no per-particle
+  // cell test.
+  const int prev = __shfl_up_sync(0xffffffffu, my_cell, 1);
+  unsigned starts = __ballot_sync(0xffffffffu, lane < cnt && (lane == 0 || my_cell != prev));
+  while (starts) {
+    const int s0 = __ffs(starts) - 1;
+    starts &= starts - 1;
+    const int e0 = starts ? __ffs(starts) - 1 : cnt;
+    const int cell = __shfl_sync(0xffffffffu, my_cell, s0);
+    if (cell < 0) continue;  // particles outside the tile (flagged by the caller)
+    int qq = s0;
+    for (; qq + 1 < e0; qq += 2) {
+      add(qq);
+      add(qq + 1);
+    }
+    if (qq < e0) add(qq);
+    flush(cell);
+  }
 }
 
 // P2G with the lanes of a warp mapped to stencil nodes rather than particles.
@@ -791,11 +891,16 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
         const R x0 = pv.at(PX, i), x1 = pv.at(PX + 1, i), x2 = pv.at(PX + 2, i);
         const AxisWeights<R> wx = axis_weights(x0, dx), wy = axis_weights(x1, dx), wz = axis_weights(x2, dx);
         const int tx = wx.base - 4 * h.bx, ty = wy.base - 4 * h.by, tz = wz.base - 4 * h.bz;
-        R v[kRecFields];
+        R v[kRec];
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          v[RW_X + 2 * a] = wx.w[a];
-          v[RW_X + 2 * a + 1] = wx.dw[a];
+          if constexpr (sizeof(R) == 4) {
+            v[RW_X + 4 * (a & 1) + (a >> 1)] = wx.w[a];
+            v[RW_X + 4 * (a & 1) + 2 + (a >> 1)] = wx.dw[a];
+          } else {
+            v[RW_X + 2 * a] = wx.w[a];
+            v[RW_X + 2 * a + 1] = wx.dw[a];
+          }
           v[RW_Y + 2 * a] = wy.w[a];
           v[RW_Y + 2 * a + 1] = wy.dw[a];
           v[RW_Z + 2 * a] = wz.w[a];
@@ -810,11 +915,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
           v[R_MV + 2] = m * pv.at(PV + 2, i);
         }
 #pragma unroll
-        for (int e = 0; e < 6; ++e) v[R_F + e] = R(0);
+        for (int e = R_F; e < kRec; ++e) v[e] = R(0);
+        Sym3<R> M{R(0), R(0), R(0), R(0), R(0), R(0)};
         if constexpr (MODE == P2G_PRE) {
           // force matrix left by the previous step's G2P (or prepare_force)
-#pragma unroll
-          for (int e = 0; e < 6; ++e) v[R_F + e] = pv.at(PFM + e, i);
+          M = Sym3<R>{pv.at(PFM, i), pv.at(PFM + 1, i), pv.at(PFM + 2, i),
+                      pv.at(PFM + 3, i), pv.at(PFM + 4, i), pv.at(PFM + 5, i)};
         } else if constexpr (kForce) {
           M3<R> FE;
 #pragma unroll
@@ -823,7 +929,17 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
 #pragma unroll
           for (int e = 0; e < 9; ++e) FP.a[e] = pv.fp[e * pv.st + i];
           const double hard = exp(sc.xi * (1.0 - det3(FP)));
-          const Sym3<R> M = force_matrix<R>(FE, pv.at(PVOL, i), (R)sc.mu0, (R)sc.lambda0, (R)hard);
+          M = force_matrix<R>(FE, pv.at(PVOL, i), (R)sc.mu0, (R)sc.lambda0, (R)hard);
+        }
+        if constexpr (sizeof(R) == 4) {
+          v[R_F] = M.xx;
+          v[R_F + 1] = M.xy;
+          v[R_F + 2] = M.xy;
+          v[R_F + 3] = M.yy;
+          v[R_F + 4] = M.xz;
+          v[R_F + 5] = M.yz;
+          v[R_F + 6] = M.zz;
+        } else {
           v[R_F] = M.xx;
           v[R_F + 1] = M.yy;
           v[R_F + 2] = M.zz;
@@ -838,85 +954,89 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
       }
       __syncwarp();
       const int cnt = min(32, n - base);
-      R acc[2][NCH];
-#pragma unroll
-      for (int x = 0; x < 2; ++x)
-#pragma unroll
-        for (int c = 0; c < NCH; ++c) acc[x][c] = R(0);
-      auto flush = [&](int at) {
+      if constexpr (sizeof(R) == 4) {
+        p2g_walk_f32<MODE>(wrec, tile, my_cell, cnt, lane, qi, qj, qk, col);
+      } else {
+        R acc[2][NCH];
 #pragma unroll
         for (int x = 0; x < 2; ++x)
 #pragma unroll
-          for (int c = 0; c < NCH; ++c) {
-            if (c == 0 && !kMass) continue;
-            if (c >= 1 && c <= 3 && !kMom) continue;
-            atomicAdd(&tile[c * TileShape<R>::N + at + col + qi + 2 * x], acc[x][c]);
-            acc[x][c] = R(0);
-          }
-      };
-      // Walk the runs of equal cells (the particles arrive cell-sorted): the
-      // run boundaries come from one ballot, so the inner loop carries no
-      // per-particle cell test.
-      auto add = [&](int qq) {
-        const R* rr = wrec + qq * kRec;
-        using R2 = typename Vec<R>::two;
-        const R2 py = *reinterpret_cast<const R2*>(rr + RW_Y + 2 * qj);
-        const R2 pz = *reinterpret_cast<const R2*>(rr + RW_Z + 2 * qk);
-        const R A = py.x * pz.x;
-        R P[4], U[3], V[3];
-        {
-          const R2 mm0 = *reinterpret_cast<const R2*>(rr + R_M);      // m, m v_x
-          const R2 mm1 = *reinterpret_cast<const R2*>(rr + R_M + 2);  // m v_y, m v_z
-          P[0] = A * mm0.x;
-          P[1] = A * mm0.y;
-          P[2] = A * mm1.x;
-          P[3] = A * mm1.y;
-        }
-        if constexpr (kForce) {
-          const R2 f0 = *reinterpret_cast<const R2*>(rr + R_F);      // xx, yy
-          const R2 f1 = *reinterpret_cast<const R2*>(rr + R_F + 2);  // zz, xy
-          const R2 f2 = *reinterpret_cast<const R2*>(rr + R_F + 4);  // xz, yz
-          const R B = py.y * pz.x, C = py.x * pz.y;
-          const R mxx = f0.x, myy = f0.y, mzz = f1.x, mxy = f1.y, mxz = f2.x, myz = f2.y;
-          U[0] = A * mxx;
-          U[1] = A * mxy;
-          U[2] = A * mxz;
-          V[0] = B * mxy + C * mxz;
-          V[1] = B * myy + C * myz;
-          V[2] = B * myz + C * mzz;
-        }
+          for (int c = 0; c < NCH; ++c) acc[x][c] = R(0);
+        auto flush = [&](int at) {
 #pragma unroll
-        for (int x = 0; x < 2; ++x) {
-          const R2 px = *reinterpret_cast<const R2*>(rr + RW_X + 2 * (qi + 2 * x));
-          const R wxv = px.x, dwx = px.y;
-          if constexpr (kMass) acc[x][0] += wxv * P[0];
-          if constexpr (kMom) {
-            acc[x][1] += wxv * P[1];
-            acc[x][2] += wxv * P[2];
-            acc[x][3] += wxv * P[3];
+          for (int x = 0; x < 2; ++x)
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) {
+              if (c == 0 && !kMass) continue;
+              if (c >= 1 && c <= 3 && !kMom) continue;
+              atomicAdd(&tile[c * TileShape<R>::N + at + col + qi + 2 * x], acc[x][c]);
+              acc[x][c] = R(0);
+            }
+        };
+        // Walk the runs of equal cells (the particles arrive cell-sorted): the
+        // run boundaries come from one ballot, so the inner loop carries no
+        // per-particle cell test.
+        auto add = [&](int qq) {
+          const R* rr = wrec + qq * kRec;
+          using R2 = typename Vec<R>::two;
+          const R2 py = *reinterpret_cast<const R2*>(rr + RW_Y + 2 * qj);
+          const R2 pz = *reinterpret_cast<const R2*>(rr + RW_Z + 2 * qk);
+          const R A = py.x * pz.x;
+          R P[4], U[3], V[3];
+          {
+            const R2 mm0 = *reinterpret_cast<const R2*>(rr + R_M);      // m, m v_x
+            const R2 mm1 = *reinterpret_cast<const R2*>(rr + R_M + 2);  // m v_y, m v_z
+            P[0] = A * mm0.x;
+            P[1] = A * mm0.y;
+            P[2] = A * mm1.x;
+            P[3] = A * mm1.y;
           }
           if constexpr (kForce) {
-            acc[x][4] += dwx * U[0] + wxv * V[0];
-            acc[x][5] += dwx * U[1] + wxv * V[1];
-            acc[x][6] += dwx * U[2] + wxv * V[2];
+            const R2 f0 = *reinterpret_cast<const R2*>(rr + R_F);      // xx, yy
+            const R2 f1 = *reinterpret_cast<const R2*>(rr + R_F + 2);  // zz, xy
+            const R2 f2 = *reinterpret_cast<const R2*>(rr + R_F + 4);  // xz, yz
+            const R B = py.y * pz.x, C = py.x * pz.y;
+            const R mxx = f0.x, myy = f0.y, mzz = f1.x, mxy = f1.y, mxz = f2.x, myz = f2.y;
+            U[0] = A * mxx;
+            U[1] = A * mxy;
+            U[2] = A * mxz;
+            V[0] = B * mxy + C * mxz;
+            V[1] = B * myy + C * myz;
+            V[2] = B * myz + C * mzz;
           }
+#pragma unroll
+          for (int x = 0; x < 2; ++x) {
+            const R2 px = *reinterpret_cast<const R2*>(rr + RW_X + 2 * (qi + 2 * x));
+            const R wxv = px.x, dwx = px.y;
+            if constexpr (kMass) acc[x][0] += wxv * P[0];
+            if constexpr (kMom) {
+              acc[x][1] += wxv * P[1];
+              acc[x][2] += wxv * P[2];
+              acc[x][3] += wxv * P[3];
+            }
+            if constexpr (kForce) {
+              acc[x][4] += dwx * U[0] + wxv * V[0];
+              acc[x][5] += dwx * U[1] + wxv * V[1];
+              acc[x][6] += dwx * U[2] + wxv * V[2];
+            }
+          }
+        };
+        const int prev = __shfl_up_sync(0xffffffffu, my_cell, 1);
+        unsigned starts = __ballot_sync(0xffffffffu, lane < cnt && (lane == 0 || my_cell != prev));
+        while (starts) {
+          const int s0 = __ffs(starts) - 1;
+          starts &= starts - 1;
+          const int e0 = starts ? __ffs(starts) - 1 : cnt;
+          const int cell = __shfl_sync(0xffffffffu, my_cell, s0);
+          if (cell < 0) continue;  // particles outside the tile (flagged above)
+          int qq = s0;
+          for (; qq + 1 < e0; qq += 2) {
+            add(qq);
+            add(qq + 1);
+          }
+          if (qq < e0) add(qq);
+          flush(cell);
         }
-      };
-      const int prev = __shfl_up_sync(0xffffffffu, my_cell, 1);
-      unsigned starts = __ballot_sync(0xffffffffu, lane < cnt && (lane == 0 || my_cell != prev));
-      while (starts) {
-        const int s0 = __ffs(starts) - 1;
-        starts &= starts - 1;
-        const int e0 = starts ? __ffs(starts) - 1 : cnt;
-        const int cell = __shfl_sync(0xffffffffu, my_cell, s0);
-        if (cell < 0) continue;  // particles outside the tile (flagged above)
-        int qq = s0;
-        for (; qq + 1 < e0; qq += 2) {
-          add(qq);
-          add(qq + 1);
-        }
-        if (qq < e0) add(qq);
-        flush(cell);
       }
       __syncwarp();
     }
