@@ -24,18 +24,32 @@ struct AxisWeights {
 // The grid position x / dx is a true division, as in the reference, so the
 // stencil base is the reference's exactly; the slopes are scaled by 1 / dx
 // (one rounding away from the reference's N_dash / dx).
+//
+// With f = gp - floor(gp) the four nodes sit at distances 1 + f, f, 1 - f and
+// 2 - f from gp, each inside one fixed piece of N and N_dash (grid.cpp:24-58),
+// so the weights and slopes are those pieces written as polynomials in f and
+// g = 1 - f, without the per-node branches:
+//   w  = (g^3/6,  f^3/2 - f^2 + 2/3,  g^3/2 - g^2 + 2/3,  f^3/6)
+//   dw = (-g^2/2, 3f^2/2 - 2f,       -(3g^2/2 - 2g),      f^2/2)
+// (equal to bspline / bspline_slope up to rounding).
 template <typename T>
 SNOW_HD AxisWeights<T> axis_weights(T x, T dx) {
+  using std::floor;
   AxisWeights<T> a;
   const T gp = x / dx;
   const T inv_dx = T(1) / dx;
-  a.base = stencil_base(gp);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const T node = static_cast<T>(a.base + i);
-    a.w[i] = bspline(node, gp);
-    a.dw[i] = bspline_slope(node, gp) * inv_dx;
-  }
+  const T fl = floor(gp);
+  a.base = static_cast<int>(fl) - 1;  // stencil_base(gp)
+  const T f = gp - fl, g = T(1) - f;
+  const T f2 = f * f, g2 = g * g;
+  a.w[0] = g2 * g * T(1.0 / 6.0);
+  a.w[1] = (T(0.5) * f - T(1)) * f2 + T(2.0 / 3.0);
+  a.w[2] = (T(0.5) * g - T(1)) * g2 + T(2.0 / 3.0);
+  a.w[3] = f2 * f * T(1.0 / 6.0);
+  a.dw[0] = -T(0.5) * g2 * inv_dx;
+  a.dw[1] = (T(1.5) * f - T(2)) * f * inv_dx;
+  a.dw[2] = -(T(1.5) * g - T(2)) * g * inv_dx;
+  a.dw[3] = T(0.5) * f2 * inv_dx;
   return a;
 }
 
