@@ -98,3 +98,13 @@ def test_autotune_restores_state(snow):
     tuned.step(4)
     for a, b in zip(rid, tid):
         assert max(errors(tuned.download(b), ref.download(a)).values()) < 1e-12
+
+
+def test_submit_rejects_nonfinite(snow):
+    sc = _requests(1, seed=3)[0][0]
+    sc.particles[7, 1] = float("nan")
+    srv = snow.Server(0)
+    with pytest.raises(snow.SnowError) as e:
+        srv.submit(sc, 3, 0.0)
+    assert e.value.code == -4
+    srv.close()
