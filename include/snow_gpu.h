@@ -216,6 +216,12 @@ int snow_gpu_server_stats(snow_gpu_server* server, snow_server_stats* stats);
  * start event), steps, live scenes and particles, and the scenes admitted into
  * and retired from the live batch after it.  *count = ticks recorded; at most
  * `capacity` are copied. */
+/* Particles per P2G/G2P work item of the live batch: 0 (the default) chooses
+ * it in run() from the particles of all admissible requests (the largest
+ * power of two in [256, 1024] that leaves about eight items per resident CTA),
+ * else a power of two in [32, 1024].  Results do not depend on it beyond the
+ * order of atomic sums.  No reference counterpart. */
+int snow_gpu_server_set_work_item(snow_gpu_server* server, int particles);
 typedef struct snow_server_tick {
   double host_start_s, host_end_s, device_start_s, device_end_s;
   int64_t steps, scenes, particles, admitted, retired;

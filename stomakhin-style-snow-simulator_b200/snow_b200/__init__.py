@@ -132,6 +132,7 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_server_result": (ctypes.c_int, [vp, i64, _dp, i64, _dp]),
         "snow_gpu_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
         "snow_gpu_server_ticks": (ctypes.c_int, [vp, ctypes.POINTER(ServerTick), i64, _i64p]),
+        "snow_gpu_server_set_work_item": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_set_chunk": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_set_dense": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_graph_kernels": (ctypes.c_int, [vp]),
@@ -465,10 +466,12 @@ class Server:
     """Continuous-batching server of independent scenes (snow_gpu_server_*)."""
 
     def __init__(self, precision: int = SNOW_FP64, budget_bytes: int = 150 * 10**9, max_scenes: int = 4096,
-                 max_steps_per_tick: int = 16):
+                 max_steps_per_tick: int = 16, work_item: int = 0):
         self._h = ctypes.c_void_p()
         _check(lib().snow_gpu_server_create(ctypes.byref(self._h), precision, int(budget_bytes), int(max_scenes),
                                             int(max_steps_per_tick)))
+        if work_item:
+            _check(lib().snow_gpu_server_set_work_item(self._h, int(work_item)))
         self.sizes: dict[int, int] = {}
 
     def close(self) -> None:

@@ -30,10 +30,10 @@ def _alone(snow, prec, sc, steps):
     return out
 
 
-@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 1e-5)])
-def test_served_results_match_alone(snow, prec, tol):
+@pytest.mark.parametrize("prec,tol,item", [(0, 1e-12, 0), (1, 1e-5, 0), (0, 1e-12, 1024), (1, 1e-5, 64)])
+def test_served_results_match_alone(snow, prec, tol, item):
     reqs = _requests()
-    srv = snow.Server(prec, max_steps_per_tick=8)
+    srv = snow.Server(prec, max_steps_per_tick=8, work_item=item)
     ids = [srv.submit(sc, steps, t) for sc, steps, t in reqs]
     srv.run()
     st = srv.stats()
@@ -108,3 +108,9 @@ def test_submit_rejects_nonfinite(snow):
         srv.submit(sc, 3, 0.0)
     assert e.value.code == -4
     srv.close()
+
+
+def test_work_item_size_checked(snow):
+    for bad in (100, 16, 2048, -1):
+        with pytest.raises(snow.SnowError):
+            snow.Server(0, work_item=bad)
