@@ -109,12 +109,33 @@ SNOW_HD void sym_mul_inplace(const Sym3<T>& D, M3<double>& F) {
 // t = sgn(a) b / (|a| + sqrt(a^2 + b^2)), a = a_qq - a_pp, b = 2 a_pq
 // (numerator and denominator multiplied by |b|): one division, one square
 // root, and cos = rsqrt(1 + t^2).
+//
+// 1 / sqrt(x) for x in [1, 2] (the rotation's 1 + t^2, |t| <= 1): in double on
+// the device, a float seed refined by two Newton-Raphson steps for the
+// reciprocal square root, y <- y (3 - x y^2) / 2, each of which squares the
+// relative error (seed 2^-22 -> 2^-44 -> below the double rounding).
+template <typename T>
+SNOW_HD T rsqrt_unit(T x) {
+#ifdef __CUDA_ARCH__
+  if constexpr (sizeof(T) == 8) {
+    T y = (T)rsqrtf((float)x);
+    y = y * (T(1.5) - T(0.5) * x * y * y);
+    y = y * (T(1.5) - T(0.5) * x * y * y);
+    return y;
+  } else {
+    return rsqrt(x);
+  }
+#else
+  return T(1) / std::sqrt(x);
+#endif
+}
+
 template <typename T>
 SNOW_HD void rotate_pq(T& app, T& aqq, T& apq, T& arp, T& arq, T q[9], int p, int qq) {
   if (apq == T(0)) return;
   const T a = aqq - app, b = T(2) * apq;
   const T t = (a >= T(0) ? b : -b) / (fabs(a) + sqrt(a * a + b * b));
-  const T c = rsqrt(t * t + T(1));
+  const T c = rsqrt_unit(t * t + T(1));
   const T s = t * c;
   app -= t * apq;
   aqq += t * apq;
@@ -292,9 +313,18 @@ SNOW_HD Plastic<T> plastic_projection(M3<T>& FE, T lo, T hi) {
     const T sc = s < lo ? lo : (s > hi ? hi : s);  // std::clamp (grid.cpp:281-283)
     if (sc != s) out.clamped = true;
     if (!(s > T(1e-6))) out.regular = false;
-    r[i] = s > T(0) ? sc / s : T(1);
-    ri[i] = s > T(0) ? s / sc : T(1);
-    e[i] = s > T(0) ? sc / (s * s) : T(0);
+    // r = sc / s, ri = s / sc, e = sc / s^2 with one division where no clamp acts
+    r[i] = ri[i] = T(1);
+    e[i] = T(0);
+    if (s > T(0)) {
+      const T inv = T(1) / s;
+      e[i] = inv;
+      if (sc != s) {
+        r[i] = sc * inv;
+        ri[i] = s / sc;
+        e[i] = r[i] * inv;
+      }
+    }
   }
   out.root = sandwich(FE, spectral(q, e));
   if (!out.clamped) {
