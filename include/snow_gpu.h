@@ -158,8 +158,13 @@ int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable);
  * last step (a singular value within 1e-5 of a clamp bound, or a clamp acting
  * with two singular values within 1e-5 of each other).  0 for an FP64 batch. */
 int64_t snow_gpu_batch_fp64_projections(snow_gpu_batch* batch);
-/* Particles per P2G/G2P work item (power of two in [32, 1024]; default 256). */
+/* Particles per P2G/G2P work item (power of two in [32, 1024]).  Until set
+ * (or chosen by snow_gpu_batch_autotune) it follows the batch's particle
+ * count: the largest power of two in [256, 1024] that leaves about eight work
+ * items per resident CTA (256 for up to ~1.8M particles on a B200). */
 int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk);
+/* The work-item size the last step used (or will use), or SNOW_E_ARG. */
+int snow_gpu_batch_chunk(snow_gpu_batch* batch);
 /* Particle ordering: 1 (default) a counting sort over dense per-cell key bins
  * with direct block lookup, used while the scenes' key boxes need at most
  * 2^26 bins; 0 the radix sort with the block hash table.  Both give the same

@@ -481,6 +481,13 @@ SceneDev Batch::scene_dev(const Scene& sc, int64_t begin) const {
   return d;
 }
 
+int auto_chunk(int64_t particles) {
+  const int64_t per = particles / (8 * 3 * (int64_t)sm_count());
+  int c = 256;
+  while (c < 1024 && 2 * c <= per) c *= 2;
+  return c;
+}
+
 void Batch::reserve(int64_t particles, int64_t staging, int scenes, int colliders) {
   if (particles < 0 || staging < 0 || scenes < 0 || colliders < 0) throw Error(SNOW_E_ARG, "negative reservation");
   step_complete();
@@ -600,6 +607,13 @@ void Batch::prepare(cudaStream_t s) {
     coll_.insert(coll_.end(), sc->colliders.begin(), sc->colliders.end());
     table_.push_back(d);
     total_ += sc->n;
+  }
+  if (chunk_auto_) {
+    const int c = auto_chunk(total_);
+    if (c != chunk_) {
+      chunk_ = c;
+      cap_items_ = 0;  // re-sized by ensure_grid below
+    }
   }
   if ((int)table_.size() > d_scenes_cap_) {
     dfree(d_scenes_);
@@ -1197,6 +1211,9 @@ int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk) {
     SNOW_BATCH_OR_FAIL;
     batch->impl->set_chunk(chunk);
   });
+}
+int snow_gpu_batch_chunk(snow_gpu_batch* batch) {
+  return batch && batch->impl ? batch->impl->chunk() : SNOW_E_ARG;
 }
 int snow_gpu_batch_sort_mode(snow_gpu_batch* batch) {
   return batch && batch->impl ? (batch->impl->dense() ? 1 : 0) : SNOW_E_ARG;

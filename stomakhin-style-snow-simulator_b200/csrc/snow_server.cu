@@ -349,25 +349,14 @@ class Server {
     if (any) retired_.give_cache(admit_);
   }
 
-  // Particles per P2G/G2P work item for the live batch: the largest power of
-  // two in [256, 1024] that still gives every resident CTA (3 per SM) about
-  // eight items when all admissible requests are live.  Larger items stage
-  // each grid block's node tile fewer times (a block of a many-scene batch
-  // holds a few hundred particles); too few items leave SMs idle at the end of
-  // each pass.  Measured on the 48-request stream: 1024 beats 512 and 256
-  // (3.29, 3.26, 3.08e9 particle-steps/s); the autotuner picks 1024 for the
-  // 256-scene batch and 256 for one 650k-particle scene.
+  // Particles per P2G/G2P work item for the live batch, fixed for the run:
+  // auto_chunk of all admissible requests' particles (measured on the
+  // 48-request stream: 3.29, 3.26, 3.08e9 particle-steps/s at 1024, 512, 256).
   int auto_work_item(const std::vector<Request*>& order) const {
     int64_t live = 0;
     for (Request* r : order)
       if (r->bytes <= budget_) live += (int64_t)r->records.size() / 26;
-    live = std::min(live, budget_ / per_particle_bytes());
-    int dev = 0, sms = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t per = live / (8 * 3 * (int64_t)std::max(sms, 1));
-    int chunk = 256;
-    while (chunk < 1024 && 2 * chunk <= per) chunk *= 2;
-    return chunk;
+    return auto_chunk(std::min(live, budget_ / per_particle_bytes()));
   }
 
   // Everything the loop needs, made before it: streams, events, and buffers

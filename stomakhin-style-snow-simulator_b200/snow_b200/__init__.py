@@ -135,6 +135,7 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_server_set_work_item": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_set_chunk": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_set_dense": (ctypes.c_int, [vp, ctypes.c_int]),
+        "snow_gpu_batch_chunk": (ctypes.c_int, [vp]),
         "snow_gpu_batch_graph_kernels": (ctypes.c_int, [vp]),
         "snow_gpu_batch_sort_mode": (ctypes.c_int, [vp]),
         "snow_gpu_batch_snapshot": (ctypes.c_int, [vp, ctypes.c_int32, vp]),
@@ -326,6 +327,13 @@ class Batch:
     def set_dense(self, enable: bool) -> None:
         """Counting sort over dense key bins (default) or the radix sort with the block hash table."""
         _check(lib().snow_gpu_batch_set_dense(self._h, int(bool(enable))))
+
+    def chunk(self) -> int:
+        """Particles per work item of the last (or next) step."""
+        c = lib().snow_gpu_batch_chunk(self._h)
+        if c < 0:
+            _check(c)
+        return c
 
     def set_chunk(self, chunk: int) -> None:
         """Particles per P2G/G2P work item (power of two, 32..1024)."""

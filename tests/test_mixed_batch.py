@@ -109,3 +109,28 @@ def test_setup_in_batch_leaves_other_scenes_alone(snow):
         want = snow.setup(s.particles.copy(), s.dx)
         got = b.download(sid)
         assert np.max(np.abs(got[:, 7] / want[:, 7] - 1)) < 1e-12
+
+
+def test_automatic_work_item_size(snow):
+    """A batch that has not been given a work-item size takes one from its
+    particle count (about eight items per resident CTA, 256..1024); the result
+    equals the same steps at a fixed 256 up to the order of atomic sums."""
+    import torch
+    from snow_b200 import scenes
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    sc = scenes.snowball_scene(n=2_000_000)
+    want = 256
+    while want < 1024 and 2 * want <= sc.n // (24 * sms):
+        want *= 2
+    auto, fixed = snow.Batch(snow.SNOW_FP64), snow.Batch(snow.SNOW_FP64)
+    fixed.set_chunk(256)
+    ia, ib = auto.add(sc), fixed.add(sc)
+    auto.setup(ia, sc.dx)
+    fixed.setup(ib, sc.dx)
+    auto.step(3)
+    fixed.step(3)
+    assert auto.chunk() == want and fixed.chunk() == 256
+    assert max(errors(auto.download(ia), fixed.download(ib)).values()) < 1e-12
+    auto.close()
+    fixed.close()
