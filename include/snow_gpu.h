@@ -160,8 +160,9 @@ int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable);
 int64_t snow_gpu_batch_fp64_projections(snow_gpu_batch* batch);
 /* Particles per P2G/G2P work item (power of two in [32, 1024]).  Until set
  * (or chosen by snow_gpu_batch_autotune) it follows the batch's particle
- * count: the largest power of two in [256, 1024] that leaves about eight work
- * items per resident CTA (256 for up to ~1.8M particles on a B200). */
+ * count: the largest power of two in [256, 1024] that leaves about four work
+ * items per resident CTA of the particle kernels (2 per SM in FP64, 3 in the
+ * mixed form). */
 int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk);
 /* The work-item size the last step used (or will use), or SNOW_E_ARG. */
 int snow_gpu_batch_chunk(snow_gpu_batch* batch);
@@ -222,9 +223,8 @@ int snow_gpu_server_stats(snow_gpu_server* server, snow_server_stats* stats);
  * and retired from the live batch after it.  *count = ticks recorded; at most
  * `capacity` are copied. */
 /* Particles per P2G/G2P work item of the live batch: 0 (the default) chooses
- * it in run() from the particles of all admissible requests (the largest
- * power of two in [256, 1024] that leaves about eight items per resident CTA),
- * else a power of two in [32, 1024].  Results do not depend on it beyond the
+ * it in run() from the particles of all admissible requests, by the rule of
+ * snow_gpu_batch_set_chunk, else a power of two in [32, 1024].  Results do not depend on it beyond the
  * order of atomic sums.  No reference counterpart. */
 int snow_gpu_server_set_work_item(snow_gpu_server* server, int particles);
 typedef struct snow_server_tick {

@@ -481,8 +481,9 @@ SceneDev Batch::scene_dev(const Scene& sc, int64_t begin) const {
   return d;
 }
 
-int auto_chunk(int64_t particles) {
-  const int64_t per = particles / (8 * 3 * (int64_t)sm_count());
+int auto_chunk(int64_t particles, int precision) {
+  const int64_t per_sm = precision == SNOW_FP64 ? 2 : 3;
+  const int64_t per = particles / (4 * per_sm * (int64_t)sm_count());
   int c = 256;
   while (c < 1024 && 2 * c <= per) c *= 2;
   return c;
@@ -609,7 +610,7 @@ void Batch::prepare(cudaStream_t s) {
     total_ += sc->n;
   }
   if (chunk_auto_) {
-    const int c = auto_chunk(total_);
+    const int c = auto_chunk(total_, prec_);
     if (c != chunk_) {
       chunk_ = c;
       cap_items_ = 0;  // re-sized by ensure_grid below

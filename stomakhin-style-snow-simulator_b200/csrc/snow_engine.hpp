@@ -21,14 +21,16 @@ struct Error : std::runtime_error {
 
 int set_error(int code, const std::string& msg);
 
-// Particles per P2G/G2P work item for `particles` in a batch: the largest power
-// of two in [256, 1024] that still leaves about eight items per resident CTA
-// (3 per SM).  Larger items stage a grid block's node tile fewer times; too few
+// Particles per P2G/G2P work item for `particles` in a batch of `precision`:
+// the largest power of two in [256, 1024] that still leaves about four items
+// per resident CTA of the particle kernels (2 per SM in FP64, 3 in the mixed
+// form).  Larger items stage a grid block's node tile fewer times; too few
 // items leave SMs idle at the end of each pass.  Measured on one B200: a 4M
 // particle sphere steps 10% faster at 1024 than at 256 (FP64 1.63 vs 1.82 ms,
-// mixed 0.89 vs 0.98 ms); two tori of 650k particles are fastest at 256-512
-// and 13% slower at 1024.
-int auto_chunk(int64_t particles);
+// mixed 0.89 vs 0.98 ms); two tori of 650k particles step fastest at 512 in
+// FP64 (0.3154 vs 0.3196 ms at 256) and at 256-512 in the mixed form, and
+// 13% slower at 1024.
+int auto_chunk(int64_t particles, int precision);
 void check_cuda(cudaError_t e, const char* what);
 
 // One scene: its particle planes (two buffers), parameters and colliders.

@@ -356,7 +356,7 @@ class Server {
     int64_t live = 0;
     for (Request* r : order)
       if (r->bytes <= budget_) live += (int64_t)r->records.size() / 26;
-    return auto_chunk(std::min(live, budget_ / per_particle_bytes()));
+    return auto_chunk(std::min(live, budget_ / per_particle_bytes()), prec_);
   }
 
   // Everything the loop needs, made before it: streams, events, and buffers

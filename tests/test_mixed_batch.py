@@ -113,15 +113,16 @@ def test_setup_in_batch_leaves_other_scenes_alone(snow):
 
 def test_automatic_work_item_size(snow):
     """A batch that has not been given a work-item size takes one from its
-    particle count (about eight items per resident CTA, 256..1024); the result
-    equals the same steps at a fixed 256 up to the order of atomic sums."""
+    particle count (about four items per resident CTA, 2 per SM in FP64,
+    256..1024); the result equals the same steps at a fixed 256 up to the
+    order of atomic sums."""
     import torch
     from snow_b200 import scenes
 
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     sc = scenes.snowball_scene(n=2_000_000)
     want = 256
-    while want < 1024 and 2 * want <= sc.n // (24 * sms):
+    while want < 1024 and 2 * want <= sc.n // (8 * sms):
         want *= 2
     auto, fixed = snow.Batch(snow.SNOW_FP64), snow.Batch(snow.SNOW_FP64)
     fixed.set_chunk(256)
