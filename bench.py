@@ -46,8 +46,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tori", choices=["tori", "cube", "snowball", "batch"],
-                    help="batch: the 256 independent scenes, split across ranks by work (strong scaling)")
+    ap.add_argument("--workload", default="tori", choices=["tori", "touching", "cube", "snowball", "batch", "served"],
+                    help="batch: the 256 independent scenes, split across ranks by work (strong scaling); "
+                         "touching: the two tori placed in contact (plastic flow from the first steps); "
+                         "served: the request stream through the server (single GPU)")
+    ap.add_argument("--particles", type=int, default=0,
+                    help="tori/touching with this many particles instead of 650,000 (small cases for ncu)")
+    ap.add_argument("--requests", type=int, default=48, help="served: number of requests in the stream")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -55,11 +60,14 @@ def parse():
     return ap.parse_args()
 
 
-def workload(name: str):
+def workload(name: str, particles: int = 0):
     from snow_b200 import scenes
 
+    per = particles // 2 if particles else 325_000
     if name == "tori":
-        return scenes.tori_scene()
+        return scenes.tori_scene(n_per_torus=per)
+    if name == "touching":
+        return scenes.tori_scene(n_per_torus=per, gap=0.0)
     if name == "cube":
         return scenes.cube_scene(32)
     return scenes.snowball_scene()
@@ -137,7 +145,7 @@ def run_reference(args, ws, rank):
         }
         print(json.dumps(line), flush=True)
         return
-    sc = workload(args.workload)
+    sc = workload(args.workload, args.particles)
     rate, steps, wall, kind, what = cpu_rate(sc, max(1, args.steps))
     cores = os.cpu_count()
     line = {
@@ -239,17 +247,18 @@ def timed_steps(batch, steps, sp, torch) -> float:
     return e0.elapsed_time(e1)
 
 
-def plain_fp64_rate(snow_b200, torch, sp, items) -> float:
+def plain_fp64_rate(snow_b200, torch, sp, items, settle: int = 0) -> float:
     """Particle-steps/s of the plain FP64 path on the given scenes: each scene
     alone in its own one-scene batch (the drop-in step on resident state, with
     its captured step graph), one scene after another.  items: (scene, steps,
-    timed steps); a scene's time is its timed steps' time scaled to `steps`."""
+    timed steps); a scene's time is its timed steps' time scaled to `steps`;
+    `settle` untimed steps first (as the batch it is compared with had)."""
     particle_steps, ms = 0.0, 0.0
     for sc, n_steps, k in items:
         b = snow_b200.Batch(snow_b200.SNOW_FP64)
         i = b.add(sc, stream=sp)
         b.setup(i, sc.dx, stream=sp)
-        b.step(3, stream=sp)
+        b.step(max(3, settle), stream=sp)
         ms += timed_steps(b, k, sp, torch) * n_steps / k
         particle_steps += sc.n * n_steps
         b.close()
@@ -297,6 +306,8 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
     forms["mixed"] = {"workload": tori.name, "value": rate, "unit": "particle-steps/s",
                       "ms_per_step": ms / steps, "vs_plain_fp64": rate / fp64_rate,
                       "error_vs_fp64": errs}
+    # -- colliding: the same measurements where the snow deforms
+    forms["colliding"] = measure_colliding(snow_b200, torch, sp, steps)
     # -- batched: 256 scenes, FP64 and mixed
     bscenes = scenes.batch_scenes(count=256)
     nb = sum(s.n for s in bscenes)
@@ -397,6 +408,108 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
     return forms
 
 
+def plastic_fraction(rec) -> float:
+    """Fraction of particles whose F_P differs from I (the clamp has acted on them)."""
+    d = np.linalg.norm(rec[:, 8:17] - np.eye(3).reshape(-1), axis=1)
+    return float((d > 1e-6).mean()) if len(d) else 0.0
+
+
+def measure_colliding(snow_b200, torch, sp, steps, settle=40) -> dict:
+    """The deforming regime: snow that strikes snow or the ground from its first
+    steps, so the plastic clamp, the hardening and (in the mixed form) the
+    double-precision fallback are all at work inside the timed window.
+
+    tori      the headline tori placed in contact (gap 0, +-8 m/s): `settle` steps
+              untimed, then `steps` timed, FP64 and mixed; the fallback fraction per
+              step; the fraction of particles with F_P != I; the mixed error against
+              the FP64 path 10 steps on from the settled FP64 state
+    batched   the 256 scenes set on the ground moving down: batched FP64 and mixed
+              against the plain FP64 path one scene at a time
+    served    the request stream set on the ground: served mixed against the plain
+              FP64 path one request at a time
+    """
+    from snow_b200 import scenes
+
+    out = {}
+    sc = scenes.tori_scene(gap=0.0)
+    res, settled = {}, None
+    for name, prec in (("fp64", snow_b200.SNOW_FP64), ("mixed", snow_b200.SNOW_MIXED)):
+        b = snow_b200.Batch(prec)
+        i = b.add(sc, stream=sp)
+        b.setup(i, sc.dx, stream=sp)
+        b.step(settle, stream=sp)
+        if name == "fp64":
+            settled = b.download(i)
+        ms = timed_steps(b, steps, sp, torch)
+        fb = []
+        for _ in range(5):
+            b.step(1, stream=sp)
+            fb.append(b.fp64_projections)
+        res[name] = {"value": sc.n * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                     "plastic_fraction_after": plastic_fraction(b.download(i))}
+        if name == "mixed":
+            res[name]["fp64_fallback_per_step"] = float(np.mean(fb)) / sc.n
+        b.close()
+    a, b = snow_b200.Batch(snow_b200.SNOW_FP64), snow_b200.Batch(snow_b200.SNOW_MIXED)
+    ia = a.add_scene(settled, sc.params(), sc.planes)
+    ib = b.add_scene(settled, sc.params(), sc.planes)
+    fb = 0
+    for _ in range(10):
+        a.step(1)
+        b.step(1)
+        fb += b.fp64_projections
+    err = errors(b.download(ib), a.download(ia))
+    a.close()
+    b.close()
+    out["tori"] = {"workload": sc.name, "settle_steps": settle, "timed_steps": steps, "fp64": res["fp64"],
+                   "mixed": res["mixed"], "mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
+                   "plastic_fraction_at_start": plastic_fraction(settled),
+                   "mixed_error_vs_fp64_10_steps_from_settled": err,
+                   "mixed_fp64_fallbacks_in_those_10_steps": fb}
+    # -- batched scenes on the ground
+    bscenes = scenes.batch_scenes(count=256, grounded=True)
+    nb = sum(x.n for x in bscenes)
+    brates = {}
+    bsteps = max(20, steps // 4)
+    for name, prec in (("fp64", snow_b200.SNOW_FP64), ("mixed", snow_b200.SNOW_MIXED)):
+        b = snow_b200.Batch(prec)
+        ids = [b.add(x, stream=sp) for x in bscenes]
+        for i, x in zip(ids, bscenes):
+            b.setup(i, x.dx, stream=sp)
+        b.step(settle, stream=sp)
+        chunk, _ = b.autotune(trial_steps=5, stream=sp)
+        b.step(3, stream=sp)
+        ms_b = timed_steps(b, bsteps, sp, torch)
+        pf = float(np.mean([plastic_fraction(b.download(i)) for i in ids]))
+        brates[name] = {"value": nb * bsteps / (ms_b * 1e-3), "ms_per_step": ms_b / bsteps, "work_item": chunk,
+                        "mean_plastic_fraction_after": pf}
+        b.close()
+    plain_b = plain_fp64_rate(snow_b200, torch, sp, [(x, bsteps, bsteps) for x in bscenes], settle=settle)
+    out["batched"] = {"scenes": len(bscenes), "particles": nb, "settle_steps": settle, "fp64": brates["fp64"],
+                      "mixed": brates["mixed"], "plain_fp64_one_scene_at_a_time": plain_b,
+                      "mixed_vs_plain_fp64_same_scenes": brates["mixed"]["value"] / plain_b,
+                      "fp64_batched_vs_plain_fp64_same_scenes": brates["fp64"]["value"] / plain_b}
+    # -- served stream on the ground
+    reqs = scenes.served_requests(count=48, rate=200.0, grounded=True)
+    runs = []
+    for _ in range(3):
+        srv = snow_b200.Server(snow_b200.SNOW_MIXED, budget_bytes=150 * 10**9, max_steps_per_tick=16)
+        for x, n, t in reqs:
+            srv.submit(x, n, t)
+        srv.run(stream=sp)
+        runs.append(srv.stats())
+        srv.close()
+    runs.sort(key=lambda r: r["particle_steps_per_s"])
+    plain_s = plain_fp64_rate(snow_b200, torch, sp, [(x, n, min(n, 40)) for x, n, _ in reqs])
+    out["served"] = {"requests": len(reqs), "precision": "mixed",
+                     "runs_particle_steps_per_s": [r["particle_steps_per_s"] for r in runs],
+                     "plain_fp64_one_request_at_a_time": plain_s,
+                     "served_vs_plain_fp64_same_requests_min_run": runs[0]["particle_steps_per_s"] / plain_s,
+                     "served_vs_plain_fp64_same_requests_median_run": runs[1]["particle_steps_per_s"] / plain_s,
+                     "p50_latency_s": runs[1]["p50_s"], "p99_latency_s": runs[1]["p99_s"]}
+    return out
+
+
 def measured_peak() -> tuple[float, str]:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -415,6 +528,68 @@ def profile_traffic(workload: str, precision: str, kernel: str):
         return None
 
 
+def profile_flops(workload: str, precision: str, kernel: str):
+    """Executed floating-point operations per particle of `kernel` ({"fp64": F, "fp32": F})
+    from the committed ncu instruction counts (profiles/flops.json): 2 per FMA, 1 per add
+    or multiply, twice that for the packed two-wide float forms."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "flops.json")) as f:
+            t = json.load(f)
+        return t.get(f"{workload}/{precision}/{kernel}")
+    except (OSError, ValueError):
+        return None
+
+
+def measure_peaks(snow_b200) -> dict:
+    """FMA throughput of this GPU measured now (TFLOP/s; snow_gpu_measure_fma_peak)."""
+    return {name: snow_b200.measure_fma_peak(kind) / 1e12
+            for name, kind in (("fp64_tflops", snow_b200.SNOW_PEAK_FP64),
+                               ("fp32_tflops", snow_b200.SNOW_PEAK_FP32),
+                               ("fp32x2_tflops", snow_b200.SNOW_PEAK_FP32X2))}
+
+
+def kernel_roofline(kernel: str, ms: float, alg_bytes: float, n_particles: int, workload: str,
+                    precision: str, peaks: dict) -> dict:
+    """One kernel against its roofs: HBM (algorithmic bytes / launch time against the
+    measured copy bandwidth) and the FMA pipes (executed FLOPs / launch time against the
+    measured FMA peaks).  `bound` is the roof with the largest fraction."""
+    hbm_peak, hbm_src = measured_peak()
+    gbs = alg_bytes / (ms * 1e-3) / 1e9
+    roofs = {"hbm": {"achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                     "peak_source": hbm_src}}
+    fl = profile_flops(workload, precision, kernel) or {}
+    for pipe, peak in (("fp64", peaks.get("fp64_tflops")),
+                       ("fp32", max(peaks.get("fp32_tflops") or 0, peaks.get("fp32x2_tflops") or 0))):
+        per = fl.get(pipe)
+        if per and peak:
+            tf = per * n_particles / (ms * 1e-3) / 1e12
+            roofs[pipe] = {"achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+                           "peak_source": "measured (snow_gpu_measure_fma_peak)",
+                           "flops_per_launch": per * n_particles}
+    bound = max(roofs, key=lambda k: roofs[k]["frac"])
+    return {"kernel": kernel, "launch_ms": ms, "alg_bytes_per_launch": alg_bytes, "bound": bound,
+            "frac": roofs[bound]["frac"], "roofs": roofs,
+            "traffic": profile_traffic(workload, precision, kernel)}
+
+
+def roofline_line(per: dict, ab: dict, n_particles: int, workload: str, precision: str, peaks: dict) -> dict:
+    """The bench line's roofline object: the dominant (longest) particle kernel's
+    binding roof, with both particle kernels' roofs beside it."""
+    ks = {"p2g": kernel_roofline("p2g", per["p2g"], ab["p2g"], n_particles, workload, precision, peaks),
+          "g2p": kernel_roofline("g2p", per["stress_update"], ab["g2p"], n_particles, workload, precision,
+                                 peaks)}
+    dom = max(ks, key=lambda k: ks[k]["launch_ms"])
+    d = ks[dom]
+    r = d["roofs"][d["bound"]]
+    return {"bound": d["bound"], "kernel": dom, "achieved": r["achieved"], "peak": r["peak"], "unit": r["unit"],
+            "frac": r["frac"], "peak_source": r["peak_source"], "traffic": d["traffic"],
+            "alg_bytes_per_launch": d["alg_bytes_per_launch"], "launch_ms": d["launch_ms"],
+            "hbm_frac": d["roofs"]["hbm"]["frac"],
+            "fp64_pipe_frac": d["roofs"].get("fp64", {}).get("frac"),
+            "fp32_pipe_frac": d["roofs"].get("fp32", {}).get("frac"),
+            "kernels": ks, "peaks": peaks}
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -431,7 +606,7 @@ def run_ours(args, ws, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     prec = snow_b200.SNOW_FP64 if args.precision == "fp64" else snow_b200.SNOW_MIXED
-    sc = workload(args.workload)
+    sc = workload(args.workload, args.particles)
     stream = torch.cuda.Stream()  # our kernels and the timing events share this stream
     torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
@@ -470,11 +645,8 @@ def run_ours(args, ws, rank, local):
     per = {k: v / args.steps for k, v in kt.items() if v > 0}
     real = 8 if args.precision == "fp64" else 4
     ab = alg_bytes(sc.n, blocks * 64, real)
-    dom = "g2p" if per.get("stress_update", 0) >= per.get("p2g", 0) else "p2g"
-    dom_ms = per["stress_update"] if dom == "g2p" else per["p2g"]
-    peak, peak_src = measured_peak()
-    achieved = ab[dom] / (dom_ms * 1e-3) / 1e9
-    traffic = profile_traffic(args.workload, args.precision, dom)
+    peaks = measure_peaks(snow_b200)
+    roof = roofline_line(per, ab, sc.n, args.workload, args.precision, peaks)
 
     # end to end through the drop-in entry point on pinned host records
     e2e = None
@@ -519,10 +691,7 @@ def run_ours(args, ws, rank, local):
                        l2="particle state > 126 MB L2 (no flush needed)" if sc.n * 416 > 126e6
                        else "state fits L2; steps read the previous step's output",
                        graph="CUDA graph per step"),
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_src,
-                     "alg_bytes_per_launch": ab[dom], "launch_ms": dom_ms,
-                     "traffic": traffic},
+        "roofline": roof,
         "stages_ms_per_step": per,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -602,11 +771,9 @@ def run_batch(args, ws, rank, local):
     kt = batch.step(args.steps, timings=True, stream=sp)
     per = {k: v / args.steps for k, v in kt.items() if v > 0}
     real = 8 if args.precision == "fp64" else 4
-    ab = alg_bytes(sum(s.n for s in mine), blocks * 64, real)
-    dom = "g2p" if per.get("stress_update", 0) >= per.get("p2g", 0) else "p2g"
-    dom_ms = per["stress_update"] if dom == "g2p" else per["p2g"]
-    peak, peak_src = measured_peak()
-    achieved = ab[dom] / (dom_ms * 1e-3) / 1e9
+    nmine = sum(s.n for s in mine)
+    ab = alg_bytes(nmine, blocks * 64, real)
+    roof = roofline_line(per, ab, nmine, "batch", args.precision, measure_peaks(snow_b200))
 
     e2e = None
     if not args.no_e2e:
@@ -646,9 +813,7 @@ def run_batch(args, ws, rank, local):
                    "precision": args.precision, "parallelism": f"scene shards x{ws}" if ws > 1 else "single GPU",
                    "rank0_scenes": len(mine), "work_item": chunk, "sort": batch.sort_mode(),
                    "l2": "particle state > 126 MB L2 (no flush needed)", "graph": "CUDA graph per step"},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_src, "alg_bytes_per_launch": ab[dom],
-                     "launch_ms": dom_ms, "traffic": None},
+        "roofline": roof,
         "stages_ms_per_step": per, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk, "grid_blocks": {"used": blocks, "capacity": cap}, "status": status,
     }

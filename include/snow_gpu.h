@@ -248,10 +248,13 @@ int snow_gpu_step(double* records, int64_t n, const snow_step_params* params,
  * device scratch lives in one fixed file-scope device array (about 26 MB,
  * held on every GPU that loads the library until exit), which limits a call
  * to 16,384 particles, 2,048 grid blocks and 16 colliders; larger inputs
- * return SNOW_E_ARG, a scene that outgrows the blocks SNOW_E_CAPACITY.  The
- * first call on a device looks up the array's address (make it before any
- * stream capture).  Calls share the array: calls that overlap on the GPU race
- * and must be serialised by the caller.  Returns after the steps complete. */
+ * return SNOW_E_ARG, a scene that outgrows the blocks SNOW_E_CAPACITY; on any
+ * error the records are left unchanged.  The first call on a device looks up
+ * the array's address, which (with lazy module loading) is when the driver
+ * reserves it; a call with n = 0 does only that set-up.  The call synchronises
+ * its stream, so it must not be made while that stream is being captured.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Returns after the steps complete. */
 int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step_params* params,
                           const snow_collider* colliders, int n_colliders, int n_steps,
                           void* stream);
@@ -299,6 +302,17 @@ int snow_gpu_stage_g2p(const int32_t* ijk, const double* fields, int64_t n_nodes
 int snow_gpu_stage_particle_collisions(double* records, int64_t n,
                                        const snow_collider* colliders, int n_colliders);
 int snow_gpu_stage_position_update(double* records, int64_t n, double time_step);
+
+/* ---- measured arithmetic peaks (roofline denominators) ------------------
+ * No counterpart in the reference.  Runs a fused multiply-add loop on every SM
+ * of the current device for at least 20 ms at the clocks the GPU runs (no clock
+ * or power setting is changed) and returns the sustained rate in FLOP/s (two
+ * per FMA): kind SNOW_PEAK_FP64 (double FMA), SNOW_PEAK_FP32 (float FMA) or
+ * SNOW_PEAK_FP32X2 (packed two-wide float FMA).  *ms (optional) receives the
+ * timed run's duration.  The roofline of the particle kernels, which do 3x3
+ * algebra and stencil sums, is the larger of their HBM and FMA-pipe fractions. */
+enum { SNOW_PEAK_FP64 = 0, SNOW_PEAK_FP32 = 1, SNOW_PEAK_FP32X2 = 2 };
+int snow_gpu_measure_fma_peak(int kind, double* flops_per_s, double* ms, void* stream);
 
 #ifdef __cplusplus
 }

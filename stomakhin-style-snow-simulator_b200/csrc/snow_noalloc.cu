@@ -17,13 +17,21 @@
 // SNOW_E_CAPACITY.  The array (about 26 MB) is held on every GPU that loads
 // the library until the process exits.
 //
-// The array's address is looked up with cudaGetSymbolAddress the first time
-// the entry point runs on a device (with that device current) and cached per
-// device; make that first call before any stream capture.  All calls share
-// the one array: calls that overlap on the GPU (different streams or host
-// threads) race and must be serialised by the caller.  Each call re-zeroes
-// the grid accumulators and counters it relies on, so the previous call's
-// leftovers never leak into its result.
+// Set-up: the first call on a device (with that device current) looks the
+// array's address up with cudaGetSymbolAddress and caches it per device.  With
+// lazy module loading (the CUDA default) that first lookup is also when the
+// driver loads this module on the device and reserves the array, which can
+// synchronise the device or fail if the application has used up its memory.
+// A call with n = 0 does only this set-up, so a caller can pay that cost up
+// front, e.g. at start-up.  Every call waits for its own copies (it
+// synchronises the stream it is given), so it must not be called while that
+// stream is being captured into a CUDA graph.
+//
+// All calls share the one array: calls that overlap on the GPU (different
+// streams or host threads) race and must be serialised by the caller.  Each
+// call re-zeroes the grid accumulators and counters it relies on, so the
+// previous call's leftovers never leak into its result.  On any error the
+// caller's records are left as they were.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -160,9 +168,9 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
       if ((colliders[c].kind != SNOW_COLLIDER_PLANE && colliders[c].kind != SNOW_COLLIDER_SPHERE) ||
           (colliders[c].kind == SNOW_COLLIDER_SPHERE && !(colliders[c].param[0] > 0.0)))
         throw Error(SNOW_E_ARG, "unsupported collider");
+    unsigned char* A = arena_for_current_device();  // per-device set-up (see the header comment)
     if (n == 0 || n_steps == 0) return SNOW_OK;
 
-    unsigned char* A = arena_for_current_device();
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const Layout& L = kLayout;
     const int64_t st = kMaxParticles;
@@ -250,11 +258,10 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
       StepLaunch<double>::g2p(b, G2P_FULL, s);
       StepLaunch<double>::finish(b, s);
     }
-    const int cur = n_steps & 1;
+    const int cur = n_steps & 1;  // k_finish swaps the buffers once per step
     k_noalloc_records_out<<<g, 256, 0, s>>>(staging, n, r[cur], fp[cur], id[cur], st);
     check_cuda(cudaGetLastError(), "noalloc step launch");
-    check_cuda(cudaMemcpyAsync(records, staging, (size_t)n * 26 * sizeof(double), cudaMemcpyDeviceToHost, s),
-               "download records");
+    // The status first: the caller's records are only overwritten by a valid result.
     Counters h{};
     check_cuda(cudaMemcpyAsync(&h, ctr, sizeof h, cudaMemcpyDeviceToHost, s), "status");
     check_cuda(cudaStreamSynchronize(s), "noalloc step");
@@ -264,6 +271,9 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
     if (h.status & ST_NONFINITE) throw Error(SNOW_E_NONFINITE, "a particle position became NaN or infinite");
     if (h.status & ST_KEY_OVERFLOW) throw Error(SNOW_E_KEYRANGE, "scene extent exceeds the block key range");
     if (h.status) throw Error(SNOW_E_STATE, "internal grid inconsistency (status " + std::to_string(h.status) + ")");
+    check_cuda(cudaMemcpyAsync(records, staging, (size_t)n * 26 * sizeof(double), cudaMemcpyDeviceToHost, s),
+               "download records");
+    check_cuda(cudaStreamSynchronize(s), "noalloc download");
     return SNOW_OK;
   } catch (const Error& e) {
     return set_error(e.code, e.what());

@@ -21,6 +21,7 @@ LIB_PATH = os.environ.get("SNOW_B200_LIB") or os.path.join(PKG_DIR, "libsnow_b20
 
 SNOW_FP64, SNOW_MIXED = 0, 1
 SNOW_COLLIDER_PLANE, SNOW_COLLIDER_SPHERE = 0, 1
+SNOW_PEAK_FP64, SNOW_PEAK_FP32, SNOW_PEAK_FP32X2 = 0, 1, 2
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "grid capacity exceeded",
           -4: "non-finite particle state", -5: "key range exceeded", -6: "invalid state"}
 
@@ -138,6 +139,7 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_batch_chunk": (ctypes.c_int, [vp]),
         "snow_gpu_batch_graph_kernels": (ctypes.c_int, [vp]),
         "snow_gpu_batch_sort_mode": (ctypes.c_int, [vp]),
+        "snow_gpu_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, _dp, _dp, vp]),
         "snow_gpu_batch_snapshot": (ctypes.c_int, [vp, ctypes.c_int32, vp]),
         "snow_gpu_batch_restore": (ctypes.c_int, [vp, ctypes.c_int32, vp]),
         "snow_gpu_setup": (ctypes.c_int, [_dp, i64, d]),
@@ -363,6 +365,13 @@ class Batch:
     @property
     def device_bytes(self) -> int:
         return int(lib().snow_gpu_batch_device_bytes(self._h))
+
+
+def measure_fma_peak(kind: int, stream: int | None = None) -> float:
+    """Measured FMA throughput of the current device in FLOP/s (SNOW_PEAK_*)."""
+    f, ms = ctypes.c_double(), ctypes.c_double()
+    _check(lib().snow_gpu_measure_fma_peak(int(kind), ctypes.byref(f), ctypes.byref(ms), ctypes.c_void_p(stream)))
+    return f.value
 
 
 def setup(records: np.ndarray, dx: float) -> np.ndarray:

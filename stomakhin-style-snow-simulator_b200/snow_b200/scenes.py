@@ -135,20 +135,30 @@ def torus(center, R: float, r: float, n_target: int, rng, axis: int = 0, exact: 
     return x, h
 
 
-def tori_scene(n_per_torus: int = 325_000, steps: int = 500, seed: int = 1) -> Scene:
+def tori_scene(n_per_torus: int = 325_000, steps: int = 500, seed: int = 1, gap: float | None = None) -> Scene:
     """Two colliding tori, R = 0.15, r = 0.06, +-8 m/s along x.
 
     The symmetry axis is x (the direction of motion), so the tori do not
     overlap at t = 0; spacing h = (2 pi^2 R r^2 / n)^(1/3) gives n per torus.
+    By default the centres are (0.3, 0.5, 0.5) and (0.7, 0.5, 0.5), 0.286 m
+    apart along x, which the tori do not close within 500 steps.  With `gap`
+    the centres are placed symmetrically about x = 0.5 with `gap` metres
+    between the tori (0: touching), so the snow deforms from the first steps:
+    the same particles, moved rigidly along x.
     """
     rng = np.random.default_rng(seed)
     xa, h = torus((0.3, 0.5, 0.5), 0.15, 0.06, n_per_torus, rng, exact=True)
     xb, _ = torus((0.7, 0.5, 0.5), 0.15, 0.06, n_per_torus, rng, exact=True)
+    if gap is not None:
+        shift = 0.2 - 0.06 - 0.5 * gap  # centre at 0.5 -+ (r + gap / 2)
+        xa[:, 0] += shift
+        xb[:, 0] -= shift
     m = 400.0 * h ** 3
     ra = records(xa, np.broadcast_to((8.0, 0.0, 0.0), xa.shape), m)
     rb = records(xb, np.broadcast_to((-8.0, 0.0, 0.0), xb.shape), m)
+    name = f"two-tori-{ra.shape[0] + rb.shape[0]}" + ("" if gap is None else f"-gap{gap:g}")
     return Scene(np.concatenate([ra, rb]), dx=0.01, dt=2e-5, steps=steps, material=Material(),
-                 planes=[GROUND], name=f"two-tori-{ra.shape[0] + rb.shape[0]}")
+                 planes=[GROUND], name=name)
 
 
 def sphere(center, radius: float, n_target: int, rng, jitter_frac: float = 0.1):
@@ -170,10 +180,24 @@ def snowball_scene(n: int = 4_000_000, steps: int = 200, seed: int = 2) -> Scene
                  name=f"snowball-{x.shape[0]}")
 
 
+def _ground(x: np.ndarray, vel: np.ndarray, h: float):
+    """Rests a particle set on the ground plane (lowest particle half a lattice
+    spacing above y = 0.05) and turns its velocity downward, so it strikes the
+    ground in its first steps."""
+    x = x.copy()
+    x[:, 1] += 0.05 + 0.5 * h - x[:, 1].min()
+    v = np.array(vel, dtype=np.float64)
+    v[1] = -abs(v[1]) - 1.0
+    return x, v
+
+
 def batch_scenes(count: int = 256, lo: int = 1000, hi: int = 64000, seed: int = 3,
-                 dt: float = 5e-5, steps: int = 200) -> list[Scene]:
+                 dt: float = 5e-5, steps: int = 200, grounded: bool = False) -> list[Scene]:
     """Independent scenes with log-uniform particle counts, box or sphere, random
-    velocity in [-5,5]^3 and material drawn per scene; dx = 0.02, spacing 0.01."""
+    velocity in [-5,5]^3 and material drawn per scene; dx = 0.02, spacing 0.01.
+    By default every scene starts 0.25 m or more above the ground plane (free
+    flight for 200 steps); `grounded` sets each scene on the ground moving
+    down (vy = -|vy| - 1 m/s), so it deforms plastically from its first steps."""
     rng = np.random.default_rng(seed)
     out = []
     for s in range(count):
@@ -193,19 +217,22 @@ def batch_scenes(count: int = 256, lo: int = 1000, hi: int = 64000, seed: int = 
         else:
             rad = (3 * n / (4 * math.pi)) ** (1 / 3) * h
             x, _ = sphere((0.5, 0.3 + rad, 0.5), rad, n, rng)
+        if grounded:
+            x, vel = _ground(x, vel, h)
         out.append(Scene(records(x, np.broadcast_to(vel, x.shape), 400.0 * h ** 3), dx=0.02,
                          dt=dt, steps=steps, material=mat, planes=[GROUND], name=f"batch{s}"))
     return out
 
 
 def served_requests(count: int = 64, rate: float = 200.0, lo: int = 2000, hi: int = 500_000,
-                    steps_lo: int = 100, steps_hi: int = 2000, seed: int = 4, dt: float = 5e-5):
+                    steps_lo: int = 100, steps_hi: int = 2000, seed: int = 4, dt: float = 5e-5,
+                    grounded: bool = False):
     """A Poisson stream of scene requests: (scene, steps, arrival seconds).
 
     Particle counts are log-uniform in [lo, hi], shapes box / sphere / torus at
     lattice spacing 0.01 (so the count sets the size), velocity in [-5, 5]^3,
     material drawn as for the batch scenes, steps uniform in [steps_lo,
-    steps_hi], grid dx = 0.02, ground plane."""
+    steps_hi], grid dx = 0.02, ground plane.  `grounded` as for batch_scenes."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -228,6 +255,8 @@ def served_requests(count: int = 64, rate: float = 200.0, lo: int = 2000, hi: in
         else:
             r_minor = (n * h ** 3 / (2 * math.pi ** 2 * 2.5)) ** (1 / 3)  # R = 2.5 r
             x, _ = torus((0.5, 0.3 + r_minor, 0.5), 2.5 * r_minor, r_minor, n, rng, axis=1)
+        if grounded:
+            x, vel = _ground(x, vel, h)
         steps = int(rng.integers(steps_lo, steps_hi + 1))
         sc = Scene(records(x, np.broadcast_to(vel, x.shape), 400.0 * h ** 3), dx=0.02, dt=dt, steps=steps,
                    material=mat, planes=[GROUND], name=f"request{r}")

@@ -74,7 +74,7 @@ def test_gpu_bodies_match_reference(snow, oracle, prec):
     if prec == 0:
         assert max(e.values()) < 1e-10, e
     else:
-        assert e["x"] < 1e-4 and e["v"] < 5e-3 and e["F_E"] < 1e-4, e
+        assert e["x"] < 1e-4 and e["v"] < 5e-3 and e["F_E"] < 1e-4 and e["F_P"] < 1e-4, e
 
 
 @pytest.mark.gpu

@@ -40,7 +40,13 @@ def test_mixed_cube_against_fp64_oracle(snow, oracle, steps):
     e = errors(got, want)
     for k, tol in MIXED_TOL.items():
         assert e[k] < tol, (k, e)
-    assert b.fp64_projections >= 0
+    # The cube is in free fall, far from the ground and from the clamp bounds:
+    # no projection is clamped or near-critical, so F_P stays I and nothing
+    # goes to the double-precision fallback.  (The touching-tori test in
+    # test_parity_full.py covers the regime where both happen.)
+    assert b.fp64_projections == 0
+    assert np.array_equal(got[:, 8:17], want[:, 8:17])
+    assert np.array_equal(want[:, 8:17], np.tile(np.eye(3).reshape(-1), (want.shape[0], 1)))
 
 
 def test_mixed_tori_in_contact(snow, oracle):

@@ -10,6 +10,7 @@ import multiprocessing as mp
 import os
 import socket
 
+import numpy as np
 import pytest
 
 
@@ -36,6 +37,40 @@ def _split_worker(rank, world, port, work, q):
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, lists, local, float(t.item())))
+
+
+def _requests():
+    """Small independent scenes with their own step counts (requests of a stream)."""
+    from snow_b200 import scenes
+
+    scs = scenes.batch_scenes(count=6, lo=300, hi=2500, seed=21, grounded=True)
+    return [(sc, 2 + (3 * i) % 5) for i, sc in enumerate(scs)]
+
+
+def _shard_step_worker(rank, world, port, q):
+    """One rank: steps its shard of the requests with the oracle (the CPU
+    stand-in for a rank-local batch) and gathers (index, records) on rank 0."""
+    import torch.distributed as dist
+
+    from oracle_lib import Oracle
+    from snow_b200 import shard
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    reqs = _requests()
+    mine = shard.shard([sc.n * n for sc, n in reqs], world, rank)
+    o = Oracle()
+    done = []
+    for i in mine:
+        sc, n = reqs[i]
+        rec = o.setup(sc.particles, sc.dx)
+        out, _ = o.step(rec, sc.params(), sc.plane_array(), n)
+        done.append((i, out))
+    gathered = [None] * world if rank == 0 else None
+    dist.gather_object(done, gathered, dst=0)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, gathered if rank == 0 else len(done)))
 
 
 def _lonely_worker(rank, world, port, q):
@@ -100,3 +135,19 @@ def test_missing_rank_fails_fast():
     # world size 2, only rank 0 starts
     out = _run(_lonely_worker, (2, _free_port()), 1)
     assert out[0][0] != "joined"
+
+
+def test_sharded_requests_equal_single_rank(oracle):
+    """Each of two ranks steps its share of a request stream (work = particles x
+    steps); the union gathered on rank 0 is the single-rank result, record for
+    record (no data crosses ranks, so nothing may change)."""
+    reqs = _requests()
+    out = _run(_shard_step_worker, (2, _free_port()), 2, limit_s=120)
+    gathered = out[0][0]
+    got = dict(item for part in gathered for item in part)
+    assert sorted(got) == list(range(len(reqs)))
+    assert out[1][0] > 0, "both ranks hold work"
+    for i, (sc, n) in enumerate(reqs):
+        rec = oracle.setup(sc.particles, sc.dx)
+        want, _ = oracle.step(rec, sc.params(), sc.plane_array(), n)
+        assert np.array_equal(got[i], want), i

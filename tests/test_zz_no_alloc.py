@@ -34,7 +34,10 @@ def _noalloc(snow, rec, params, planes, steps):
     return rc, out
 
 
-def test_noalloc_matches_step_on_two_calls(snow):
+@pytest.mark.parametrize("steps", [6, 5])
+def test_noalloc_matches_step_on_two_calls(snow, steps):
+    """Even and odd step counts per call (the result lies in the buffer the
+    last step wrote, which alternates)."""
     from snow_b200 import scenes
 
     sc = scenes.cube_scene(16)  # 4,096 particles falling onto the ground plane
@@ -43,11 +46,38 @@ def test_noalloc_matches_step_on_two_calls(snow):
     ref = start.copy()
     cur = start.copy()
     for call in range(2):
-        snow.step(ref, sc.params(), sc.planes, 6)
-        rc, cur = _noalloc(snow, cur, sc.params(), sc.planes, 6)
+        snow.step(ref, sc.params(), sc.planes, steps)
+        rc, cur = _noalloc(snow, cur, sc.params(), sc.planes, steps)
         assert rc == 0, snow.lib().snow_gpu_last_error().decode()
         e = errors(cur, ref)
         assert max(e.values()) < TOL, (call, e)
+
+
+def test_noalloc_setup_call_with_no_particles(snow):
+    """n = 0 only does the per-device set-up and succeeds."""
+    from snow_b200 import scenes
+
+    sc = scenes.cube_scene(4)
+    rc, _ = _noalloc(snow, np.zeros((0, 26)), sc.params(), sc.planes, 1)
+    assert rc == 0, snow.lib().snow_gpu_last_error().decode()
+
+
+def test_noalloc_capacity_error_leaves_records_unchanged(snow):
+    """A sparse scene whose particles each need their own grid blocks: 1,000
+    particles 0.1 m apart need far more than the 2,048 blocks the fixed array
+    holds.  The call reports SNOW_E_CAPACITY and leaves the records alone."""
+    from snow_b200 import scenes
+
+    g = (np.arange(10) + 0.5) * 0.1
+    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    rec = scenes.records(x, np.zeros_like(x), 0.001)
+    rec[:, 7] = 1e-6
+    sc = scenes.cube_scene(4)
+    before = rec.copy()
+    rc, out = _noalloc(snow, rec, sc.params(), [], 1)
+    assert rc == -3, (rc, snow.lib().snow_gpu_last_error().decode())
+    assert "2048" in snow.lib().snow_gpu_last_error().decode()
+    assert np.array_equal(out, before)
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit(snow):
