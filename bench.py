@@ -308,6 +308,8 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
                       "error_vs_fp64": errs}
     # -- colliding: the same measurements where the snow deforms
     forms["colliding"] = measure_colliding(snow_b200, torch, sp, steps)
+    # -- input / output and the frame loop
+    forms["io"] = measure_io(tori)
     # -- batched: 256 scenes, FP64 and mixed
     bscenes = scenes.batch_scenes(count=256)
     nb = sum(s.n for s in bscenes)
@@ -507,6 +509,98 @@ def measure_colliding(snow_b200, torch, sp, steps, settle=40) -> dict:
                      "served_vs_plain_fp64_same_requests_min_run": runs[0]["particle_steps_per_s"] / plain_s,
                      "served_vs_plain_fp64_same_requests_median_run": runs[1]["particle_steps_per_s"] / plain_s,
                      "p50_latency_s": runs[1]["p50_s"], "p99_latency_s": runs[1]["p99_s"]}
+    return out
+
+
+def write_scene_csv(sc, d: str) -> tuple[str, str]:
+    """The scene as the reference's input files (one group per distinct
+    velocity and mass)."""
+    rec = sc.particles
+    keys, inv = np.unique(np.concatenate([rec[:, 3:7]], axis=1), axis=0, return_inverse=True)
+    g, p = os.path.join(d, "groups.csv"), os.path.join(d, "particles.csv")
+    with open(g, "w") as f:
+        f.write("group_id,vx,vy,vz,mass\n")
+        for i, k in enumerate(keys):
+            f.write(f"{i},{float(k[0])!r},{float(k[1])!r},{float(k[2])!r},{float(k[3])!r}\n")
+    np.savetxt(p, np.column_stack([inv.reshape(-1), rec[:, 0:3]]), fmt=["%d", "%.17g", "%.17g", "%.17g"],
+               delimiter=",", header="group_id,x,y,z", comments="")
+    return g, p
+
+
+def measure_io(sc) -> dict:
+    """The drop-in's input and output against the reference's on the headline
+    scene: import of its groups.csv/particles.csv, export of one frame, and the
+    reference's frame loop (import, setup, frames of steps, a frame written
+    after each) run by the snow_frames app with the state resident on the GPU,
+    without export, with the reference's synchronous export and with the
+    background export that overlaps the next frame's steps."""
+    import ctypes
+    import tempfile
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import REF_SO
+
+    dp = ctypes.POINTER(ctypes.c_double)
+    L = ctypes.CDLL(os.path.join(PKG, "libsnow.so"))
+    L.snow_io_import.argtypes = [ctypes.c_char_p, ctypes.c_char_p, dp, ctypes.c_int64]
+    L.snow_io_import.restype = ctypes.c_int64
+    L.snow_io_export.argtypes = [dp, ctypes.c_int64, ctypes.c_int]
+    R = ctypes.CDLL(REF_SO) if os.path.exists(REF_SO) else None
+    if R is not None:
+        R.ref_import.argtypes = [ctypes.c_char_p, ctypes.c_char_p, dp, ctypes.c_int64]
+        R.ref_import.restype = ctypes.c_int64
+        R.ref_export.argtypes = [dp, ctypes.c_int64, ctypes.c_int]
+    out = {"workload": sc.name, "particles": sc.n}
+    rec = np.ascontiguousarray(sc.particles)
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as d:
+        g, p = write_scene_csv(sc, d)
+        out["particles_csv_bytes"] = os.path.getsize(p)
+
+        def best(fn, reps=2):
+            t = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                fn()
+                t.append(time.perf_counter() - t0)
+            return 1e3 * min(t)
+
+        n_ours = L.snow_io_import(g.encode(), p.encode(), None, 0)
+        if n_ours != sc.n:
+            raise RuntimeError(f"snow_io_import read {n_ours} particles, expected {sc.n}")
+        out["import_ms"] = {"ours": best(lambda: L.snow_io_import(g.encode(), p.encode(), None, 0))}
+        os.makedirs(os.path.join(d, "output"), exist_ok=True)
+        os.chdir(d)
+        try:
+            out["export_ms"] = {"ours": best(lambda: L.snow_io_export(rec.ctypes.data_as(dp), sc.n, 1))}
+            if R is not None:
+                out["import_ms"]["reference"] = best(lambda: R.ref_import(g.encode(), p.encode(), None, 0))
+                out["export_ms"]["reference"] = best(lambda: R.ref_export(rec.ctypes.data_as(dp), sc.n, 2))
+        finally:
+            os.chdir(cwd)
+        for k in ("import_ms", "export_ms"):
+            if "reference" in out[k]:
+                out[k]["reference_over_ours"] = out[k]["reference"] / out[k]["ours"]
+        m = sc.material
+        args = [os.path.join(PKG, "snow_frames"), g, p, "--frames", "6", "--substeps", "25", "--dx", str(sc.dx),
+                "--dt", str(sc.dt), "--E", str(m.E), "--nu", str(m.nu), "--xi", str(m.xi),
+                "--theta-c", str(m.theta_c), "--theta-s", str(m.theta_s), "--alpha", str(m.alpha),
+                "--gravity", str(m.gravity[1]), "--plane-y", "0.05", "--friction", "0.2"]
+        loops = {}
+        for mode in ("none", "async", "sync"):
+            r = subprocess.run(args + ["--export", mode], cwd=d, capture_output=True, text=True, timeout=600)
+            if r.returncode != 0:
+                loops[mode] = {"error": (r.stderr or r.stdout)[-300:]}
+                continue
+            j = json.loads(r.stdout.strip().splitlines()[-1])
+            loops[mode] = {k: j[k] for k in ("loop_ms", "steps_done_ms", "export_wait_ms", "particle_steps_per_s",
+                                             "import_ms", "setup_ms")}
+        out["frame_loop"] = {"frames": 6, "substeps": 25, "resident": True, "modes": loops}
+        try:
+            base, a, s = (loops[k]["loop_ms"] for k in ("none", "async", "sync"))
+            out["frame_loop"]["export_cost_ms_per_frame"] = {"sync": (s - base) / 6, "async": (a - base) / 6}
+        except (KeyError, TypeError):
+            pass
     return out
 
 

@@ -50,13 +50,35 @@ struct SphereNormal
     Eigen::Vector3d operator()(const Eigen::Vector3d& x) const { return (x - center).normalized(); }
 };
 
+// Solid oriented box centred at `center` with orthonormal axes u, w, u x w and
+// half extents h along them.  phi is the exact signed distance
+// |max(q, 0)| + min(max_k q_k, 0) with q_k = |l_k| - h_k, l the point in the
+// box's axes.  The normal inside the box (where collisions act) is the outward
+// normal of the face with the largest q_k (the first on a tie, +1 side at
+// l_k = 0); outside it is the gradient of phi.
+struct BoxDistance
+{
+    Eigen::Vector3d center, u, w, half;
+    double operator()(const Eigen::Vector3d& x) const;
+};
+struct BoxNormal
+{
+    Eigen::Vector3d center, u, w, half;
+    Eigen::Vector3d operator()(const Eigen::Vector3d& x) const;
+};
+
 // Not in the reference (which takes any CollisionBody): bodies the GPU step
-// can run besides make_plane -- a plane moving with a constant velocity and a
-// solid sphere, resting or moving.
+// can run besides make_plane -- a plane moving with a constant velocity, a
+// solid sphere and a solid oriented box, resting or moving.
 CollisionBody make_moving_plane(const Eigen::Vector3d& point, const Eigen::Vector3d& normal,
                                 const Eigen::Vector3d& velocity, double friction);
 CollisionBody make_sphere(const Eigen::Vector3d& center, double radius, double friction,
                           const Eigen::Vector3d& velocity = Eigen::Vector3d::Zero());
+// `axis_u` and `axis_w` are normalised and w is made orthogonal to u
+// (Gram-Schmidt); they must not be parallel.
+CollisionBody make_box(const Eigen::Vector3d& center, const Eigen::Vector3d& half_extents,
+                       const Eigen::Vector3d& axis_u, const Eigen::Vector3d& axis_w, double friction,
+                       const Eigen::Vector3d& velocity = Eigen::Vector3d::Zero());
 }  // namespace snow
 
 CollisionBody make_plane(const Eigen::Vector3d& point, const Eigen::Vector3d& normal, double friction);

@@ -125,4 +125,10 @@ void set_resident(bool on);
 bool resident();
 void sync_to_host(std::vector<Particle>& snow);
 void invalidate();
+// Resident steps fill StepTimings per stage by default, which times each
+// stage between events and waits for the step.  With stage timings off a
+// resident step() launches the captured step graph and returns at once,
+// leaving StepTimings untouched; the GPU runs ahead of the host until the next
+// read-back (sync_to_host, export_particles, a non-resident call).
+void set_stage_timings(bool on);
 }  // namespace snow::gpu

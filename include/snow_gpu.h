@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SNOW_GPU_ABI_VERSION 1
+#define SNOW_GPU_ABI_VERSION 2
 #define SNOW_RECORD_DOUBLES 26
 
 enum {
@@ -58,14 +58,21 @@ enum {
 };
 
 /* Collider kinds. */
-enum { SNOW_COLLIDER_PLANE = 0, SNOW_COLLIDER_SPHERE = 1 };
+enum { SNOW_COLLIDER_PLANE = 0, SNOW_COLLIDER_SPHERE = 1, SNOW_COLLIDER_BOX = 2 };
 
 /* A collider (CollisionBody, include/snow/collision.hpp:6-12; the reference
  * takes any phi / normal / velocity functions and defines make_plane,
  * src/collision.cpp:5-27).  A plane is the half-space
  * phi(x) = normal . (x - point) <= 0 with unit `normal`; a sphere (kind 1) is
  * the solid ball |x - point| <= param[0] with normal (x - point)/|x - point|.
- * Either moves with constant `velocity` (zero for make_plane). */
+ * A box (kind 2) is the solid oriented box centred at `point` with orthonormal
+ * axes u = `normal`, w = `axis` and u x w, and half extents `extent` along
+ * them: with l = (u.d, w.d, (u x w).d) for d = x - point and q_k = |l_k| -
+ * extent[k], phi = |max(q, 0)| + min(max_k q_k, 0) (the exact signed
+ * distance), and inside the box (phi <= 0, where collisions act) the normal is
+ * the outward normal sign(l_k) e_k of the face k with the largest q_k (the
+ * first such k on a tie, sign +1 at l_k = 0), in world axes.  Every kind moves
+ * with constant `velocity` (zero for make_plane). */
 typedef struct snow_collider {
   int32_t kind;
   int32_t reserved;
@@ -74,6 +81,8 @@ typedef struct snow_collider {
   double velocity[3];
   double friction;
   double param[2];
+  double axis[3];    /* box: second axis (unit, orthogonal to normal) */
+  double extent[3];  /* box: half extents along normal, axis, normal x axis */
 } snow_collider;
 
 /* Arguments 4-12 of step() (src/grid.cpp:359). */

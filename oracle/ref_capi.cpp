@@ -7,7 +7,9 @@
 // Particles travel as 26-double records in the reference's struct Particle order.
 // Step calls report the ten StepTimings stages and, in slot 10, the wall time
 // of the step loop (milliseconds).
+#include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -43,16 +45,62 @@ std::vector<CollisionBody> planes(const double* q, int n) {
     b.push_back(make_plane({q[0], q[1], q[2]}, {q[3], q[4], q[5]}, q[6]));
   return b;
 }
-// Bodies as n x 12 rows: kind, point[3], normal[3], velocity[3], friction,
-// radius.  A resting plane is the reference's own make_plane; a moving plane
-// and a solid sphere are CollisionBody values with their phi / normal /
-// velocity functions written out, as a user of the reference would.
+// Solid oriented box (centre p, axes u, w, u x w, half extents h) as a user of
+// the reference would write it: the point in the box's axes l, q_k = |l_k| -
+// h_k; phi = |max(q, 0)| + min(max q, 0); normal inside = outward normal of
+// the face with the largest q_k (first on a tie, + side at l_k = 0), outside =
+// the normalised gradient of phi.
+struct BoxFrame {
+  Eigen::Vector3d p, ax[3], h;
+  void local(const Eigen::Vector3d& x, double l[3], double q[3]) const {
+    for (int k = 0; k < 3; ++k) {
+      l[k] = ax[k].dot(x - p);
+      q[k] = std::abs(l[k]) - h[k];
+    }
+  }
+};
+CollisionBody box_body(const BoxFrame& f, const Eigen::Vector3d& v, double mu) {
+  return CollisionBody{[f](const Eigen::Vector3d& x) {
+                         double l[3], q[3], out2 = 0.0;
+                         f.local(x, l, q);
+                         for (double e : q) out2 += e > 0.0 ? e * e : 0.0;
+                         return std::sqrt(out2) + std::min(std::max(q[0], std::max(q[1], q[2])), 0.0);
+                       },
+                       [f](const Eigen::Vector3d& x) {
+                         double l[3], q[3];
+                         f.local(x, l, q);
+                         int k = 0;
+                         for (int a = 1; a < 3; ++a)
+                           if (q[a] > q[k]) k = a;
+                         if (q[k] <= 0.0) return Eigen::Vector3d((l[k] < 0.0 ? -1.0 : 1.0) * f.ax[k]);
+                         Eigen::Vector3d g = Eigen::Vector3d::Zero();
+                         for (int a = 0; a < 3; ++a)
+                           if (q[a] > 0.0) g = g + (l[a] < 0.0 ? -q[a] : q[a]) * f.ax[a];
+                         return Eigen::Vector3d(g.normalized());
+                       },
+                       [v](const Eigen::Vector3d&) { return v; }, mu};
+}
+
+// Bodies as n x 18 rows: kind, point[3], normal[3], velocity[3], friction,
+// radius, axis[3], half extents[3].  A resting plane is the reference's own
+// make_plane; a moving plane, a solid sphere and an oriented box are
+// CollisionBody values with their phi / normal / velocity functions written
+// out, as a user of the reference would.
 std::vector<CollisionBody> bodies(const double* q, int n) {
   std::vector<CollisionBody> b;
-  for (int i = 0; i < n; ++i, q += 12) {
+  for (int i = 0; i < n; ++i, q += 18) {
     const Eigen::Vector3d p{q[1], q[2], q[3]}, nrm{q[4], q[5], q[6]}, v{q[7], q[8], q[9]};
     const double mu = q[10], r = q[11];
-    if (q[0] == 1.0) {
+    if (q[0] == 2.0) {
+      BoxFrame f;
+      f.p = p;
+      f.ax[0] = nrm;
+      f.ax[1] = Eigen::Vector3d{q[12], q[13], q[14]};
+      f.ax[2] = Eigen::Vector3d{nrm[1] * q[14] - nrm[2] * q[13], nrm[2] * q[12] - nrm[0] * q[14],
+                                nrm[0] * q[13] - nrm[1] * q[12]};
+      f.h = Eigen::Vector3d{q[15], q[16], q[17]};
+      b.push_back(box_body(f, v, mu));
+    } else if (q[0] == 1.0) {
       b.push_back(CollisionBody{[p, r](const Eigen::Vector3d& x) { return (x - p).norm() - r; },
                                 [p](const Eigen::Vector3d& x) { return Eigen::Vector3d((x - p).normalized()); },
                                 [v](const Eigen::Vector3d&) { return v; }, mu});

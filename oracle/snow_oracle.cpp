@@ -279,11 +279,12 @@ using Stencil = std::array<StencilEntry, 64>;
 // and zero velocity; the same plane may move with a constant velocity; a solid
 // sphere has phi(x) = |x - c| - r and normal (x - c)/|x - c|.
 struct Plane {
-  int kind = 0;        // 0 plane, 1 sphere
-  Vec3 point, normal;  // plane: point, unit normal; sphere: centre in `point`
+  int kind = 0;        // 0 plane, 1 sphere, 2 oriented box
+  Vec3 point, normal;  // plane: point, unit normal; sphere and box: centre in `point`
   double friction = 0.0;
   Vec3 velocity{0.0, 0.0, 0.0};
   double radius = 0.0;
+  Vec3 axis{0.0, 0.0, 0.0}, half{0.0, 0.0, 0.0};  // box: axes normal, axis, normal x axis; half extents
 };
 inline Vec3 unit(const Vec3& n) {
   const double len = norm(n);
@@ -296,10 +297,53 @@ inline Plane make_plane(const Vec3& p, const Vec3& n, double mu) {
   b.friction = mu;
   return b;
 }
+// A solid oriented box as a user of the reference would write its CollisionBody:
+// l = the point in the box's axes (u, w, u x w), q_k = |l_k| - h_k; phi is the
+// signed distance |max(q, 0)| + min(max q, 0); the normal is, inside, the
+// outward normal of the face with the largest q_k (first on a tie, + side at
+// l_k = 0) and, outside, the normalised gradient of phi.
+inline Vec3 cross(const Vec3& a, const Vec3& b) {
+  return Vec3{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+inline void box_frame(const Plane& b, const Vec3& x, Vec3 ax[3], double l[3], double q[3]) {
+  ax[0] = b.normal;
+  ax[1] = b.axis;
+  ax[2] = cross(b.normal, b.axis);
+  const Vec3 d = x - b.point;
+  for (int k = 0; k < 3; ++k) {
+    l[k] = dot(ax[k], d);
+    q[k] = std::abs(l[k]) - b.half[k];
+  }
+}
+inline double box_phi(const Plane& b, const Vec3& x) {
+  Vec3 ax[3];
+  double l[3], q[3];
+  box_frame(b, x, ax, l, q);
+  double out2 = 0.0;
+  for (double v : q) out2 += v > 0.0 ? v * v : 0.0;
+  return std::sqrt(out2) + std::min(std::max(q[0], std::max(q[1], q[2])), 0.0);
+}
+inline Vec3 box_normal(const Plane& b, const Vec3& x) {
+  Vec3 ax[3];
+  double l[3], q[3];
+  box_frame(b, x, ax, l, q);
+  int k = 0;
+  for (int a = 1; a < 3; ++a)
+    if (q[a] > q[k]) k = a;
+  if (q[k] <= 0.0) return (l[k] < 0.0 ? -1.0 : 1.0) * ax[k];
+  Vec3 g{0.0, 0.0, 0.0};
+  for (int a = 0; a < 3; ++a)
+    if (q[a] > 0.0) g = g + (l[a] < 0.0 ? -q[a] : q[a]) * ax[a];
+  return unit(g);
+}
 inline double body_phi(const Plane& b, const Vec3& x) {
+  if (b.kind == 2) return box_phi(b, x);
   return b.kind == 1 ? norm(x - b.point) - b.radius : dot(b.normal, x - b.point);
 }
-inline Vec3 body_normal(const Plane& b, const Vec3& x) { return b.kind == 1 ? unit(x - b.point) : b.normal; }
+inline Vec3 body_normal(const Plane& b, const Vec3& x) {
+  if (b.kind == 2) return box_normal(b, x);
+  return b.kind == 1 ? unit(x - b.point) : b.normal;
+}
 
 // ------------------------------------------------------------------ kernels
 // N(a, b): cubic B-spline of |a - b| (grid.cpp:24-40).
@@ -586,15 +630,18 @@ std::vector<Plane> to_planes(const double* planes, int n) {
   }
   return b;
 }
-// bodies: n x 12 doubles = kind, point[3], normal[3], velocity[3], friction, radius
+// bodies: n x 18 doubles = kind, point[3], normal[3], velocity[3], friction,
+// radius, axis[3], half extents[3]
 std::vector<Plane> to_bodies(const double* rows, int n) {
   std::vector<Plane> b;
   for (int i = 0; i < n; ++i) {
-    const double* q = rows + 12 * i;
+    const double* q = rows + 18 * i;
     Plane c = make_plane(Vec3{q[1], q[2], q[3]}, Vec3{q[4], q[5], q[6]}, q[10]);
     c.kind = (int)q[0];
     c.velocity = Vec3{q[7], q[8], q[9]};
     c.radius = q[11];
+    c.axis = Vec3{q[12], q[13], q[14]};
+    c.half = Vec3{q[15], q[16], q[17]};
     b.push_back(c);
   }
   return b;

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -29,6 +30,37 @@ int set_error(int code, const std::string& msg) {
 
 void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw Error(SNOW_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static_assert(sizeof(snow_collider) == sizeof(Collider), "collider layouts must agree");
+
+std::vector<Collider> device_colliders(const snow_collider* c, int n) {
+  if (n < 0 || (n > 0 && !c)) throw Error(SNOW_E_ARG, "bad collider array");
+  std::vector<Collider> out;
+  for (int i = 0; i < n; ++i) {
+    const snow_collider& x = c[i];
+    if (x.kind != SNOW_COLLIDER_PLANE && x.kind != SNOW_COLLIDER_SPHERE && x.kind != SNOW_COLLIDER_BOX)
+      throw Error(SNOW_E_ARG, "unsupported collider kind " + std::to_string(x.kind));
+    if (x.kind == SNOW_COLLIDER_SPHERE && !(x.param[0] > 0.0 && std::isfinite(x.param[0])))
+      throw Error(SNOW_E_ARG, "sphere collider needs a positive finite radius in param[0]");
+    if (x.kind == SNOW_COLLIDER_BOX) {
+      double uu = 0, ww = 0, uw = 0;
+      for (int a = 0; a < 3; ++a) {
+        uu += x.normal[a] * x.normal[a];
+        ww += x.axis[a] * x.axis[a];
+        uw += x.normal[a] * x.axis[a];
+        if (!(x.extent[a] > 0.0 && std::isfinite(x.extent[a])))
+          throw Error(SNOW_E_ARG, "box collider needs positive finite half extents");
+      }
+      if (!(std::fabs(uu - 1.0) < 1e-9 && std::fabs(ww - 1.0) < 1e-9 && std::fabs(uw) < 1e-9))
+        throw Error(SNOW_E_ARG, "box collider axes (normal, axis) must be unit and orthogonal");
+    }
+    Collider d{};
+    std::memcpy(&d, &x, sizeof d);
+    d.pad = 0;
+    out.push_back(d);
+  }
+  return out;
 }
 
 namespace {
@@ -351,25 +383,7 @@ int32_t Batch::add_scene(const double* records, int64_t n, const snow_step_param
 }
 
 void Batch::set_colliders(Scene& sc, const snow_collider* c, int n) {
-  if (n < 0 || (n > 0 && !c)) throw Error(SNOW_E_ARG, "bad collider array");
-  sc.colliders.clear();
-  for (int i = 0; i < n; ++i) {
-    if (c[i].kind != SNOW_COLLIDER_PLANE && c[i].kind != SNOW_COLLIDER_SPHERE)
-      throw Error(SNOW_E_ARG, "unsupported collider kind " + std::to_string(c[i].kind));
-    if (c[i].kind == SNOW_COLLIDER_SPHERE && !(c[i].param[0] > 0.0 && std::isfinite(c[i].param[0])))
-      throw Error(SNOW_E_ARG, "sphere collider needs a positive finite radius in param[0]");
-    Collider d{};
-    d.kind = c[i].kind;
-    for (int a = 0; a < 3; ++a) {
-      d.point[a] = c[i].point[a];
-      d.normal[a] = c[i].normal[a];
-      d.velocity[a] = c[i].velocity[a];
-    }
-    d.friction = c[i].friction;
-    d.param[0] = c[i].param[0];
-    d.param[1] = c[i].param[1];
-    sc.colliders.push_back(d);
-  }
+  sc.colliders = device_colliders(c, n);
 }
 
 void Batch::remove_scene(int32_t id) {

@@ -33,6 +33,11 @@ int set_error(int code, const std::string& msg);
 int auto_chunk(int64_t particles, int precision);
 void check_cuda(cudaError_t e, const char* what);
 
+// Checks a caller's collider array (kinds, finite positive sphere radius, box
+// axes unit and orthogonal, box half extents finite and positive) and returns
+// it as device records; throws Error(SNOW_E_ARG) on the first bad entry.
+std::vector<Collider> device_colliders(const snow_collider* c, int n);
+
 // One scene: its particle planes (two buffers), parameters and colliders.
 struct Scene {
   int32_t sid = 0;  // handle returned to the caller

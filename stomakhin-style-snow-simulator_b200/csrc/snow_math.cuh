@@ -391,20 +391,53 @@ struct Collider {
   double normal[3];
   double velocity[3];
   double friction;
-  double param[2];  // sphere: param[0] = radius
+  double param[2];   // sphere: param[0] = radius
+  double axis[3];    // box: second axis w (unit, orthogonal to `normal`)
+  double extent[3];  // box: half extents along u = normal, w, u x w
 };
-enum : int32_t { COLLIDER_PLANE = 0, COLLIDER_SPHERE = 1 };
+enum : int32_t { COLLIDER_PLANE = 0, COLLIDER_SPHERE = 1, COLLIDER_BOX = 2 };
+
+// Solid oriented box: inside test and outward face normal.  l = the point in
+// the box's axes (u, w, u x w), q_k = |l_k| - h_k; inside (phi = max_k q_k <= 0)
+// the normal is sign(l_k) times the axis of the largest q_k (first k on a tie,
+// sign +1 at l_k = 0).  Returns false outside, where phi > 0.
+template <typename T>
+SNOW_HD bool box_contact(const Collider& b, T x, T y, T z, T& nx, T& ny, T& nz) {
+  const T dx = x - T(b.point[0]), dy = y - T(b.point[1]), dz = z - T(b.point[2]);
+  const T u[3] = {T(b.normal[0]), T(b.normal[1]), T(b.normal[2])};
+  const T w[3] = {T(b.axis[0]), T(b.axis[1]), T(b.axis[2])};
+  const T t[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+  const T l[3] = {u[0] * dx + u[1] * dy + u[2] * dz, w[0] * dx + w[1] * dy + w[2] * dz,
+                  t[0] * dx + t[1] * dy + t[2] * dz};
+  int k = 0;
+  T qmax = fabs(l[0]) - T(b.extent[0]);
+#pragma unroll
+  for (int a = 1; a < 3; ++a) {
+    const T q = fabs(l[a]) - T(b.extent[a]);
+    if (q > qmax) {
+      qmax = q;
+      k = a;
+    }
+  }
+  if (!(qmax <= T(0))) return false;
+  const T s = l[k] < T(0) ? T(-1) : T(1);
+  const T* e = k == 0 ? u : (k == 1 ? w : t);
+  nx = s * e[0], ny = s * e[1], nz = s * e[2];
+  return true;
+}
 
 // collision_helper (grid.cpp:206-231): Coulomb friction, stick when
 // |v_t| <= -mu v_n, else slide.
 // Bodies: a plane phi(x) = n . (x - p) with unit normal n (make_plane,
-// src/collision.cpp:5-27), or a solid sphere phi(x) = |x - c| - r with normal
-// (x - c) / |x - c| (zero at the centre, as Eigen's normalized() leaves it);
-// either moves with the constant velocity v_c.
+// src/collision.cpp:5-27), a solid sphere phi(x) = |x - c| - r with normal
+// (x - c) / |x - c| (zero at the centre, as Eigen's normalized() leaves it), or
+// a solid oriented box (box_contact); each moves with the constant velocity v_c.
 template <typename T>
 SNOW_HD void collide(const Collider& b, T x, T y, T z, T& vx, T& vy, T& vz) {
   T nx, ny, nz;
-  if (b.kind == COLLIDER_SPHERE) {
+  if (b.kind == COLLIDER_BOX) {
+    if (!box_contact(b, x, y, z, nx, ny, nz)) return;
+  } else if (b.kind == COLLIDER_SPHERE) {
     const T ex = x - T(b.point[0]), ey = y - T(b.point[1]), ez = z - T(b.point[2]);
     const T len = sqrt(ex * ex + ey * ey + ez * ez);
     if (!(len - T(b.param[0]) <= T(0))) return;

@@ -164,10 +164,7 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
                                   " colliders");
     if (!params || !(params->grid_spacing > 0.0)) throw Error(SNOW_E_ARG, "bad step parameters");
     if (n_steps < 0) throw Error(SNOW_E_ARG, "negative step count");
-    for (int c = 0; c < n_colliders; ++c)
-      if ((colliders[c].kind != SNOW_COLLIDER_PLANE && colliders[c].kind != SNOW_COLLIDER_SPHERE) ||
-          (colliders[c].kind == SNOW_COLLIDER_SPHERE && !(colliders[c].param[0] > 0.0)))
-        throw Error(SNOW_E_ARG, "unsupported collider");
+    const std::vector<Collider> cols = device_colliders(colliders, n_colliders);
     unsigned char* A = arena_for_current_device();  // per-device set-up (see the header comment)
     if (n == 0 || n_steps == 0) return SNOW_OK;
 
@@ -218,11 +215,9 @@ extern "C" int snow_gpu_step_noalloc(double* records, int64_t n, const snow_step
       sd.nb_hi[a] = INT_MIN;
     }
     check_cuda(cudaMemcpyAsync(scene, &sd, sizeof sd, cudaMemcpyHostToDevice, s), "scene");
-    if (n_colliders > 0) {
-      static_assert(sizeof(snow_collider) == sizeof(Collider), "collider layouts must agree");
-      check_cuda(cudaMemcpyAsync(coll, colliders, sizeof(Collider) * n_colliders, cudaMemcpyHostToDevice, s),
+    if (n_colliders > 0)
+      check_cuda(cudaMemcpyAsync(coll, cols.data(), sizeof(Collider) * n_colliders, cudaMemcpyHostToDevice, s),
                  "colliders");
-    }
 
     BatchDev b{};
     b.scenes = scene;

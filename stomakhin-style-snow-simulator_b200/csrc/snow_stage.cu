@@ -285,18 +285,7 @@ void gather_stage(const int32_t* ijk, const double* fields, int64_t n_nodes, dou
   sg.batch.download(sg.id, rec, n, nullptr);
 }
 
-std::vector<Collider> to_colliders(const snow_collider* c, int nc) {
-  if (nc < 0 || (nc > 0 && !c)) throw Error(SNOW_E_ARG, "bad collider array");
-  std::vector<Collider> out((size_t)nc);
-  if (nc) std::memcpy(out.data(), c, sizeof(Collider) * nc);
-  for (auto& x : out) {
-    if (x.kind != SNOW_COLLIDER_PLANE && x.kind != SNOW_COLLIDER_SPHERE)
-      throw Error(SNOW_E_ARG, "unsupported collider kind");
-    if (x.kind == SNOW_COLLIDER_SPHERE && !(x.param[0] > 0.0))
-      throw Error(SNOW_E_ARG, "sphere collider needs a positive radius in param[0]");
-  }
-  return out;
-}
+std::vector<Collider> to_colliders(const snow_collider* c, int nc) { return device_colliders(c, nc); }
 
 }  // namespace
 }  // namespace snow

@@ -325,6 +325,8 @@ std::vector<snow_collider> to_colliders(const std::vector<CollisionBody>& bodies
         const auto* nrm = b.normal.target<snow::PlaneNormal>();
         const auto* sd = b.phi.target<snow::SphereDistance>();
         const auto* sn = b.normal.target<snow::SphereNormal>();
+        const auto* bd = b.phi.target<snow::BoxDistance>();
+        const auto* bn = b.normal.target<snow::BoxNormal>();
         snow_collider c{};
         if (vel && d && nrm && d->unit_normal == nrm->unit_normal)
         {
@@ -341,11 +343,23 @@ std::vector<snow_collider> to_colliders(const std::vector<CollisionBody>& bodies
             for (int a = 0; a < 3; ++a) c.point[a] = sd->center[a];
             c.param[0] = sd->radius;
         }
+        else if (vel && bd && bn && bd->center == bn->center && bd->u == bn->u && bd->w == bn->w &&
+                 bd->half == bn->half)
+        {
+            c.kind = SNOW_COLLIDER_BOX;
+            for (int a = 0; a < 3; ++a)
+            {
+                c.point[a] = bd->center[a];
+                c.normal[a] = bd->u[a];
+                c.axis[a] = bd->w[a];
+                c.extent[a] = bd->half[a];
+            }
+        }
         else
         {
             throw std::invalid_argument(
-                "collider is not a make_plane, snow::make_moving_plane or snow::make_sphere body "
-                "(a std::function cannot execute on the device)");
+                "collider is not a make_plane, snow::make_moving_plane, snow::make_sphere or snow::make_box "
+                "body (a std::function cannot execute on the device)");
         }
         for (int a = 0; a < 3; ++a) c.velocity[a] = vel->value[a];
         c.friction = b.friction;

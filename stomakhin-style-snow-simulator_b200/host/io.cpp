@@ -21,6 +21,7 @@
 #include "snow/export.hpp"
 #include "snow/import.hpp"
 #include "snow_host_detail.hpp"
+#include "snow_io.h"
 
 namespace
 {
@@ -168,21 +169,37 @@ std::vector<Particle> import_particles(const std::string& filename_group, const 
 
 namespace
 {
+// One number as the default stream formatting writes it (export.cpp:13-19:
+// operator<< on a double, precision 6, %g style), via std::to_chars in its
+// general format with the same precision.
+char* put_number(char* at, double v)
+{
+    return std::to_chars(at, at + 32, v, std::chars_format::general, 6).ptr;
+}
+
 // output/frame_<frame>.csv with header "x,y,z" and rows (x, -z, y), default
-// stream formatting (export.cpp:10-22).
+// stream formatting (export.cpp:10-22), formatted into one buffer and written
+// in one piece.
 void write_frame(const double* rec, std::size_t n, int frame_no)
 {
     std::ostringstream name;
     name << "output/frame_" << std::setw(6) << std::setfill('0') << frame_no << ".csv";
-    std::ofstream file{name.str()};
-    std::ostringstream out;
-    out << "x,y,z\n";
+    std::ofstream file{name.str(), std::ios::binary};
+    std::string out(6 + n * 3 * 32, '\0');
+    char* at = out.data();
+    std::memcpy(at, "x,y,z\n", 6);
+    at += 6;
     for (std::size_t i = 0; i < n; ++i)
     {
         const double* p = rec + SNOW_RECORD_DOUBLES * i;
-        out << p[0] << "," << p[2] * -1 << "," << p[1] << "\n";
+        at = put_number(at, p[0]);
+        *at++ = ',';
+        at = put_number(at, p[2] * -1);
+        *at++ = ',';
+        at = put_number(at, p[1]);
+        *at++ = '\n';
     }
-    file << out.str();
+    file.write(out.data(), at - out.data());
 }
 
 std::mutex g_export_mu;
@@ -224,3 +241,51 @@ void wait_exports()
     for (auto& t : jobs) t.join();
 }
 }  // namespace snow::gpu
+
+// ---------------------------------------------------------------- C ABI
+// include/snow_io.h: the importer and the frame writer above for callers
+// that bind C (ctypes, cgo, JNI).
+
+namespace
+{
+thread_local std::string g_io_error;
+}
+
+extern "C" int64_t snow_io_import(const char* groups_csv, const char* particles_csv, double* records,
+                                  int64_t capacity)
+{
+    try
+    {
+        if (!groups_csv || !particles_csv) throw std::runtime_error("snow_io_import: NULL file name");
+        const std::vector<Particle> v = import_particles(groups_csv, particles_csv);
+        const auto n = static_cast<int64_t>(v.size());
+        if (records)
+        {
+            if (n > capacity) return -2;
+            if (n) std::memcpy(records, v.data(), v.size() * sizeof(Particle));
+        }
+        return n;
+    }
+    catch (const std::exception& e)
+    {
+        g_io_error = e.what();
+        return -1;
+    }
+}
+
+extern "C" int snow_io_export(const double* records, int64_t n, int frame_no)
+{
+    try
+    {
+        if (n < 0 || (n > 0 && !records)) throw std::runtime_error("snow_io_export: bad record array");
+        write_frame(records, static_cast<std::size_t>(n), frame_no);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_io_error = e.what();
+        return -1;
+    }
+}
+
+extern "C" const char* snow_io_last_error(void) { return g_io_error.c_str(); }

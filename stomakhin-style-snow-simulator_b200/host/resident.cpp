@@ -1,5 +1,6 @@
 // GPU residency for the drop-in step(): one batch holding the particle vector
 // last stepped, keyed by its data pointer and size.
+#include <cstring>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -24,6 +25,11 @@ struct Resident
     const Particle* data = nullptr;
     std::size_t size = 0;
     bool host_stale = false;  // the vector lags the GPU copy
+    bool stage_timings = true;
+    // the parameters and colliders the batch holds (set_params only when they
+    // change: it makes the next step recompute every particle's force matrix)
+    snow_step_params params{};
+    std::vector<snow_collider> colliders;
 
     void drop()
     {
@@ -56,6 +62,12 @@ void set_resident(bool on)
     r.on = on;
     if (!on) r.drop();
 }
+void set_stage_timings(bool on)
+{
+    auto& r = state();
+    std::lock_guard<std::mutex> lk(r.mu);
+    r.stage_timings = on;
+}
 bool resident()
 {
     auto& r = state();
@@ -87,6 +99,10 @@ void snow_host_resident_step(std::vector<Particle>& snow, const snow_step_params
     auto& r = state();
     std::lock_guard<std::mutex> lk(r.mu);
     const int64_t n = static_cast<int64_t>(snow.size());
+    const bool same_params =
+        std::memcmp(&r.params, &p, sizeof p) == 0 && r.colliders.size() == colliders.size() &&
+        (colliders.empty() ||
+         std::memcmp(r.colliders.data(), colliders.data(), colliders.size() * sizeof(snow_collider)) == 0);
     if (!r.batch || r.data != snow.data() || r.size != snow.size())
     {
         r.drop();
@@ -96,12 +112,17 @@ void snow_host_resident_step(std::vector<Particle>& snow, const snow_step_params
         r.data = snow.data();
         r.size = snow.size();
     }
-    else
+    else if (!same_params)
     {
         check(snow_gpu_batch_set_params(r.batch, r.scene, &p, colliders.data(),
                                         static_cast<int>(colliders.size())));
     }
-    check(snow_gpu_batch_step(r.batch, 1, &t, nullptr));
+    r.params = p;
+    r.colliders = colliders;
+    // With stage timings the step is launched kernel by kernel between events
+    // and waited for; without, it is the batch's captured step graph, left
+    // running on the GPU (the next read-back waits for it).
+    check(snow_gpu_batch_step(r.batch, 1, r.stage_timings ? &t : nullptr, nullptr));
     r.host_stale = true;
 }
 

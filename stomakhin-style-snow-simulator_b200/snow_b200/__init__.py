@@ -20,7 +20,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.environ.get("SNOW_B200_LIB") or os.path.join(PKG_DIR, "libsnow_b200.so")
 
 SNOW_FP64, SNOW_MIXED = 0, 1
-SNOW_COLLIDER_PLANE, SNOW_COLLIDER_SPHERE = 0, 1
+SNOW_COLLIDER_PLANE, SNOW_COLLIDER_SPHERE, SNOW_COLLIDER_BOX = 0, 1, 2
 SNOW_PEAK_FP64, SNOW_PEAK_FP32, SNOW_PEAK_FP32X2 = 0, 1, 2
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "grid capacity exceeded",
           -4: "non-finite particle state", -5: "key range exceeded", -6: "invalid state"}
@@ -34,7 +34,7 @@ class Collider(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("point", ctypes.c_double * 3), ("normal", ctypes.c_double * 3),
                 ("velocity", ctypes.c_double * 3), ("friction", ctypes.c_double),
-                ("param", ctypes.c_double * 2)]
+                ("param", ctypes.c_double * 2), ("axis", ctypes.c_double * 3), ("extent", ctypes.c_double * 3)]
 
 
 class StepParams(ctypes.Structure):
@@ -223,12 +223,35 @@ def moving_plane(point, normal, friction: float, velocity) -> "Collider":
     return c
 
 
+def box(center, half_extents, axis_u, axis_w, friction: float, velocity=(0.0, 0.0, 0.0)) -> "Collider":
+    """A solid oriented box collider: centre, half extents along the axes u, w and
+    u x w (u and w are normalised and w made orthogonal to u), moving with `velocity`."""
+    u = np.asarray(axis_u, dtype=np.float64)
+    u = u / np.linalg.norm(u)
+    w = np.asarray(axis_w, dtype=np.float64)
+    w = w - u.dot(w) * u
+    w = w / np.linalg.norm(w)
+    c = Collider()
+    c.kind = SNOW_COLLIDER_BOX
+    for a in range(3):
+        c.point[a] = float(center[a])
+        c.normal[a] = float(u[a])
+        c.axis[a] = float(w[a])
+        c.extent[a] = float(half_extents[a])
+        c.velocity[a] = float(velocity[a])
+    c.friction = float(friction)
+    return c
+
+
+BODY_COLUMNS = 18
+
+
 def body_rows(cols) -> np.ndarray:
-    """(k, 12) rows (kind, point, normal, velocity, friction, radius) of Collider values,
-    the form the oracle and the reference build take."""
-    out = np.zeros((len(cols), 12))
+    """(k, 18) rows (kind, point[3], normal[3], velocity[3], friction, radius, axis[3],
+    extent[3]) of Collider values, the form the oracle and the reference build take."""
+    out = np.zeros((len(cols), BODY_COLUMNS))
     for i, c in enumerate(cols):
-        out[i] = [c.kind, *c.point, *c.normal, *c.velocity, c.friction, c.param[0]]
+        out[i] = [c.kind, *c.point, *c.normal, *c.velocity, c.friction, c.param[0], *c.axis, *c.extent]
     return out
 
 

@@ -284,6 +284,33 @@ int main()
              expect(a[0].v_p[1] > -1.0 + 1e-6, "sphere pushes back the falling particle");
              expect(a[1].v_p[1] > 0.0, "the rising plane lifts the particle");
          }},
+        {"oriented box bodies run on the device and match their phi", [] {
+             // a particle falling onto the tilted top face of a resting box is turned
+             // back along the face normal; make_box's phi is the exact signed
+             // distance (negative inside, the face distance at the centre)
+             const Eigen::Vector3d u{1, 0.2, 0}, w{-0.2, 1, 0};
+             CollisionBody box = snow::make_box({0.5, 0.4, 0.5}, {0.1, 0.05, 0.1}, u, w, 0.0);
+             expect(std::abs(box.phi({0.5, 0.4, 0.5}) + 0.05) < 1e-12, "phi at the centre is -h_min");
+             expect(std::abs(box.phi({0.5, 0.4, 0.8}) - 0.2) < 1e-12, "phi beyond a face");
+             const Eigen::Vector3d top = box.normal({0.5, 0.44, 0.5});
+             expect(std::abs(top.dot(w.normalized()) - 1.0) < 1e-12, "inside normal of the nearest face");
+             std::vector<Particle> a{Particle({0.5, 0.449, 0.5}, {0, -1, 0}, 1, 1e-6)};
+             std::vector<ParticleStencil> st(1);
+             StepTimings t;
+             std::vector<CollisionBody> bodies{box};
+             step(a, bodies, st, {0, 0, 0}, 1e-4, 0.02, 1, 1, 1, 0.02, 0.01, 0.95, t);
+             expect(a[0].v_p.dot(w.normalized()) > -1e-9, "the box stops motion into its face");
+             bool threw = false;
+             try
+             {
+                 snow::make_box({0, 0, 0}, {1, 1, 1}, {1, 0, 0}, {2, 0, 0}, 0.1);
+             }
+             catch (const std::invalid_argument&)
+             {
+                 threw = true;
+             }
+             expect(threw, "parallel box axes are rejected");
+         }},
         {"CSV import, its errors, and frame export", [] {
              namespace fs = std::filesystem;
              const fs::path dir = fs::temp_directory_path() / "snow_gpu_io_test";

@@ -5,14 +5,17 @@ src/collision.cpp compiled unmodified against the project's Eigen-subset shim
 into oracle/_ref/libsnow_ref.so by oracle/Makefile -- and stores its outputs:
 
   sample_scene.npz   the reference's sample input (input/groups.csv +
-                     input/particles.csv, 957 particles) imported by the
-                     reference's import_particles, setup() at dx = 0.05, then
-                     1 and 10 step() calls with the parameters of src/main.cpp
+                     input/particles.csv, 957 particles; the two files' bytes
+                     are kept as groups_csv / particles_csv so the importer
+                     can be tested on them) imported by the reference's
+                     import_particles, setup() at dx = 0.05, then 1 and 10
+                     step() calls with the parameters of src/main.cpp
   cube_scene.npz     an 8^3 jittered lattice cube (seed 0) with the small-case
                      material, setup() at dx = 0.02, then 1 and 10 steps with a
                      ground plane the lower particles already touch
 
-Run from the repository root, where the reference tree exists:
+Run from the repository root, with the reference tree's location given as
+the argument or in the environment variable SNOW_REFERENCE_DIR:
     python tests/golden/make_golden.py [/path/to/reference]
 """
 from __future__ import annotations
@@ -53,7 +56,15 @@ def import_sample(ref_root: str) -> np.ndarray:
     return out
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def file_bytes(path: str) -> np.ndarray:
+    with open(path, "rb") as f:
+        return np.frombuffer(f.read(), dtype=np.uint8)
+
+
+def main(ref_root: str | None = None) -> None:
+    ref_root = ref_root or os.environ.get("SNOW_REFERENCE_DIR")
+    if not ref_root:
+        sys.exit("give the reference tree as the argument or in SNOW_REFERENCE_DIR")
     ref = Reference()
     # sample scene, exactly as src/main.cpp drives it
     rec = import_sample(ref_root)
@@ -63,7 +74,9 @@ def main(ref_root: str = "/root/reference") -> None:
     s1, _ = ref.step(s0, prm, planes, 1)
     s10, _ = ref.step(s0, prm, planes, 10)
     np.savez_compressed(os.path.join(HERE, "sample_scene.npz"), imported=rec, setup=s0, step1=s1,
-                        step10=s10, params=prm, planes=planes, dx=0.05)
+                        step10=s10, params=prm, planes=planes, dx=0.05,
+                        groups_csv=file_bytes(os.path.join(ref_root, "input", "groups.csv")),
+                        particles_csv=file_bytes(os.path.join(ref_root, "input", "particles.csv")))
     # small cube resting on the ground plane (contact from the first step)
     cube = scenes.cube(8, lo=(0.46, 0.045, 0.46), velocity=(0.5, -1.5, 0.25), seed=0)
     sc = scenes.Scene(cube, dx=0.02, dt=1e-4, steps=10, material=scenes.Material(),

@@ -44,11 +44,16 @@ class _StepLib:
         return out
 
     def step_bodies(self, rec: np.ndarray, params, bodies, steps: int = 1):
-        """Like step() with general colliders: (k, 12) rows of kind (0 plane, 1 sphere),
-        point[3], normal[3], velocity[3], friction, radius."""
+        """Like step() with general colliders: (k, 18) rows of kind (0 plane, 1 sphere,
+        2 oriented box), point[3], normal[3], velocity[3], friction, radius, axis[3],
+        extent[3] (the box's centre, first axis, second axis and half extents)."""
         out = np.ascontiguousarray(rec, dtype=np.float64).copy()
         prm = np.ascontiguousarray(params, dtype=np.float64)
-        b = np.ascontiguousarray(np.asarray(bodies, dtype=np.float64).reshape(-1, 12))
+        b = np.asarray(bodies, dtype=np.float64)
+        b = b.reshape(-1, b.shape[-1]) if b.size else np.zeros((0, 18))
+        if b.shape[1] < 18:
+            b = np.concatenate([b, np.zeros((b.shape[0], 18 - b.shape[1]))], axis=1)
+        b = np.ascontiguousarray(b)
         ms = np.zeros(11)
         getattr(self.L, self.prefix + "_step_bodies")(_p(out), out.shape[0], _p(prm), _p(b), b.shape[0],
                                                       int(steps), _p(ms))

@@ -1,0 +1,91 @@
+"""The particle input and frame output of the drop-in library (CPU only).
+
+* The importer (snow_io_import, the C face of import_particles) reads the
+  reference's own sample input -- its input/groups.csv and input/particles.csv,
+  kept byte for byte in tests/golden/sample_scene.npz by make_golden.py -- and
+  returns exactly the records the reference's import_particles made from them.
+* A frame written by snow_io_export is byte-identical to the one the
+  reference's export_particles writes for the same records (oracle/_ref).
+* A missing file fails with the reference's error text.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle_lib import REF_SO, ROOT
+
+LIBSNOW = os.path.join(ROOT, "stomakhin-style-snow-simulator_b200", "libsnow.so")
+GOLDEN = os.path.join(ROOT, "tests", "golden", "sample_scene.npz")
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _io():
+    L = ctypes.CDLL(LIBSNOW)
+    L.snow_io_import.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _dp, ctypes.c_int64]
+    L.snow_io_import.restype = ctypes.c_int64
+    L.snow_io_export.argtypes = [_dp, ctypes.c_int64, ctypes.c_int]
+    L.snow_io_export.restype = ctypes.c_int
+    L.snow_io_last_error.restype = ctypes.c_char_p
+    return L
+
+
+def _import(L, groups, particles):
+    n = L.snow_io_import(groups.encode(), particles.encode(), None, 0)
+    if n < 0:
+        return n, None
+    out = np.zeros((n, 26))
+    assert L.snow_io_import(groups.encode(), particles.encode(), out.ctypes.data_as(_dp), n) == n
+    return n, out
+
+
+def test_import_reproduces_reference_import_of_its_sample_input(tmp_path):
+    g = np.load(GOLDEN)
+    (tmp_path / "groups.csv").write_bytes(g["groups_csv"].tobytes())
+    (tmp_path / "particles.csv").write_bytes(g["particles_csv"].tobytes())
+    n, got = _import(_io(), str(tmp_path / "groups.csv"), str(tmp_path / "particles.csv"))
+    assert n == g["imported"].shape[0] == 957
+    assert np.array_equal(got, g["imported"])
+
+
+def test_import_capacity_and_missing_file(tmp_path):
+    L = _io()
+    g = np.load(GOLDEN)
+    (tmp_path / "groups.csv").write_bytes(g["groups_csv"].tobytes())
+    (tmp_path / "particles.csv").write_bytes(g["particles_csv"].tobytes())
+    small = np.zeros((10, 26))
+    assert L.snow_io_import(str(tmp_path / "groups.csv").encode(), str(tmp_path / "particles.csv").encode(),
+                            small.ctypes.data_as(_dp), 10) == -2
+    missing = str(tmp_path / "nope.csv")
+    assert L.snow_io_import(missing.encode(), str(tmp_path / "particles.csv").encode(), None, 0) == -1
+    assert L.snow_io_last_error().decode() == "File not open: " + missing
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference build (oracle/_ref) not present")
+def test_export_matches_reference_export_byte_for_byte(tmp_path):
+    g = np.load(GOLDEN)
+    rec = np.ascontiguousarray(g["step10"])
+    # formatting corner cases, then numbers of every magnitude and sign
+    rec[:12, 0] = [0.0, -0.0, 1e-300, 12345.678901234, -7.5e-7, 4e-320, 999999.5, 123456.5, 1e21,
+                   0.000123456789, np.inf, -np.inf]
+    rng = np.random.default_rng(5)
+    mags = 10.0 ** rng.uniform(-12, 12, (rec.shape[0] - 12, 3))
+    rec[12:, 0:3] = mags * rng.choice([-1.0, 1.0], mags.shape)
+    L = _io()
+    R = ctypes.CDLL(REF_SO)
+    R.ref_export.argtypes = [_dp, ctypes.c_int64, ctypes.c_int]
+    cwd = os.getcwd()
+    try:
+        for who, d in (("ours", tmp_path / "a"), ("ref", tmp_path / "b")):
+            (d / "output").mkdir(parents=True)
+            os.chdir(d)
+            if who == "ours":
+                assert L.snow_io_export(rec.ctypes.data_as(_dp), rec.shape[0], 7) == 0
+            else:
+                R.ref_export(rec.ctypes.data_as(_dp), rec.shape[0], 7)
+    finally:
+        os.chdir(cwd)
+    a = (tmp_path / "a" / "output" / "frame_000007.csv").read_bytes()
+    b = (tmp_path / "b" / "output" / "frame_000007.csv").read_bytes()
+    assert a == b and a.startswith(b"x,y,z\n") and a.count(b"\n") == rec.shape[0] + 1
