@@ -34,7 +34,10 @@ def test_library_exports_every_declared_symbol():
 def test_library_loads_and_reports_abi_without_gpu():
     L = ctypes.CDLL(LIB)
     L.snow_gpu_abi_version.restype = ctypes.c_int
-    assert L.snow_gpu_abi_version() == 1
+    assert L.snow_gpu_abi_version() == 2  # 2: snow_collider gained the box fields (axis, extent)
+    import snow_b200
+
+    assert ctypes.sizeof(snow_b200.Collider) == 152
     # make_plane is pure host logic: unit normal, zero velocity (src/collision.cpp:5-27)
     import snow_b200
 
