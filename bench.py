@@ -52,7 +52,7 @@ def parse():
                          "served: the request stream through the server (single GPU)")
     ap.add_argument("--particles", type=int, default=0,
                     help="tori/touching with this many particles instead of 650,000 (small cases for ncu)")
-    ap.add_argument("--requests", type=int, default=48, help="served: number of requests in the stream")
+    ap.add_argument("--requests", type=int, default=512, help="served: number of requests in the stream")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -265,7 +265,78 @@ def plain_fp64_rate(snow_b200, torch, sp, items, settle: int = 0) -> float:
     return particle_steps / (ms * 1e-3)
 
 
-def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
+def serve_stream(snow_b200, sp, reqs, precision, streaming: bool = True) -> dict:
+    """One served run.  Streaming: run() loops on a thread while this thread
+    submits each request at its arrival time (a Poisson stream in real time,
+    each request stamped on arrival), then closes the stream; otherwise every
+    request is queued with its arrival time before run()."""
+    import threading
+
+    srv = snow_b200.Server(precision, budget_bytes=150 * 10**9, max_steps_per_tick=16)
+    if not streaming:
+        for sc, n, t in reqs:
+            srv.submit(sc, n, t)
+        srv.run(stream=sp)
+    else:
+        srv.set_streaming(True)
+        failure = []
+
+        def serve():
+            try:
+                srv.run(stream=sp)
+            except Exception as e:  # re-raised below
+                failure.append(e)
+
+        th = threading.Thread(target=serve)
+        t0 = time.perf_counter()
+        th.start()
+        for sc, n, t in reqs:
+            wait = t - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            srv.submit(sc, n)
+        srv.end_of_stream()
+        th.join()
+        if failure:
+            raise failure[0]
+    st = srv.stats()
+    srv.close()
+    return st
+
+
+def measure_served(snow_b200, torch, sp, count: int, fp64_rate: float | None = None, grounded: bool = False,
+                   runs: int = 3) -> dict:
+    """The served form on `count` requests (2k..500k particles, 100..2000 steps,
+    Poisson 200/s): every run's throughput, the slowest run's ratio against
+    the plain FP64 path stepping the same requests one at a time, and the
+    median run's latencies."""
+    from snow_b200 import scenes
+
+    reqs = scenes.served_requests(count=count, rate=200.0, grounded=grounded)
+    allruns = [serve_stream(snow_b200, sp, reqs, snow_b200.SNOW_MIXED) for _ in range(runs)]
+    order = sorted(allruns, key=lambda r: r["particle_steps_per_s"])
+    med = order[len(order) // 2]
+    plain_s = plain_fp64_rate(snow_b200, torch, sp, [(sc, n, min(n, 40)) for sc, n, _ in reqs],
+                              settle=40 if grounded else 0)
+    out = {"requests": len(reqs), "arrival_rate_per_s": 200.0, "budget_bytes": 150 * 10**9,
+           "submission": "streaming: submitted at their arrival times while run() loops",
+           "grounded": grounded, "precision": "mixed",
+           "plain_fp64_one_request_at_a_time": plain_s,
+           "plain_fp64_sample": "each request's scene alone, min(steps, 40) timed steps scaled to its requested steps",
+           "runs_particle_steps_per_s": [r["particle_steps_per_s"] for r in allruns],
+           "served_vs_plain_fp64_same_requests_min_run": order[0]["particle_steps_per_s"] / plain_s,
+           "served_vs_plain_fp64_same_requests_median_run": med["particle_steps_per_s"] / plain_s,
+           "p50_latency_s": med["p50_s"], "p99_latency_s": med["p99_s"], "mean_latency_s": med["mean_s"],
+           "particle_steps_per_s": med["particle_steps_per_s"], "completed": med["completed"],
+           "rejected": med["rejected"], "peak_concurrent_scenes": med["peak_scenes"], "ticks": med["ticks"],
+           "reservations": med["reservations"], "wall_s": med["wall_s"],
+           "host_phases_s": {"admit": med["admit_s"], "step": med["step_s"], "retire": med["retire_s"]}}
+    if fp64_rate:
+        out["served_vs_plain_fp64_headline"] = med["particle_steps_per_s"] / fp64_rate
+    return out
+
+
+def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps, served_count: int = 512) -> dict:
     """The mixed-precision, batched and served forms (single GPU).
 
     mixed     the headline scene in the mixed form: particle-steps/s, ratio to the
@@ -356,31 +427,8 @@ def measure_forms(snow_b200, torch, sp, tori, fp64_rate, steps) -> dict:
                         "mixed_vs_plain_fp64_headline": brates["mixed"]["value"] / fp64_rate,
                         "mixed_error_vs_fp64_step10_first16": worst,
                         "graph": "CUDA graph per step", "autotuned": "work-item size and particle ordering"}
-    # -- served: Poisson stream, mixed form
-    reqs = scenes.served_requests(count=48, rate=200.0)
-    runs = []
-    for _ in range(3):  # the host's share varies from run to run: report the median run
-        srv = snow_b200.Server(snow_b200.SNOW_MIXED, budget_bytes=150 * 10**9, max_steps_per_tick=16)
-        for sc, n, t in reqs:
-            srv.submit(sc, n, t)
-        srv.run(stream=sp)
-        runs.append(srv.stats())
-        srv.close()
-    runs.sort(key=lambda r: r["particle_steps_per_s"])
-    st = runs[len(runs) // 2]
-    plain_s = plain_fp64_rate(snow_b200, torch, sp, [(sc, n, min(n, 40)) for sc, n, _ in reqs])
-    forms["served"] = {"requests": len(reqs), "arrival_rate_per_s": 200.0, "budget_bytes": 150 * 10**9,
-                       "plain_fp64_one_request_at_a_time": plain_s,
-                       "plain_fp64_sample": "each request's scene alone, min(steps, 40) timed steps "
-                                            "scaled to its requested steps",
-                       "served_vs_plain_fp64_same_requests": st["particle_steps_per_s"] / plain_s,
-                       "runs_particle_steps_per_s": [r["particle_steps_per_s"] for r in runs],
-                       "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"],
-                       "mean_latency_s": st["mean_s"], "particle_steps_per_s": st["particle_steps_per_s"],
-                       "served_vs_plain_fp64_headline": st["particle_steps_per_s"] / fp64_rate,
-                       "peak_concurrent_scenes": st["peak_scenes"], "ticks": st["ticks"],
-                       "wall_s": st["wall_s"], "precision": "mixed",
-                       "host_phases_s": {"admit": st["admit_s"], "step": st["step_s"], "retire": st["retire_s"]}}
+    # -- served: a Poisson stream submitted while the server runs, mixed form
+    forms["served"] = measure_served(snow_b200, torch, sp, count=served_count, fp64_rate=fp64_rate)
     # -- snowball: error of the mixed form at steps 1, 10, 200
     ball = scenes.snowball_scene()
     a = snow_b200.Batch(snow_b200.SNOW_FP64)
@@ -492,23 +540,7 @@ def measure_colliding(snow_b200, torch, sp, steps, settle=40) -> dict:
                       "mixed_vs_plain_fp64_same_scenes": brates["mixed"]["value"] / plain_b,
                       "fp64_batched_vs_plain_fp64_same_scenes": brates["fp64"]["value"] / plain_b}
     # -- served stream on the ground
-    reqs = scenes.served_requests(count=48, rate=200.0, grounded=True)
-    runs = []
-    for _ in range(3):
-        srv = snow_b200.Server(snow_b200.SNOW_MIXED, budget_bytes=150 * 10**9, max_steps_per_tick=16)
-        for x, n, t in reqs:
-            srv.submit(x, n, t)
-        srv.run(stream=sp)
-        runs.append(srv.stats())
-        srv.close()
-    runs.sort(key=lambda r: r["particle_steps_per_s"])
-    plain_s = plain_fp64_rate(snow_b200, torch, sp, [(x, n, min(n, 40)) for x, n, _ in reqs])
-    out["served"] = {"requests": len(reqs), "precision": "mixed",
-                     "runs_particle_steps_per_s": [r["particle_steps_per_s"] for r in runs],
-                     "plain_fp64_one_request_at_a_time": plain_s,
-                     "served_vs_plain_fp64_same_requests_min_run": runs[0]["particle_steps_per_s"] / plain_s,
-                     "served_vs_plain_fp64_same_requests_median_run": runs[1]["particle_steps_per_s"] / plain_s,
-                     "p50_latency_s": runs[1]["p50_s"], "p99_latency_s": runs[1]["p99_s"]}
+    out["served"] = measure_served(snow_b200, torch, sp, count=96, grounded=True, runs=2)
     return out
 
 
@@ -772,8 +804,9 @@ def run_ours(args, ws, rank, local):
 
     value = ws * sc.n * args.steps / (ms * 1e-3)
     forms = None
-    if ws == 1 and not args.no_forms and args.workload == "tori" and args.precision == "fp64":
-        forms = measure_forms(snow_b200, torch, sp, sc, sc.n * args.steps / (ms * 1e-3), args.steps)
+    if ws == 1 and not args.no_forms and args.workload == "tori" and args.precision == "fp64" and not args.particles:
+        forms = measure_forms(snow_b200, torch, sp, sc, sc.n * args.steps / (ms * 1e-3), args.steps,
+                              served_count=args.requests)
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
@@ -919,6 +952,62 @@ def run_batch(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_served(args, ws, rank, local):
+    """The served stream alone (--workload served): --requests requests (2k..500k
+    particles, 100..2000 steps, Poisson 200/s) submitted at their arrival times
+    while the server runs, mixed form.  With N ranks every rank serves its share
+    of the stream (snow_b200.shard by particles x steps) on its own GPU; value =
+    all requests' particle-steps / the slowest rank's wall time."""
+    import torch
+
+    torch.cuda.set_device(local)
+    import snow_b200
+    from snow_b200 import scenes, shard
+
+    snow_b200.init(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    reqs = scenes.served_requests(count=args.requests, rate=200.0)
+    mine = [reqs[i] for i in shard.shard([sc.n * n for sc, n, _ in reqs], ws, rank)]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    serve_stream(snow_b200, sp, mine[: min(4, len(mine))], snow_b200.SNOW_MIXED)  # warm-up
+    clocks = Clocks(device_selector(torch, local))
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    st = serve_stream(snow_b200, sp, mine, snow_b200.SNOW_MIXED)
+    torch.cuda.synchronize()
+    wall = st["wall_s"]
+    if dist is not None:
+        t = torch.tensor([wall], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall = float(t.item())
+    clk = clocks.stop()
+    total = sum(sc.n * n for sc, n, _ in reqs)
+    line = {"metric": "particle-steps/s", "value": total / wall, "unit": "particle-steps/s", "n_gpus": ws,
+            "steps": None, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic: seeded Poisson stream of scene requests",
+            "config": {"workload": f"served-{len(reqs)}-requests", "precision": "mixed",
+                       "parallelism": f"request shards x{ws}" if ws > 1 else "single GPU",
+                       "submission": "streaming"},
+            "rank0": {k: st[k] for k in ("p50_s", "p99_s", "mean_s", "completed", "ticks", "peak_scenes",
+                                          "reservations", "particle_steps_per_s")},
+            "clocks": clk}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
@@ -926,6 +1015,8 @@ def main():
         run_reference(args, ws, rank)
     elif args.workload == "batch":
         run_batch(args, ws, rank, local)
+    elif args.workload == "served":
+        run_served(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 

@@ -200,12 +200,23 @@ int snow_gpu_batch_autotune(snow_gpu_batch* batch, int trial_steps, int* chosen,
 
 /* ---- serving: continuous batching of independent scenes -----------------
  * No reference counterpart.  Requests are queued with an arrival time (seconds
- * on the server's clock, which starts when run() starts); run() admits each
+ * on the server's clock, which starts when run() starts; a negative arrival_s
+ * stamps the request with the current time on that clock); run() admits each
  * one once it has arrived and the device-memory budget and scene slots allow,
  * runs setup() on it, advances all admitted scenes together (at most
  * max_steps_per_tick steps per tick, never past a scene's end), and retires
  * finished scenes, until every request is done or rejected (a request larger
- * than the whole budget).  Latency = completion - arrival. */
+ * than the whole budget).  Latency = completion - arrival.
+ *
+ * submit, result and stats may be called from any thread, also while run()
+ * loops on another.  With streaming on (set_streaming(1) before or during
+ * run()), run() does not return when it runs out of work but waits for more
+ * submissions, until close() has been called and every request is done;
+ * submit after close() fails with SNOW_E_STATE.  result() returns
+ * SNOW_E_STATE until the request is complete.  Device buffers are reserved
+ * when run() starts for the requests queued then, and grown between ticks,
+ * with 2x headroom, when later requests need more (stats.reservations counts
+ * the reservations of the last run). */
 typedef struct snow_gpu_server snow_gpu_server;
 typedef struct snow_server_stats {
   int64_t completed, rejected, peak_scenes, peak_bytes, ticks, particle_steps;
@@ -214,6 +225,7 @@ typedef struct snow_server_stats {
    * stepping (batched steps, including graph capture after a change of
    * membership), retirement (download + release) */
   double admit_s, step_s, retire_s;
+  int64_t reservations;
 } snow_server_stats;
 int snow_gpu_server_create(snow_gpu_server** out, int precision, int64_t hbm_budget_bytes,
                            int max_scenes, int max_steps_per_tick);
@@ -225,6 +237,8 @@ int snow_gpu_server_run(snow_gpu_server* server, void* stream);
 int snow_gpu_server_result(snow_gpu_server* server, int64_t request_id, double* records, int64_t n,
                            double* latency_s);
 int snow_gpu_server_stats(snow_gpu_server* server, snow_server_stats* stats);
+int snow_gpu_server_set_streaming(snow_gpu_server* server, int on);
+int snow_gpu_server_close(snow_gpu_server* server);
 /* One tick of the last run(): host times on the server's clock (launch of the
  * tick's steps, and the moment the host saw them complete), the device span of
  * the steps (CUDA events on the run's stream, seconds after the first tick's

@@ -11,11 +11,21 @@
 // while a tick runs.  A finished scene is copied
 // back, removed, and its latency (arrival to result) recorded.  Scenes do not
 // interact, so each result is the one the scene would get alone.
+//
+// Requests may be submitted from any thread, also while run() loops.  In
+// streaming mode run() keeps serving (waiting for submissions when idle) until
+// close() is called and every request is done; otherwise it returns once the
+// requests submitted so far are done.  Device buffers are reserved before the
+// loop for the requests already queued, and grown, with headroom and between
+// ticks, only when a request submitted later does not fit what is reserved.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <deque>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -38,9 +48,10 @@ struct Request {
   // progress
   int32_t scene = -1;
   int64_t remaining = 0;
-  double admitted = -1.0, finished = -1.0;
+  double admitted = -1.0;
+  std::atomic<double> finished{-1.0};  // set by the loop once the result is in `records`
   int64_t bytes = 0;
-  bool rejected = false;
+  std::atomic<bool> rejected{false};
   bool pinned = false;  // records page-locked with cudaHostRegister
   int64_t box_blocks = 0;       // upper bound on the block box at the grid spacing
   cudaEvent_t done = nullptr;   // the admission's setup, then the result copy, has passed
@@ -94,15 +105,18 @@ class Server {
   Server(const Server&) = delete;
   Server& operator=(const Server&) = delete;
 
+  // Thread-safe; may be called while run() loops.  arrival < 0 stamps the
+  // request with the current time on the server clock (0 before run()).
   int64_t submit(const double* rec, int64_t n, const snow_step_params* p, const snow_collider* c, int nc,
                  int64_t steps, double arrival) {
     if (n < 0 || (n > 0 && !rec) || steps < 0 || !p || nc < 0 || (nc > 0 && !c))
       throw Error(SNOW_E_ARG, "bad request");
     if (!(p->grid_spacing > 0.0) || !std::isfinite(p->grid_spacing))
       throw Error(SNOW_E_ARG, "grid_spacing must be positive and finite");
+    if (!std::isfinite(arrival)) throw Error(SNOW_E_ARG, "arrival time must be finite");
+    device_colliders(c, nc);  // reject bad colliders at submission, not inside the loop
     const int64_t box = host_box_blocks(rec, n, p->grid_spacing);
     auto r = std::make_unique<Request>();
-    r->id = (int64_t)reqs_.size();
     r->box_blocks = box;
     r->records.assign(rec, rec + n * 26);
     // page-lock the request's records so uploads and result copies run as
@@ -115,11 +129,36 @@ class Server {
     r->params = *p;
     r->colliders.assign(c, c + nc);
     r->steps = steps;
-    r->arrival = arrival;
     r->bytes = footprint(n);
+    check_cuda(cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming), "cudaEventCreate");
+    std::lock_guard<std::mutex> lk(mu_);
+    if (closed_) {
+      if (r->pinned) cudaHostUnregister(r->records.data());
+      cudaEventDestroy(r->done);
+      throw Error(SNOW_E_STATE, "the server is closed to new requests");
+    }
+    r->arrival = arrival >= 0.0 ? arrival : (running_ ? seconds_since(t0_) : 0.0);
+    r->id = (int64_t)reqs_.size();
+    incoming_.push_back(r.get());
     reqs_.push_back(std::move(r));
+    cv_.notify_all();
     return reqs_.back()->id;
   }
+
+  // Streaming mode: run() waits for further submissions when it has nothing
+  // to do, until close().
+  void set_streaming(bool on) {
+    std::lock_guard<std::mutex> lk(mu_);
+    streaming_ = on;
+    cv_.notify_all();
+  }
+  // No more submissions: run() returns once every queued request is done.
+  void close() {
+    std::lock_guard<std::mutex> lk(mu_);
+    closed_ = true;
+    cv_.notify_all();
+  }
+  int64_t reservations() const { return reservations_; }
 
   // Device bytes a scene of n particles holds: two particle buffers, sort
   // buffers, and its share of the grid (about one 4x4x4 block per 32
@@ -134,9 +173,11 @@ class Server {
     return n * per_particle_bytes() + grid + (1 << 16);
   }
 
-  // The loop allocates nothing: streams, events and every buffer that scales
-  // with the requests are made before it (a cudaMalloc or cudaFree inside it
-  // can wait for the tick in flight).  Each pass launches a tick of steps for
+  // The loop allocates nothing for the requests queued when it starts:
+  // streams, events and every buffer that scales with them are made before it
+  // (a cudaMalloc or cudaFree inside it can wait for the tick in flight).
+  // Requests submitted while it runs are reserved for between ticks
+  // (grow_for), in doublings.  Each pass launches a tick of steps for
   // the live scenes, then, while it runs, issues the setup of newly arrived
   // requests in a second batch on a second stream and the result copies of
   // finished scenes on a third, without waiting for either; after the tick it
@@ -144,12 +185,24 @@ class Server {
   // (without copying their particles), finished scenes out of it, and
   // releases scenes whose results have arrived.
   void run(cudaStream_t s) {
-    const auto t0 = clock_t_::now();
+    std::vector<Request*> order;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (running_) throw Error(SNOW_E_STATE, "run() is already running");
+      running_ = true;
+      t0_ = clock_t_::now();
+      order.swap(incoming_);
+    }
+    struct Stop {  // run() may leave by an exception: the server stays usable
+      Server* sv;
+      ~Stop() {
+        std::lock_guard<std::mutex> lk(sv->mu_);
+        sv->running_ = false;
+      }
+    } stop{this};
+    const auto t0 = t0_;
     auto now = [&] { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
     if (!s) s = main_stream();
-    std::vector<Request*> order;
-    for (auto& r : reqs_)
-      if (r->finished < 0 && !r->rejected) order.push_back(r.get());
     std::stable_sort(order.begin(), order.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
     std::deque<Request*> pending(order.begin(), order.end());
     std::vector<Request*> live, admitting, leaving;
@@ -160,7 +213,32 @@ class Server {
     batch_.set_chunk(work_item_ ? work_item_ : auto_work_item(order));
     reserve(order, s);
     admit_s_ += now() - t_phase;
-    while (!pending.empty() || !live.empty() || !admitting.empty() || !leaving.empty()) {
+    for (;;) {
+      // requests submitted since the last pass join the queue in arrival order
+      std::vector<Request*> fresh;
+      bool more_may_come;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        fresh.swap(incoming_);
+        more_may_come = streaming_ && !closed_;
+      }
+      if (!fresh.empty()) {
+        t_phase = now();
+        grow_for(fresh, live, admitting, s);
+        std::stable_sort(fresh.begin(), fresh.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
+        std::deque<Request*> merged;
+        std::merge(pending.begin(), pending.end(), fresh.begin(), fresh.end(), std::back_inserter(merged),
+                   [](Request* a, Request* b) { return a->arrival < b->arrival; });
+        pending.swap(merged);
+        admit_s_ += now() - t_phase;
+      }
+      if (pending.empty() && live.empty() && admitting.empty() && leaving.empty()) {
+        if (!more_may_come) break;
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait_for(lk, std::chrono::milliseconds(5),
+                     [&] { return !incoming_.empty() || closed_ || !streaming_; });
+        continue;
+      }
       // launch this tick (the steps run while the host admits and retires below)
       int64_t k = 0;
       t_phase = now();
@@ -291,12 +369,24 @@ class Server {
     work_item_ = particles;
   }
 
-  const Request& req(int64_t id) const {
-    if (id < 0 || id >= (int64_t)reqs_.size()) throw Error(SNOW_E_ARG, "unknown request id");
-    return *reqs_[id];
+  // The request's result, once run() has completed it (thread-safe).
+  void result(int64_t id, double* records, int64_t n, double* latency_s) {
+    Request* r = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (id < 0 || id >= (int64_t)reqs_.size()) throw Error(SNOW_E_ARG, "unknown request id");
+      r = reqs_[id].get();
+    }
+    if (r->rejected) throw Error(SNOW_E_CAPACITY, "request was rejected: larger than the memory budget");
+    const double fin = r->finished.load();
+    if (fin < 0) throw Error(SNOW_E_STATE, "request has not completed");
+    if (n != (int64_t)r->records.size() / 26) throw Error(SNOW_E_ARG, "particle count differs");
+    std::copy(r->records.begin(), r->records.end(), records);
+    if (latency_s) *latency_s = fin - r->arrival;
   }
 
-  void stats(snow_server_stats* st) const {
+  void stats(snow_server_stats* st) {
+    std::lock_guard<std::mutex> lk(mu_);
     std::vector<double> lat;
     for (auto& r : reqs_)
       if (r->finished >= 0) lat.push_back(r->finished - r->arrival);
@@ -322,6 +412,7 @@ class Server {
     st->admit_s = admit_s_;
     st->step_s = step_s_;
     st->retire_s = retire_s_;
+    st->reservations = reservations_;
   }
 
  private:
@@ -359,6 +450,41 @@ class Server {
     return auto_chunk(std::min(live, budget_ / per_particle_bytes()), prec_);
   }
 
+  // What a set of requests needs reserved at once.
+  struct Need {
+    int64_t live_n = 0, scene_max = 0, box_sum = 0, box_max = 0, grid_max = 0, colliders = 0, slots = 0;
+    std::vector<int64_t> sizes;
+    void add(const Request& r) {
+      const int64_t n = (int64_t)r.records.size() / 26;
+      live_n += n;
+      scene_max = std::max(scene_max, n);
+      box_sum += r.box_blocks;
+      box_max = std::max(box_max, r.box_blocks);
+      grid_max = std::max(grid_max, std::min<int64_t>(2 * r.box_blocks + 1024, 8 * n + 1024));
+      colliders += (int64_t)r.colliders.size();
+      ++slots;
+      sizes.push_back(n);
+    }
+  };
+
+  // Reserves `need` (capped by the budget and the scene slots) in the live,
+  // admission and retirement batches.  Called with no tick in flight.
+  void reserve_need(const Need& need, cudaStream_t s, bool carve_scenes) {
+    const int64_t live_n = std::min(need.live_n, budget_ / per_particle_bytes());
+    const int slots = (int)std::min<int64_t>(need.slots, max_scenes_);
+    batch_.reserve(live_n, 0, slots, (int)std::min<int64_t>(need.colliders, INT32_MAX));
+    batch_.reserve_grid(std::min<int64_t>(2 * need.box_sum + 1024, std::max<int64_t>(8 * live_n + 64, 1024)),
+                        need.box_sum, s);
+    admit_.reserve(need.scene_max, need.scene_max);
+    admit_.reserve_grid(need.grid_max, need.box_max, admit_stream());
+    if (carve_scenes) admit_.reserve_scenes(need.sizes, budget_);
+    retired_.reserve(0, need.scene_max);
+    check_cuda(cudaStreamSynchronize(s), "reserve");
+    check_cuda(cudaStreamSynchronize(admit_stream()), "reserve");
+    reserved_ = need;
+    ++reservations_;
+  }
+
   // Everything the loop needs, made before it: streams, events, and buffers
   // sized for the requests (the live batch's particle buffers, grid and key
   // bins for all admissible requests at once; the admission batch's for the
@@ -368,30 +494,38 @@ class Server {
     retire_stream();
     for (cudaEvent_t* e : {&ev_base_, &ev_start_, &ev_end_})
       if (!*e) check_cuda(cudaEventCreate(e), "cudaEventCreate");
-    int64_t live_n = 0, scene_max = 0, box_sum = 0, box_max = 0, grid_max = 0, colliders = 0;
-    std::vector<int64_t> sizes;
-    for (Request* r : order) {
-      if (!r->done) check_cuda(cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming), "cudaEventCreate");
-      if (r->bytes > budget_) continue;
-      const int64_t n = (int64_t)r->records.size() / 26;
-      live_n += n;
-      scene_max = std::max(scene_max, n);
-      box_sum += r->box_blocks;
-      box_max = std::max(box_max, r->box_blocks);
-      grid_max = std::max(grid_max, std::min<int64_t>(2 * r->box_blocks + 1024, 8 * n + 1024));
-      sizes.push_back(n);
-      colliders += (int64_t)r->colliders.size();
-    }
-    live_n = std::min(live_n, budget_ / per_particle_bytes());
-    const int slots = (int)std::min<int64_t>((int64_t)sizes.size(), max_scenes_);
-    batch_.reserve(live_n, 0, slots, (int)std::min<int64_t>(colliders, INT32_MAX));
-    batch_.reserve_grid(std::min<int64_t>(2 * box_sum + 1024, std::max<int64_t>(8 * live_n + 64, 1024)), box_sum, s);
-    admit_.reserve(scene_max, scene_max);
-    admit_.reserve_grid(grid_max, box_max, admit_stream());
-    admit_.reserve_scenes(sizes, budget_);
-    retired_.reserve(0, scene_max);
-    check_cuda(cudaStreamSynchronize(s), "reserve");
-    check_cuda(cudaStreamSynchronize(admit_stream()), "reserve");
+    Need need;
+    for (Request* r : order)
+      if (r->bytes <= budget_) need.add(*r);
+    reserve_need(need, s, true);
+  }
+
+  // Requests submitted while the loop runs: when the scenes that may be live
+  // together with them (the live and admitting ones, the queue and these) need
+  // more than is reserved, reserve twice that need, so that a stream of
+  // requests causes a logarithmic number of reservations.  Runs between
+  // ticks; the batches grow by themselves in any case, this only moves the
+  // allocations out of the ticks and batches them.
+  void grow_for(const std::vector<Request*>& fresh, const std::vector<Request*>& live,
+                const std::vector<Request*>& admitting, cudaStream_t s) {
+    Need need;
+    for (const auto* group : {&live, &admitting})
+      for (Request* r : *group) need.add(*r);
+    for (Request* r : fresh)
+      if (r->bytes <= budget_) need.add(*r);
+    const Need& have = reserved_;
+    if (need.live_n <= have.live_n && need.scene_max <= have.scene_max && need.box_sum <= have.box_sum &&
+        need.grid_max <= have.grid_max && need.colliders <= have.colliders && need.slots <= have.slots)
+      return;
+    Need twice = need;
+    twice.live_n = 2 * std::max(need.live_n, have.live_n);
+    twice.box_sum = 2 * std::max(need.box_sum, have.box_sum);
+    twice.colliders = 2 * std::max(need.colliders, have.colliders);
+    twice.slots = 2 * std::max(need.slots, have.slots);
+    twice.scene_max = std::max(need.scene_max, have.scene_max);
+    twice.box_max = std::max(need.box_max, have.box_max);
+    twice.grid_max = std::max(need.grid_max, have.grid_max);
+    reserve_need(twice, s, false);
   }
 
   cudaStream_t main_stream() {
@@ -428,7 +562,18 @@ class Server {
   int max_scenes_;
   int64_t max_tick_;
   int work_item_ = 0;
-  std::vector<std::unique_ptr<Request>> reqs_;
+  // Submissions (any thread) and the loop share these under mu_.
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::unique_ptr<Request>> reqs_;  // every request, by id (stable addresses)
+  std::vector<Request*> incoming_;             // submitted, not yet taken by run()
+  bool streaming_ = false, closed_ = false, running_ = false;
+  clock_t_::time_point t0_ = clock_t_::now();  // the server clock starts with run()
+  static double seconds_since(clock_t_::time_point t) {
+    return std::chrono::duration<double>(clock_t_::now() - t).count();
+  }
+  Need reserved_;
+  int64_t reservations_ = 0;
   int64_t rejected_ = 0, peak_scenes_ = 0, peak_bytes_ = 0, ticks_ = 0, particle_steps_ = 0;
   double wall_ = 0.0, admit_s_ = 0.0, step_s_ = 0.0, retire_s_ = 0.0;
 };
@@ -499,12 +644,22 @@ int snow_gpu_server_result(snow_gpu_server* server, int64_t request_id, double* 
                            double* latency_s) {
   return guarded([&] {
     if (!server) throw snow::Error(SNOW_E_ARG, "server is NULL");
-    const auto& r = server->impl->req(request_id);
-    if (r.rejected) throw snow::Error(SNOW_E_CAPACITY, "request was rejected: larger than the memory budget");
-    if (r.finished < 0) throw snow::Error(SNOW_E_STATE, "request has not completed");
-    if (n != (int64_t)r.records.size() / 26) throw snow::Error(SNOW_E_ARG, "particle count differs");
-    std::copy(r.records.begin(), r.records.end(), records);
-    if (latency_s) *latency_s = r.finished - r.arrival;
+    if (n > 0 && !records) throw snow::Error(SNOW_E_ARG, "records is NULL");
+    server->impl->result(request_id, records, n, latency_s);
+  });
+}
+
+int snow_gpu_server_set_streaming(snow_gpu_server* server, int on) {
+  return guarded([&] {
+    if (!server) throw snow::Error(SNOW_E_ARG, "server is NULL");
+    server->impl->set_streaming(on != 0);
+  });
+}
+
+int snow_gpu_server_close(snow_gpu_server* server) {
+  return guarded([&] {
+    if (!server) throw snow::Error(SNOW_E_ARG, "server is NULL");
+    server->impl->close();
   });
 }
 

@@ -68,7 +68,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("completed", "rejected", "peak_scenes", "peak_bytes", "ticks",
                                                "particle_steps")] + \
                [(n, ctypes.c_double) for n in ("wall_s", "p50_s", "p99_s", "mean_s", "particle_steps_per_s",
-                                                "admit_s", "step_s", "retire_s")]
+                                                "admit_s", "step_s", "retire_s")] + \
+               [("reservations", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -134,6 +135,8 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
         "snow_gpu_server_ticks": (ctypes.c_int, [vp, ctypes.POINTER(ServerTick), i64, _i64p]),
         "snow_gpu_server_set_work_item": (ctypes.c_int, [vp, ctypes.c_int]),
+        "snow_gpu_server_set_streaming": (ctypes.c_int, [vp, ctypes.c_int]),
+        "snow_gpu_server_close": (ctypes.c_int, [vp]),
         "snow_gpu_batch_set_chunk": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_set_dense": (ctypes.c_int, [vp, ctypes.c_int]),
         "snow_gpu_batch_chunk": (ctypes.c_int, [vp]),
@@ -525,7 +528,26 @@ class Server:
         except Exception:
             pass
 
-    def submit(self, scene, steps: int, arrival_s: float) -> int:
+    def set_streaming(self, on: bool = True) -> None:
+        """run() waits for further submissions until end_of_stream()."""
+        _check(lib().snow_gpu_server_set_streaming(self._h, int(bool(on))))
+
+    def end_of_stream(self) -> None:
+        """No more submissions (snow_gpu_server_close): run() returns once all are done."""
+        _check(lib().snow_gpu_server_close(self._h))
+
+    def done(self, rid: int) -> bool:
+        """True once request `rid` is complete (its result can be read)."""
+        out = np.empty((self.sizes[rid], 26))
+        rc = lib().snow_gpu_server_result(self._h, rid, _ptr(out), out.shape[0], None)
+        if rc == -6:  # SNOW_E_STATE: not complete yet
+            return False
+        _check(rc)
+        return True
+
+    def submit(self, scene, steps: int, arrival_s: float = -1.0) -> int:
+        """Queues a request; arrival_s < 0 stamps it with the current server time.
+        Thread-safe: may be called while run() loops on another thread."""
         rec = _records(scene.particles)
         prm = StepParams.from_array(scene.params())
         col = colliders(scene.planes) if len(scene.planes) else (Collider * 1)()

@@ -114,3 +114,53 @@ def test_work_item_size_checked(snow):
     for bad in (100, 16, 2048, -1):
         with pytest.raises(snow.SnowError):
             snow.Server(0, work_item=bad)
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 1e-5)])
+def test_requests_submitted_while_running(snow, prec, tol):
+    """Streaming: run() loops on one thread while requests are submitted on
+    another, each stamped with its arrival on the server clock; later requests
+    are larger than anything queued when run() started, so the server grows its
+    reservation between ticks.  Every result equals the scene alone."""
+    import threading
+    import time
+
+    from snow_b200 import scenes
+
+    small = _requests(n=3, seed=31)
+    large = scenes.served_requests(count=5, rate=2000.0, lo=6000, hi=12000, steps_lo=20, steps_hi=40, seed=32)
+    srv = snow.Server(prec, max_steps_per_tick=8)
+    srv.set_streaming(True)
+    ids = [(srv.submit(sc, steps, 0.0), sc, steps) for sc, steps, _ in small]
+    failure = []
+
+    def serve():
+        try:
+            srv.run()
+        except Exception as e:  # reported by the main thread
+            failure.append(e)
+
+    th = threading.Thread(target=serve)
+    th.start()
+    # the first requests complete while the stream is still open
+    deadline = time.time() + 60
+    while not srv.done(ids[0][0]) and time.time() < deadline and not failure:
+        time.sleep(0.005)
+    assert srv.done(ids[0][0]), failure
+    for sc, steps, _ in large:
+        ids.append((srv.submit(sc, steps), sc, steps))
+        time.sleep(0.003)
+    srv.end_of_stream()
+    th.join(timeout=120)
+    assert not th.is_alive() and not failure, failure
+    with pytest.raises(snow.SnowError):
+        srv.submit(small[0][0], 5)  # closed to new requests
+    st = srv.stats()
+    assert st["completed"] == len(ids) and st["rejected"] == 0
+    assert st["reservations"] >= 2, "later, larger requests should grow the reservation"
+    for rid, sc, steps in ids:
+        got, lat = srv.result(rid)
+        assert lat > 0
+        e = errors(got, _alone(snow, prec, sc, steps))
+        assert max(e.values()) < tol, (sc.name, e)
+    srv.close()
