@@ -57,6 +57,32 @@ def test_single_particle(snow, oracle, prec):
     assert max(e["x"], e["F_E"]) < tol, e
 
 
+@pytest.mark.parametrize("graphs", [True, False])
+def test_particle_outrunning_its_key_box(snow, oracle, graphs):
+    """G2P writes the next step's sort keys against the particles' block box
+    grown by one block; a particle that moves more than a block in one step
+    (here 0.12 m per step, 1.5 blocks at dx = 0.02) falls outside it, and that
+    step's keys come from the keys kernel instead, after the counts G2P wrote
+    are cleared.  The result matches the oracle to the FP64 parity bound over
+    steps that take that path and steps that do not."""
+    sc = _cube()
+    fast = sc.particles[:1].copy()
+    fast[0, 0:3] = (0.1, 0.6, 0.5)
+    fast[0, 3:6] = (1200.0, 0.0, 0.0)
+    rec0 = np.concatenate([sc.particles, fast])
+    rec = oracle.setup(rec0, sc.dx)
+    want, _ = oracle.step(rec, sc.params(), sc.plane_array(), 6)
+    b = snow.Batch(snow.SNOW_FP64)
+    b.set_graphs(graphs)
+    sid = b.add_scene(rec, sc.params(), sc.planes)
+    b.step(3)
+    b.step(3)
+    got = b.download(sid)
+    b.close()
+    e = errors(got, want)
+    assert max(e.values()) < 1e-10, e
+
+
 def test_nonfinite_position_is_reported(snow):
     sc = _cube()
     rec = snow.setup(sc.particles.copy(), sc.dx)
