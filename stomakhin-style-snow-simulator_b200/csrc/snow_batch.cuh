@@ -87,6 +87,11 @@ struct SceneDev {
   uint32_t key_count;
   // bounding box of particle blocks measured for the next step (atomics)
   int32_t nb_lo[3], nb_hi[3];
+  // emission box: the key box G2P writes the next step's sort keys against,
+  // the blocks of this step's particles grown by one block on every side (a
+  // particle moves less than a block per step); the next step sorts in it
+  int32_t elo[3], edim[3];
+  uint32_t ekey_base;
 };
 
 struct Counters {
@@ -99,6 +104,12 @@ struct Counters {
   uint32_t fp64_projections;  // mixed form: plastic projections redone in double
   uint32_t bin_ticket;  // next tile of the dense-bin scan
   uint32_t last_blocks, last_fp64;  // n_blocks and fp64_projections of the previous step
+  // next-step keys written by G2P (dense bins only): emit_ok when the emission
+  // boxes fit the bins, emit_fail when a particle fell outside its emission
+  // box; keys_ready when this step's keys and bin counts are G2P's (the keys
+  // kernel then has nothing to do)
+  uint32_t emit_ok, emit_fail, keys_ready;
+  uint32_t emit_blocks;  // block keys of the emission boxes G2P writes against
 };
 
 struct BatchDev {
@@ -140,6 +151,10 @@ struct BatchDev {
   void* acc;                // R[kAccCh][cap_blocks * 64]
   void* vel;                // R[kVelCh][cap_blocks * 64]
   Counters* ctr;
+  // semi-implicit update (null when off): the grid update also writes each
+  // node's mass here and leaves -momentum/mass in the FLIP channels, which the
+  // solve completes once the velocities are final
+  void* imp_mass;           // R[cap_blocks * 64]
 };
 
 // 32-bit mixer (finaliser of MurmurHash3) for the block table.

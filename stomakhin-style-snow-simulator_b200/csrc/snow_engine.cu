@@ -300,6 +300,8 @@ void Batch::size_dense(int64_t key_blocks, cudaStream_t s) {
   if (bins_dirty_) {
     check_cuda(cudaMemsetAsync(bins_, 0, (size_t)cap_bins_ * sizeof(uint32_t), s), "clear bins");
     check_cuda(cudaMemsetAsync(occ_, 0, (size_t)(cap_bins_ / 64), s), "clear bins");
+    check_cuda(cudaMemsetAsync(bin_state_, 0, (size_t)(cap_bins_ / kBinTile + 1) * sizeof(unsigned long long), s),
+               "clear bins");
     bins_dirty_ = false;
   }
 }

@@ -32,11 +32,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdio>
 #include <type_traits>
 
 #include "snow_batch.cuh"
+#include "snow_engine.hpp"
 
 namespace snow {
 
@@ -149,44 +151,19 @@ __global__ void __launch_bounds__(256) k_bbox_init(const BatchDev b) {
 }
 
 // ------------------------------------------------------------------ keyspace
-// kSwap: also swap every scene's particle buffers first (the end of a step:
-// the same launch then prepares the next step's keys).
-template <bool kSwap>
-__global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
+// Exclusive prefix of one count per scene over the block (256 threads, scenes
+// in rounds of 256): writes each scene's base and count through `put` and
+// returns the total (to every thread).
+template <typename Count, typename Put>
+__device__ unsigned long long scene_prefix(const BatchDev& b, Count&& count, Put&& put) {
   __shared__ unsigned long long s_carry;
   __shared__ unsigned long long s_warp[8];
-  if (kSwap)
-    for (int s = threadIdx.x; s < b.num_scenes; s += blockDim.x) b.scenes[s].cur ^= 1;
   if (threadIdx.x == 0) s_carry = 0;
   __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int base = 0; base < b.num_scenes; base += 256) {
     const int s = base + threadIdx.x;
-    unsigned long long cnt = 0;
-    if (s < b.num_scenes) {
-      SceneDev& sc = b.scenes[s];
-      bool empty = false;
-      for (int a = 0; a < 3; ++a) {
-        const int lo = sc.nb_lo[a], hi = sc.nb_hi[a];
-        if (lo > hi) empty = true;
-        sc.lo[a] = lo;
-        sc.dim[a] = empty ? 0 : (hi - lo + 2);  // +1 block of margin for the neighbours
-      }
-      if (empty) {
-        // no finite position (or no particles): a one-block box keeps the keys
-        // of any particles inside this scene's key range
-        for (int a = 0; a < 3; ++a) {
-          sc.lo[a] = 0;
-          sc.dim[a] = sc.n > 0 ? 2 : 0;
-        }
-      }
-      cnt = (unsigned long long)sc.dim[0] * sc.dim[1] * sc.dim[2];
-      for (int a = 0; a < 3; ++a) {
-        sc.nb_lo[a] = INT_MAX;
-        sc.nb_hi[a] = INT_MIN;
-      }
-    }
-    // inclusive scan of cnt over the block
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned long long cnt = s < b.num_scenes ? count(s) : 0ull;
     unsigned long long x = cnt;
     for (int o = 1; o < 32; o <<= 1) {
       const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
@@ -197,18 +174,99 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
     unsigned long long before = 0;
     for (int w = 0; w < warp; ++w) before += s_warp[w];
     const unsigned long long incl = s_carry + before + x;
-    if (s < b.num_scenes) {
-      SceneDev& sc = b.scenes[s];
-      const unsigned long long kb = incl - cnt;
-      sc.key_base = (uint32_t)(kb > 0xFFFFFFFFull ? 0xFFFFFFFFull : kb);
-      sc.key_count = (uint32_t)(cnt > 0xFFFFFFFFull ? 0xFFFFFFFFull : cnt);
-    }
+    if (s < b.num_scenes) put(s, incl - cnt, cnt);
     __syncthreads();
     if (threadIdx.x == 255) s_carry = incl;
     __syncthreads();
   }
+  const unsigned long long total = s_carry;
+  __syncthreads();  // s_carry is reset by the next call
+  return total;
+}
+
+__device__ __forceinline__ uint32_t clamp32(unsigned long long v) {
+  return (uint32_t)(v > 0xFFFFFFFFull ? 0xFFFFFFFFull : v);
+}
+
+// Key boxes of the coming step.  kSwap: also swap every scene's particle
+// buffers first (the end of a step: the same launch then prepares the next
+// step's keys).
+//
+// The sorting box of the coming step is the emission box the step just ended
+// wrote its particles' keys against, when it wrote them all (emit_ok and no
+// emit_fail; keys_ready then tells the keys kernel to do nothing); otherwise
+// the particles' own block box, one block of margin on the high side (the
+// keys kernel computes the keys).  The emission box for the coming step's G2P
+// is the particles' block box grown by one block on every side, plus the same
+// high margin: emit_ok when those boxes fit the dense bins.
+template <bool kSwap>
+__global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
+  __shared__ int s_emitted, s_cleanup;
+  if (kSwap)
+    for (int s = threadIdx.x; s < b.num_scenes; s += blockDim.x) b.scenes[s].cur ^= 1;
   if (threadIdx.x == 0) {
-    const unsigned long long total = s_carry;
+    const bool armed = b.ctr->emit_ok != 0;  // the last G2P may have written keys and counts
+    const bool tried = kSwap && b.dense && armed;
+    s_emitted = tried && !b.ctr->emit_fail;
+    const bool leftovers = kSwap ? tried && b.ctr->emit_fail : armed;
+    const unsigned long long eb = b.ctr->emit_blocks;
+    s_cleanup = leftovers && b.bins && b.occ && eb * 64 <= (unsigned long long)b.cap_bins ? (int)eb : 0;
+  }
+  __syncthreads();
+  const bool emitted = s_emitted != 0;
+  if (s_cleanup) {
+    // Counts and occupancy G2P wrote that no step will consume: G2P gave up
+    // part way (a particle left its emission box, which a particle moving less
+    // than a block per step never does), or this is a fresh start (after an
+    // upload, setup or a change of scenes) and the keys kernel sorts.
+    uint4* bins4 = reinterpret_cast<uint4*>(b.bins);
+    for (int64_t k = threadIdx.x; k < (int64_t)s_cleanup * 16; k += blockDim.x) bins4[k] = make_uint4(0, 0, 0, 0);
+    for (int64_t k = threadIdx.x; k < (int64_t)s_cleanup; k += blockDim.x) b.occ[k] = 0;
+    __syncthreads();
+  }
+  // a scene's particle block box (empty: a one-block box keeps the keys of any
+  // particles inside this scene's key range)
+  auto measured = [&](const SceneDev& sc, int lo[3], int dim[3], int grow) {
+    bool empty = false;
+    for (int a = 0; a < 3; ++a) empty |= sc.nb_lo[a] > sc.nb_hi[a];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = empty ? 0 : sc.nb_lo[a] - grow;
+      dim[a] = empty ? (sc.n > 0 ? 2 : 0) : (sc.nb_hi[a] - sc.nb_lo[a] + 2 + 2 * grow);
+    }
+  };
+  const unsigned long long total = scene_prefix(
+      b,
+      [&](int s) {
+        SceneDev& sc = b.scenes[s];
+        int lo[3], dim[3];
+        if (emitted) {
+          for (int a = 0; a < 3; ++a) lo[a] = sc.elo[a], dim[a] = sc.edim[a];
+        } else {
+          measured(sc, lo, dim, 0);
+        }
+        for (int a = 0; a < 3; ++a) sc.lo[a] = lo[a], sc.dim[a] = dim[a];
+        return (unsigned long long)dim[0] * dim[1] * dim[2];
+      },
+      [&](int s, unsigned long long base, unsigned long long cnt) {
+        b.scenes[s].key_base = clamp32(base);
+        b.scenes[s].key_count = clamp32(cnt);
+      });
+  const unsigned long long etotal = scene_prefix(
+      b,
+      [&](int s) {
+        SceneDev& sc = b.scenes[s];
+        int lo[3], dim[3];
+        measured(sc, lo, dim, 1);
+        for (int a = 0; a < 3; ++a) {
+          sc.elo[a] = lo[a];
+          sc.edim[a] = dim[a];
+          sc.nb_lo[a] = INT_MAX;
+          sc.nb_hi[a] = INT_MIN;
+        }
+        return (unsigned long long)dim[0] * dim[1] * dim[2];
+      },
+      [&](int s, unsigned long long base, unsigned long long) { b.scenes[s].ekey_base = clamp32(base); });
+  if (threadIdx.x == 0) {
     uint32_t bits = 6;
     if (total > (1ull << 26)) {
       atomicOr(&b.ctr->status, ST_KEY_OVERFLOW);
@@ -224,6 +282,10 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
     c->sort_bits = bits;
     c->key_blocks = (uint32_t)min(total, (unsigned long long)UINT32_MAX);
     if (b.dense && total * 64 > (unsigned long long)b.cap_bins) atomicOr(&c->status, ST_BIN_OVERFLOW);
+    c->keys_ready = emitted ? 1u : 0u;
+    c->emit_fail = 0;
+    c->emit_ok = (b.dense && etotal <= (1ull << 26) && etotal * 64 <= (unsigned long long)b.cap_bins) ? 1u : 0u;
+    c->emit_blocks = (uint32_t)min(etotal, (unsigned long long)UINT32_MAX);
     c->bin_ticket = 0;
     c->n_blocks = 0;
     c->work_p2g = c->work_grid = c->work_g2p = c->work_aux = 0;
@@ -255,14 +317,28 @@ __device__ __forceinline__ void key_run(uint32_t key, int lane, int& first, int&
 // bins, also the per-key particle counts (one atomic per run of equal keys in
 // a warp: the particles arrive nearly sorted from the previous step) and the
 // occupancy of each block key; the tile states of the bin scan are cleared.
+// Nothing to do when the previous step's G2P wrote all of it (keys_ready).
+// Grid-stride over warps of 32 consecutive particles, so that a launch with
+// nothing to do ends after a small grid.
+template <typename R>
+__device__ __forceinline__ void keys_for(const BatchDev& b, int64_t t, bool dense);
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_keys(const BatchDev b) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b.ctr->keys_ready) return;
   const bool dense = b.dense && bins_fit(b);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (dense) {
     const int64_t ntiles = ((int64_t)b.ctr->key_blocks * 64 + kBinTile - 1) / kBinTile;
-    for (int64_t j = t; j < ntiles; j += (int64_t)gridDim.x * blockDim.x) b.bin_state[j] = 0;
+    for (int64_t j = t0; j < ntiles; j += stride) b.bin_state[j] = 0;
   }
+  const int64_t span = (b.total + 31) / 32 * 32;  // whole warps: key_run uses every lane
+  for (int64_t t = t0; t < span; t += stride) keys_for<R>(b, t, dense);
+}
+
+template <typename R>
+__device__ __forceinline__ void keys_for(const BatchDev& b, int64_t t, bool dense) {
   const bool valid = t < b.total;
   uint32_t key = 0xFFFFFFFFu;
   if (valid) {
@@ -526,6 +602,9 @@ __global__ void __launch_bounds__(256) k_bins(const BatchDev b) {
 __global__ void __launch_bounds__(256) k_scatter(const BatchDev b) {
   if (!bins_fit(b)) return;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // the scan's tile states are spent: clear every tile for the next step (whose
+  // keys G2P may write before any other kernel runs)
+  for (int64_t j = t; j < b.cap_bins / kBinTile + 1; j += (int64_t)gridDim.x * blockDim.x) b.bin_state[j] = 0;
   const int lane = threadIdx.x & 31;
   const bool valid = t < b.total;
   const uint32_t key = valid ? b.keys[0][t] : 0xFFFFFFFFu;
@@ -1088,10 +1167,12 @@ __global__ void __launch_bounds__(256) k_grid_update(const BatchDev b) {
     const R py = dx * (R)(4 * bc.y + ((node >> 2) & 3));
     const R pz = dx * (R)(4 * bc.z + (node >> 4));
     for (int c = 0; c < sc.coll_count; ++c) collide(b.colliders[sc.coll_begin + c], px, py, pz, v[0], v[1], v[2]);
+    const bool later = b.imp_mass != nullptr;  // the implicit solve finishes the FLIP channels
+    if (later) reinterpret_cast<R*>(b.imp_mass)[e] = m;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       vel[a * plane + e] = v[a];
-      vel[(3 + a) * plane + e] = m > R(0) ? v[a] - pm[a] : R(0);
+      vel[(3 + a) * plane + e] = m > R(0) ? (later ? -pm[a] : v[a] - pm[a]) : R(0);
     }
 #pragma unroll
     for (int ch = 0; ch < kAccCh; ++ch) acc[ch * plane + e] = R(0);
@@ -1135,13 +1216,23 @@ __device__ __forceinline__ void flush_box(SceneDev& ps, int bmin[3], int bmax[3]
 // kMixedTau of each other (used_fp64 = true; see near_critical).
 constexpr float kMixedTau = 1e-5f;
 
+// Both precisions first try the elastic fast path (elastic_projection: no
+// clamp within a margin, root from the polar factor); particles near or past a
+// clamp bound take the eigensolve as before.
+constexpr double kElasticMargin = 1e-12;
+
 template <typename R>
 __device__ __forceinline__ Plastic<R> project(M3<R>& FE, const SceneDev& sc, bool& used_fp64) {
   if constexpr (std::is_same<R, double>::value) {
-    return plastic_projection(FE, 1.0 - sc.theta_c, 1.0 + sc.theta_s);
+    const double lo = 1.0 - sc.theta_c, hi = 1.0 + sc.theta_s;
+    Plastic<double> fast;
+    if (elastic_projection(FE, lo, hi, kElasticMargin, fast)) return fast;
+    return plastic_projection(FE, lo, hi);
   } else {
     const M3<float> trial = FE;
     const float lo = 1.0f - (float)sc.theta_c, hi = 1.0f + (float)sc.theta_s;
+    Plastic<float> fast;
+    if (elastic_projection(FE, lo, hi, kMixedTau, fast)) return fast;
     Plastic<float> pl = plastic_projection(FE, lo, hi);
     if (!near_critical(pl.sigma, lo, hi, kMixedTau, pl.clamped)) return pl;
     used_fp64 = true;
@@ -1312,6 +1403,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
   const int64_t plane = (int64_t)b.cap_blocks * 64;
   int bmin[3] = {INT_MAX, INT_MAX, INT_MAX}, bmax[3] = {INT_MIN, INT_MIN, INT_MIN};
   int last_scene = -1;
+  // write the next step's sort keys and bin counts (see k_keyspace)
+  const bool emit = MODE == G2P_FULL && b.dense && b.ctr->emit_ok;
 
   __shared__ int s_item;
   ItemQueue q;
@@ -1380,6 +1473,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
       const int tx = wx.base - 4 * h.bx, ty = wy.base - 4 * h.by, tz = wz.base - 4 * h.bz;
       if ((unsigned)tx > 3u || (unsigned)ty > 3u || (unsigned)tz > 3u) {
         flag(b, ST_OUT_OF_BOX);  // non-finite or mis-sorted particle: never index the tile with it
+        if (emit) atomicOr(&b.ctr->emit_fail, 1u);  // and no key of it for the next step
         continue;
       }
 
@@ -1486,18 +1580,46 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
           for (int c = 0; c < sc.coll_count; ++c)
             collide(b.colliders[sc.coll_begin + c], x[0], x[1], x[2], vn[0], vn[1], vn[2]);
           R* rw = (R*)sc.r[cur ^ 1];
+          int nblk[3], ncell[3];
+          bool finite = true;
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
             const R xn = x[a] + dt * vn[a];
             rw[(PX + a) * st + o] = xn;
             rw[(PV + a) * st + o] = vn[a];
+            nblk[a] = ncell[a] = 0;
             if (isfinite((double)xn)) {
-              int cell;
-              const int bc = block_coord(xn, dx, cell);
-              bmin[a] = min(bmin[a], bc);
-              bmax[a] = max(bmax[a], bc);
+              nblk[a] = block_coord(xn, dx, ncell[a]);
+              bmin[a] = min(bmin[a], nblk[a]);
+              bmax[a] = max(bmax[a], nblk[a]);
             } else {
+              finite = false;
               flag(b, ST_NONFINITE);
+            }
+          }
+          if (emit) {
+            // the next step's sort key against the scene's emission box, as
+            // k_keys would compute it, and its bin count (one atomic per key
+            // among the warp's lanes: neighbouring particles share cells)
+            bool ok = finite;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) ok &= nblk[a] >= sc.elo[a] && nblk[a] <= sc.elo[a] + sc.edim[a] - 2;
+            uint32_t key = 0xFFFFFFFFu;
+            if (ok) {
+              const uint32_t bk =
+                  sc.ekey_base + (uint32_t)(((int64_t)(nblk[2] - sc.elo[2]) * sc.edim[1] + (nblk[1] - sc.elo[1])) *
+                                                sc.edim[0] +
+                                            (nblk[0] - sc.elo[0]));
+              key = (bk << 6) | (uint32_t)(ncell[0] + 4 * ncell[1] + 16 * ncell[2]);
+              b.keys[0][j] = key;
+              b.vals[0][j] = (uint32_t)o;
+            } else {
+              atomicOr(&b.ctr->emit_fail, 1u);
+            }
+            const unsigned same = __match_any_sync(__activemask(), key);
+            if (ok && (threadIdx.x & 31) == __ffs(same) - 1) {
+              atomicAdd(&b.bins[key], (uint32_t)__popc(same));
+              b.occ[key >> 6] = 1;
             }
           }
           V0 = slot->v0[me];
@@ -1528,8 +1650,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_g2p(const Batch
           // from the trial F_E, which is kept for it in the output slot.
           trial = FEn;
           const R lo = R(1) - (R)sc.theta_c, hi = R(1) + (R)sc.theta_s;
-          pl = plastic_projection(FEn, lo, hi);
-          needs_double = near_critical(pl.sigma, lo, hi, (R)kMixedTau, pl.clamped);
+          if (!elastic_projection(FEn, lo, hi, (R)kMixedTau, pl)) {
+            pl = plastic_projection(FEn, lo, hi);
+            needs_double = near_critical(pl.sigma, lo, hi, (R)kMixedTau, pl.clamped);
+          }
         } else {
           bool used_fp64 = false;
           pl = project(FEn, sc, used_fp64);
@@ -1662,30 +1786,62 @@ __global__ void k_finish(const BatchDev b) {
 }
 
 // ------------------------------------------------------------ launch helpers
+// Launch settings that depend on the device (SM count, the occupancy of a
+// persistent kernel, a kernel's shared-memory attribute) are set up once per
+// device and kept per device: a process may drive several GPUs, from several
+// host threads.
+constexpr int kMaxDevices = 64;
+
+int current_device() {
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) throw Error(SNOW_E_ARG, "device index out of range");
+  return dev;
+}
+
+struct PerDevice {
+  std::atomic<int> v[kMaxDevices];
+  PerDevice() {
+    for (auto& x : v) x.store(0);
+  }
+  // The value for the current device, computed by `make` the first time
+  // (two threads may both compute it; they store the same value).
+  template <typename F>
+  int get(F&& make) {
+    std::atomic<int>& x = v[current_device()];
+    int r = x.load(std::memory_order_acquire);
+    if (!r) {
+      r = make();
+      x.store(r, std::memory_order_release);
+    }
+    return r;
+  }
+};
+
 template <typename K>
 int persistent_grid(K kernel, int threads, size_t smem) {
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem), "occupancy");
   if (per_sm < 1) per_sm = 1;
   return per_sm * sm_count();
 }
 
 template <typename K>
 void set_smem(K kernel, size_t smem) {
-  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024)
+    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               "shared memory size");
 }
 
 }  // namespace
 
 int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 1;
-  }
-  return n;
+  static PerDevice count;
+  return count.get([] {
+    int n = 0;
+    check_cuda(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, current_device()), "SM count");
+    return n > 0 ? n : 1;
+  });
 }
 
 template <typename R>
@@ -1700,31 +1856,35 @@ void StepLaunch<R>::keyspace(const BatchDev& b, cudaStream_t s, bool) {
 template <typename R>
 void StepLaunch<R>::keys(const BatchDev& b, cudaStream_t s) {
   if (b.total <= 0) return;
-  k_keys<R><<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
+  // grid-stride: a few waves at most, so that the launch is short when the
+  // previous step's G2P already wrote the keys
+  const int64_t want = (b.total + 255) / 256;
+  k_keys<R><<<(unsigned)std::min<int64_t>(want, 8 * (int64_t)sm_count()), 256, 0, s>>>(b);
 }
 template <typename R>
 void StepLaunch<R>::blocks(const BatchDev& b, cudaStream_t s) {
   if (b.total <= 0) return;
   if (b.dense) {
-    static int grid = 0;
-    if (!grid) grid = persistent_grid(k_bins, 256, 0);
+    static PerDevice bins_grid;
+    const int grid = bins_grid.get([] { return persistent_grid(k_bins, 256, 0); });
     const int64_t tiles = b.cap_bins / kBinTile;
     k_bins<<<(unsigned)std::min<int64_t>(grid, std::max<int64_t>(tiles, 1)), 256, 0, s>>>(b);
     k_scatter<<<(unsigned)((b.total + 255) / 256), 256, 0, s>>>(b);
     return;
   }
-  cudaMemsetAsync(b.htab, 0xFF, sizeof(unsigned long long) * ((size_t)b.hmask + 1), s);
+  check_cuda(cudaMemsetAsync(b.htab, 0xFF, sizeof(unsigned long long) * ((size_t)b.hmask + 1), s),
+             "clear block table");
   k_blocks<<<(unsigned)((b.total + b.chunk - 1) / b.chunk), b.chunk, 0, s>>>(b);
 }
 
 template <typename R, int MODE>
 static void launch_p2g(const BatchDev& b, cudaStream_t s) {
   const size_t smem = p2g_smem<R, MODE>();
-  static int grid = 0;
-  if (!grid) {
+  static PerDevice grids;
+  const int grid = grids.get([&] {
     set_smem(k_p2g<R, MODE>, smem);
-    grid = persistent_grid(k_p2g<R, MODE>, 256, smem);
-  }
+    return persistent_grid(k_p2g<R, MODE>, 256, smem);
+  });
   k_p2g<R, MODE><<<grid, 256, smem, s>>>(b);
 }
 template <typename R>
@@ -1741,8 +1901,8 @@ void StepLaunch<R>::p2g(const BatchDev& b, int mode, cudaStream_t s) {
 template <typename R>
 void StepLaunch<R>::grid_update(const BatchDev& b, cudaStream_t s) {
   if (b.total <= 0) return;
-  static int grid = 0;
-  if (!grid) grid = persistent_grid(k_grid_update<R>, 256, 0);
+  static PerDevice grids;
+  const int grid = grids.get([] { return persistent_grid(k_grid_update<R>, 256, 0); });
   k_grid_update<R><<<grid, 256, 0, s>>>(b);
 }
 template <typename R>
@@ -1753,11 +1913,11 @@ void StepLaunch<R>::zero_grid(const BatchDev& b, cudaStream_t s) {
 template <typename R, int MODE>
 static void launch_g2p(const BatchDev& b, cudaStream_t s) {
   const size_t smem = sizeof(R) * G2PTile<R, MODE>::size() + (MODE == G2P_FULL ? sizeof(G2PSlots<R>) : 0);
-  static int grid = 0;
-  if (!grid) {
+  static PerDevice grids;
+  const int grid = grids.get([&] {
     set_smem(k_g2p<R, MODE>, smem);
-    grid = persistent_grid(k_g2p<R, MODE>, 256, smem);
-  }
+    return persistent_grid(k_g2p<R, MODE>, 256, smem);
+  });
   k_g2p<R, MODE><<<grid, 256, smem, s>>>(b);
 }
 template <typename R>

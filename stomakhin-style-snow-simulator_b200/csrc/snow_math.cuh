@@ -345,6 +345,208 @@ SNOW_HD Plastic<T> plastic_projection(M3<T>& FE, T lo, T hi) {
   return out;
 }
 
+// ------------------------------------------------------ elastic fast path
+// Most particles are not clamped in a step; for them the projection is the
+// identity and only sqrt(F F^T) is needed, which the polar factor gives
+// without an eigensolve: F = R S (R orthogonal, S symmetric positive
+// definite), sqrt(F F^T) = R S R^T = F R^T, and the singular values of F are
+// the eigenvalues of S.
+//
+// polar_newton: Newton's iteration X <- (X + X^-T) / 2 from X = F (Higham,
+// "Computing the polar decomposition -- with applications", SIAM J. Sci.
+// Stat. Comput. 7 (1986) 1160-1174).  It keeps the singular vectors and maps
+// each singular value s to (s + 1/s) / 2, so the error e = s - 1 becomes
+// e^2 / (2 (1 + e)): from |e| <= 0.1, 4 iterations fall below double rounding
+// (0.1 -> 4.5e-3 -> 1e-5 -> 5e-11 -> 1e-21) and 3 below float rounding.  The
+// iteration is accepted when the last one moved X by at most last_step (so
+// the error left is below last_step^2 / 2) and det X stayed positive; else the
+// caller takes the general path.  X^-T = cof(X) / det X (cofactor matrix).
+template <typename T>
+struct PolarTol;
+template <>
+struct PolarTol<double> {
+  static constexpr int iters = 4;
+  static constexpr double last_step = 1e-8;
+};
+template <>
+struct PolarTol<float> {
+  static constexpr int iters = 3;
+  static constexpr float last_step = 3e-4f;
+};
+
+template <typename T>
+SNOW_HD bool polar_newton(const M3<T>& F, M3<T>& X) {
+  X = F;
+  T moved = T(0);
+#pragma unroll
+  for (int it = 0; it < PolarTol<T>::iters; ++it) {
+    M3<T> C;  // cofactors: C(r, c) = (-1)^(r+c) minor(r, c)
+    C(0, 0) = X(1, 1) * X(2, 2) - X(1, 2) * X(2, 1);
+    C(0, 1) = X(1, 2) * X(2, 0) - X(1, 0) * X(2, 2);
+    C(0, 2) = X(1, 0) * X(2, 1) - X(1, 1) * X(2, 0);
+    C(1, 0) = X(0, 2) * X(2, 1) - X(0, 1) * X(2, 2);
+    C(1, 1) = X(0, 0) * X(2, 2) - X(0, 2) * X(2, 0);
+    C(1, 2) = X(0, 1) * X(2, 0) - X(0, 0) * X(2, 1);
+    C(2, 0) = X(0, 1) * X(1, 2) - X(0, 2) * X(1, 1);
+    C(2, 1) = X(0, 2) * X(1, 0) - X(0, 0) * X(1, 2);
+    C(2, 2) = X(0, 0) * X(1, 1) - X(0, 1) * X(1, 0);
+    const T det = X(0, 0) * C(0, 0) + X(0, 1) * C(0, 1) + X(0, 2) * C(0, 2);
+    if (!(det > T(0))) return false;
+    const T h = T(0.5) / det;
+    moved = T(0);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      const T x = T(0.5) * X.a[e] + h * C.a[e];
+      moved = fmax(moved, fabs(x - X.a[e]));
+      X.a[e] = x;
+    }
+  }
+  return moved <= PolarTol<T>::last_step;
+}
+
+// Positive definiteness of a symmetric 3x3 by its leading principal minors.
+template <typename T>
+SNOW_HD bool positive_definite(const Sym3<T>& A) {
+  if (!(A.xx > T(0))) return false;
+  if (!(A.xx * A.yy - A.xy * A.xy > T(0))) return false;
+  const T det = A.xx * (A.yy * A.zz - A.yz * A.yz) - A.xy * (A.xy * A.zz - A.yz * A.xz) +
+                A.xz * (A.xy * A.yz - A.yy * A.xz);
+  return det > T(0);
+}
+
+// The projection of a particle whose singular values all lie in
+// [lo + margin, hi - margin]: S - (lo + margin) I and (hi - margin) I - S are
+// positive definite.  Then no clamp acts (F_E stays, D = I) and the root is
+// F R^T; returns true with `out` filled in.  Returns false (out untouched)
+// when the iteration did not settle or a singular value may lie outside, or
+// within `margin` of a bound: the general path (plastic_projection) decides
+// those, so every clamp decision near a bound is the eigensolve's, as before.
+// margin: 1e-12 in double (rounding of S is ~1e-16), the mixed form's
+// near-critical distance in float.
+template <typename T>
+SNOW_HD bool elastic_projection(const M3<T>& F, T lo, T hi, T margin, Plastic<T>& out) {
+  M3<T> R;
+  if (!polar_newton(F, R)) return false;
+  Sym3<T> S;  // R^T F
+  S.xx = R(0, 0) * F(0, 0) + R(1, 0) * F(1, 0) + R(2, 0) * F(2, 0);
+  S.yy = R(0, 1) * F(0, 1) + R(1, 1) * F(1, 1) + R(2, 1) * F(2, 1);
+  S.zz = R(0, 2) * F(0, 2) + R(1, 2) * F(1, 2) + R(2, 2) * F(2, 2);
+  S.xy = R(0, 0) * F(0, 1) + R(1, 0) * F(1, 1) + R(2, 0) * F(2, 1);
+  S.xz = R(0, 0) * F(0, 2) + R(1, 0) * F(1, 2) + R(2, 0) * F(2, 2);
+  S.yz = R(0, 1) * F(0, 2) + R(1, 1) * F(1, 2) + R(2, 1) * F(2, 2);
+  const T a = lo + margin, b = hi - margin;
+  if (!positive_definite(Sym3<T>{S.xx - a, S.yy - a, S.zz - a, S.xy, S.xz, S.yz})) return false;
+  if (!positive_definite(Sym3<T>{b - S.xx, b - S.yy, b - S.zz, -S.xy, -S.xz, -S.yz})) return false;
+  out.root.xx = F(0, 0) * R(0, 0) + F(0, 1) * R(0, 1) + F(0, 2) * R(0, 2);  // (F R^T)(r, c) = sum_k F(r,k) R(c,k)
+  out.root.yy = F(1, 0) * R(1, 0) + F(1, 1) * R(1, 1) + F(1, 2) * R(1, 2);
+  out.root.zz = F(2, 0) * R(2, 0) + F(2, 1) * R(2, 1) + F(2, 2) * R(2, 2);
+  out.root.xy = F(0, 0) * R(1, 0) + F(0, 1) * R(1, 1) + F(0, 2) * R(1, 2);
+  out.root.xz = F(0, 0) * R(2, 0) + F(0, 1) * R(2, 1) + F(0, 2) * R(2, 2);
+  out.root.yz = F(1, 0) * R(2, 0) + F(1, 1) * R(2, 1) + F(1, 2) * R(2, 2);
+  out.Dinv = Sym3<T>{T(1), T(1), T(1), T(0), T(0), T(0)};
+  out.sigma[0] = out.sigma[1] = out.sigma[2] = T(1);  // inside [lo, hi]; not used on this path
+  out.clamped = false;
+  out.regular = true;
+  return true;
+}
+
+// ------------------------------------------------- implicit update algebra
+// Differential of the fixed-corotated first Piola-Kirchhoff stress
+// P = 2 mu (F - R) + lambda (J - 1) J F^-T at F (Stomakhin et al. 2013, the
+// implicit update's A_p), given the polar factors F = R S:
+//   dP = 2 mu (dF - dR) + lambda (C : dF) C + lambda (J - 1) dC,
+// C = J F^-T = cof(F), dC its differential, and dR = R [w]_x with
+// (tr(S) I - S) w = axial(R^T dF - dF^T R) (R^T dR is skew and
+// R^T dR S + S R^T dR equals the skew right-hand side).
+template <typename T>
+SNOW_HD M3<T> cofactor3(const M3<T>& F) {
+  M3<T> C;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+      C(r, c) = F(r1, c1) * F(r2, c2) - F(r1, c2) * F(r2, c1);
+    }
+  return C;
+}
+
+template <typename T>
+SNOW_HD M3<T> corotated_differential(const M3<T>& F, const M3<T>& R, const Sym3<T>& S, T mu, T lambda,
+                                     const M3<T>& dF) {
+  // m = axial(R^T dF - dF^T R); K = R^T dF, so the skew part's axial vector is
+  // (K(2,1) - K(1,2), K(0,2) - K(2,0), K(1,0) - K(0,1))
+  T K[9];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) K[c * 3 + r] = R(0, r) * dF(0, c) + R(1, r) * dF(1, c) + R(2, r) * dF(2, c);
+  const T m0 = K[1 * 3 + 2] - K[2 * 3 + 1], m1 = K[2 * 3 + 0] - K[0 * 3 + 2], m2 = K[0 * 3 + 1] - K[1 * 3 + 0];
+  // A = tr(S) I - S (symmetric), w = A^-1 m by cofactors
+  const T tr = S.xx + S.yy + S.zz;
+  const T a = tr - S.xx, b = tr - S.yy, c = tr - S.zz, d = -S.xy, e = -S.xz, f = -S.yz;
+  const T i00 = b * c - f * f, i01 = e * f - d * c, i02 = d * f - b * e;
+  const T i11 = a * c - e * e, i12 = d * e - a * f, i22 = a * b - d * d;
+  const T inv = T(1) / (a * i00 + d * i01 + e * i02);
+  const T w0 = (i00 * m0 + i01 * m1 + i02 * m2) * inv;
+  const T w1 = (i01 * m0 + i11 * m1 + i12 * m2) * inv;
+  const T w2 = (i02 * m0 + i12 * m1 + i22 * m2) * inv;
+  const M3<T> C = cofactor3(F);
+  const T J = F(0, 0) * C(0, 0) + F(0, 1) * C(0, 1) + F(0, 2) * C(0, 2);
+  T dJ = T(0);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) dJ += C.a[k] * dF.a[k];
+  M3<T> out;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      // dR(r, cc) = sum_k R(r, k) W(k, cc), W = [w]_x
+      const T W0 = cc == 0 ? T(0) : (cc == 1 ? -w2 : w1);  // W(0, cc)
+      const T W1 = cc == 0 ? w2 : (cc == 1 ? T(0) : -w0);  // W(1, cc)
+      const T W2 = cc == 0 ? -w1 : (cc == 1 ? w0 : T(0));  // W(2, cc)
+      const T dR = R(r, 0) * W0 + R(r, 1) * W1 + R(r, 2) * W2;
+      const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
+      const T dC = dF(r1, c1) * F(r2, c2) + F(r1, c1) * dF(r2, c2) - dF(r1, c2) * F(r2, c1) -
+                   F(r1, c2) * dF(r2, c1);
+      out(r, cc) = T(2) * mu * (dF(r, cc) - dR) + lambda * dJ * C(r, cc) + lambda * (J - T(1)) * dC;
+    }
+  return out;
+}
+
+// Polar factors F = R S of F (S symmetric positive definite): the Newton
+// iteration when it settles, else the eigensolve of F^T F (S = V sqrt(L) V^T,
+// R = F S^-1).  Returns false for a singular F.
+template <typename T>
+SNOW_HD bool polar_factors(const M3<T>& F, M3<T>& R, Sym3<T>& S) {
+  if (!polar_newton(F, R)) {
+    T lam[3], q[9];
+    sym_eig3(gram_cols(F), lam, q, EigTol<T>::tol, EigTol<T>::sweeps);
+    T inv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const T s = sqrt(lam[i] > T(0) ? lam[i] : T(0));
+      if (!(s > T(0))) return false;
+      inv[i] = T(1) / s;
+    }
+    const Sym3<T> Si = spectral(q, inv);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const T f0 = F(r, 0), f1 = F(r, 1), f2 = F(r, 2);
+      R(r, 0) = f0 * Si.xx + f1 * Si.xy + f2 * Si.xz;
+      R(r, 1) = f0 * Si.xy + f1 * Si.yy + f2 * Si.yz;
+      R(r, 2) = f0 * Si.xz + f1 * Si.yz + f2 * Si.zz;
+    }
+  }
+  S.xx = R(0, 0) * F(0, 0) + R(1, 0) * F(1, 0) + R(2, 0) * F(2, 0);
+  S.yy = R(0, 1) * F(0, 1) + R(1, 1) * F(1, 1) + R(2, 1) * F(2, 1);
+  S.zz = R(0, 2) * F(0, 2) + R(1, 2) * F(1, 2) + R(2, 2) * F(2, 2);
+  S.xy = R(0, 0) * F(0, 1) + R(1, 0) * F(1, 1) + R(2, 0) * F(2, 1);
+  S.xz = R(0, 0) * F(0, 2) + R(1, 0) * F(1, 2) + R(2, 0) * F(2, 2);
+  S.yz = R(0, 1) * F(0, 2) + R(1, 1) * F(1, 2) + R(2, 1) * F(2, 2);
+  return true;
+}
+
 // Mixed-precision guard: true when a singular value of the trial F_E lies
 // within `tau` of a clamp bound (the float eigensolve may decide the clamp
 // wrongly), or when a clamp acts and two singular values lie within `tau` of
