@@ -253,6 +253,7 @@ struct NodeIdxHash {
 struct Node {
   double mass = 0.0;
   Vec3 momentum, velocity, force;
+  Vec3 delta_v, delta_force;  // the implicit update's Krylov vector and its force differential
 };
 using Grid = std::unordered_map<NodeIdx, Node, NodeIdxHash>;
 
@@ -543,6 +544,185 @@ void particle_collisions(Particle& p, const std::vector<Plane>& bodies) {
 }
 void position_update(Particle& p, double dt) { p.x = p.x + dt * p.v; }
 
+// ---------------------------------------------------------- implicit update
+// The semi-implicit grid velocity update of Stomakhin et al., "A material
+// point method for snow simulation", SIGGRAPH 2013, Section 4 (eq. 9) and its
+// technical report's differentials.  The reference declares the functions
+// (include/snow/grid.hpp:76,80,88-92: constitutive_differential, index_nodes,
+// deformation_differential, force_differential, apply_A, Conjugate_residual)
+// and defines none; these follow the paper:
+//   (I + beta dt^2 M^-1 H) v = v*   on the nodes with mass, v* the explicit
+// update after collisions, H u = -delta f(u) with
+//   delta F_p = dt (sum_i u_i grad w_ip^T) F_Ep,
+//   delta f_i = -sum_p V_p0 A_p(delta F_p) F_Ep^T grad w_ip,
+// A_p the differential of the fixed-corotated P at F_Ep (F_P and so the
+// hardening held fixed).  The operator is self-adjoint in the mass-weighted
+// inner product <a, b>_M = sum_i m_i a_i . b_i, in which the conjugate
+// residual method is run (it also handles the indefinite case).
+
+inline Mat3 cofactor(const Mat3& F) {  // J F^-T
+  Mat3 C;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+      C(r, c) = F(r1, c1) * F(r2, c2) - F(r1, c2) * F(r2, c1);
+    }
+  return C;
+}
+inline Mat3 cofactor_differential(const Mat3& F, const Mat3& dF) {
+  Mat3 C;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+      C(r, c) = dF(r1, c1) * F(r2, c2) + F(r1, c1) * dF(r2, c2) - dF(r1, c2) * F(r2, c1) - F(r1, c2) * dF(r2, c1);
+    }
+  return C;
+}
+
+// constitutive_differential (declared at grid.hpp:76): dP for P = 2 mu (F - R)
+// + lambda (J - 1) J F^-T at F = F_E:
+//   dP = 2 mu (dF - dR) + lambda (J F^-T : dF) J F^-T + lambda (J - 1) d(J F^-T).
+// dR from F = R S: W = R^T dR is skew and W S + S W = R^T dF - dF^T R, i.e.
+// (tr(S) I - S) w = m for the axial vectors w of W and m of the right side.
+Mat3 constitutive_differential(const Particle& p, const Mat3& dF, double mu0, double lambda0, double xi) {
+  const double h = std::exp(xi * (1.0 - det(p.FP)));
+  const double mu = mu0 * h, lambda = lambda0 * h;
+  Mat3 U, V;
+  Vec3 sv;
+  svd3(p.FE, U, sv, V);
+  const Mat3 R = U * transpose(V);
+  const Mat3 S = V * diag(sv) * transpose(V);
+  const Mat3 M = transpose(R) * dF - transpose(dF) * R;
+  const Vec3 m{M(2, 1), M(0, 2), M(1, 0)};
+  const double tr = S(0, 0) + S(1, 1) + S(2, 2);
+  const Mat3 A = tr * Mat3::identity() - S;
+  const Vec3 w = inverse(A) * m;
+  Mat3 W;
+  W(0, 1) = -w[2];
+  W(0, 2) = w[1];
+  W(1, 0) = w[2];
+  W(1, 2) = -w[0];
+  W(2, 0) = -w[1];
+  W(2, 1) = w[0];
+  const Mat3 dR = R * W;
+  const Mat3 C = cofactor(p.FE);
+  const double J = det(p.FE);
+  double dJ = 0.0;
+  for (int e = 0; e < 9; ++e) dJ += C.a[e] * dF.a[e];
+  return (2 * mu) * (dF - dR) + (lambda * dJ) * C + (lambda * (J - 1)) * cofactor_differential(p.FE, dF);
+}
+
+// index_nodes (declared at grid.hpp:80): the nodes with mass, the unknowns.
+std::vector<Node*> index_nodes(Grid& grid) {
+  std::vector<Node*> out;
+  for (auto& [idx, node] : grid)
+    if (node.mass > 0) out.push_back(&node);
+  return out;
+}
+
+// Stencil gradient of node idx at gp = x / dx (the same product as
+// stress_update's basis_gradient, grid.cpp:262-270).
+inline Vec3 basis_gradient(const NodeIdx& idx, const Vec3& gp, double dx) {
+  const double Nx = N(idx.i, gp[0]), Ny = N(idx.j, gp[1]), Nz = N(idx.k, gp[2]);
+  const double dNx = N_dash(idx.i, gp[0]), dNy = N_dash(idx.j, gp[1]), dNz = N_dash(idx.k, gp[2]);
+  return Vec3{dNx * Ny * Nz * (1 / dx), Nx * dNy * Nz * (1 / dx), Nx * Ny * dNz * (1 / dx)};
+}
+
+// deformation_differential (declared at grid.hpp:88): dt (sum_i dv_i grad w_ip^T) F_Ep.
+Mat3 deformation_differential(const Grid& grid, const Particle& p, double dx, double dt) {
+  const Vec3 gp = p.x / dx;
+  int base[3];
+  base_of(gp, base);
+  Mat3 g;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j)
+      for (int k = 0; k < 4; ++k) {
+        const NodeIdx idx{i + base[0], j + base[1], k + base[2]};
+        auto it = grid.find(idx);
+        if (it == grid.end()) continue;
+        g = g + outer(it->second.delta_v, basis_gradient(idx, gp, dx));
+      }
+  return dt * (g * p.FE);
+}
+
+// force_differential (declared at grid.hpp:89): node delta_force += -V_p0 dP F_E^T grad w.
+void force_differential(Grid& grid, const Particle& p, double dx, double dt, double mu0, double lambda0,
+                        double xi) {
+  const Mat3 dP = constitutive_differential(p, deformation_differential(grid, p, dx, dt), mu0, lambda0, xi);
+  const Mat3 G = (-p.V0) * (dP * transpose(p.FE));
+  const Vec3 gp = p.x / dx;
+  int base[3];
+  base_of(gp, base);
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j)
+      for (int k = 0; k < 4; ++k) {
+        const NodeIdx idx{i + base[0], j + base[1], k + base[2]};
+        auto it = grid.find(idx);
+        if (it == grid.end()) continue;
+        it->second.delta_force += G * basis_gradient(idx, gp, dx);
+      }
+}
+
+// apply_A (declared at grid.hpp:90): (A q)_i = q_i - beta dt delta f_i(q) / m_i
+// over the Krylov nodes.
+std::vector<Vec3> apply_A(Grid& grid, const std::vector<Particle>& snow, const std::vector<Node*>& nodes,
+                          const std::vector<Vec3>& q, double dx, double dt, double mu0, double lambda0, double xi,
+                          double beta) {
+  for (auto& [idx, node] : grid) node.delta_v = node.delta_force = Vec3{};
+  for (std::size_t i = 0; i < nodes.size(); ++i) nodes[i]->delta_v = q[i];
+  for (const Particle& p : snow) force_differential(grid, p, dx, dt, mu0, lambda0, xi);
+  std::vector<Vec3> out(nodes.size());
+  for (std::size_t i = 0; i < nodes.size(); ++i)
+    out[i] = q[i] - (beta * dt / nodes[i]->mass) * nodes[i]->delta_force;
+  return out;
+}
+
+inline double mdot(const std::vector<Node*>& nodes, const std::vector<Vec3>& a, const std::vector<Vec3>& b) {
+  double s = 0.0;
+  for (std::size_t i = 0; i < nodes.size(); ++i) s += nodes[i]->mass * dot(a[i], b[i]);
+  return s;
+}
+
+// Conjugate_residual (declared at grid.hpp:91): solves A v = v* from v = v*
+// until <r, r>_M <= squared_tolerance <v*, v*>_M or maximum_iterations;
+// writes the node velocities.  Returns the iterations taken.
+int Conjugate_residual(Grid& grid, const std::vector<Particle>& snow, const std::vector<Node*>& nodes, double dx,
+                       double dt, double mu0, double lambda0, double xi, double beta, double squared_tolerance,
+                       int maximum_iterations, double* residual = nullptr) {
+  const std::size_t n = nodes.size();
+  std::vector<Vec3> b(n), x(n), r(n), p(n), Ar, Ap;
+  for (std::size_t i = 0; i < n; ++i) b[i] = x[i] = nodes[i]->velocity;
+  const double bb = mdot(nodes, b, b);
+  const std::vector<Vec3> Ax = apply_A(grid, snow, nodes, x, dx, dt, mu0, lambda0, xi, beta);
+  for (std::size_t i = 0; i < n; ++i) p[i] = r[i] = b[i] - Ax[i];
+  Ar = apply_A(grid, snow, nodes, r, dx, dt, mu0, lambda0, xi, beta);
+  Ap = Ar;
+  double gamma = mdot(nodes, r, Ar);
+  double rr = mdot(nodes, r, r);
+  int it = 0;
+  while (it < maximum_iterations && rr > squared_tolerance * bb) {
+    const double alpha = gamma / mdot(nodes, Ap, Ap);
+    for (std::size_t i = 0; i < n; ++i) {
+      x[i] += alpha * p[i];
+      r[i] = r[i] - alpha * Ap[i];
+    }
+    ++it;
+    rr = mdot(nodes, r, r);
+    if (rr <= squared_tolerance * bb) break;
+    Ar = apply_A(grid, snow, nodes, r, dx, dt, mu0, lambda0, xi, beta);
+    const double gamma_next = mdot(nodes, r, Ar);
+    const double beta_k = gamma_next / gamma;
+    gamma = gamma_next;
+    for (std::size_t i = 0; i < n; ++i) {
+      p[i] = r[i] + beta_k * p[i];
+      Ap[i] = Ar[i] + beta_k * Ap[i];
+    }
+  }
+  for (std::size_t i = 0; i < n; ++i) nodes[i]->velocity = x[i];
+  if (residual) *residual = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+  return it;
+}
+
 // setup (grid.cpp:340-357).
 void setup(std::vector<Particle>& snow, double dx) {
   Grid grid;
@@ -559,8 +739,17 @@ struct StepParams {
 
 // step (grid.cpp:359-450): same stage order and OpenMP placement.  `ms` gets
 // the ten stage times in StepTimings order (include/snow/debug.hpp:3-15).
+// Optional semi-implicit update (beta = 0: the reference's explicit step).
+struct ImplicitParams {
+  double beta = 0.0, squared_tolerance = 1e-12;
+  int max_iterations = 50;
+  int iterations = 0;     // out: Conjugate_residual iterations of the last step
+  double residual = 0.0;  // out: its relative residual
+};
+
 void step(std::vector<Particle>& snow, const std::vector<Plane>& bodies,
-          std::vector<Stencil>& stencils, const StepParams& prm, double ms[10]) {
+          std::vector<Stencil>& stencils, const StepParams& prm, double ms[10],
+          ImplicitParams* imp = nullptr) {
   using clk = std::chrono::steady_clock;
   auto since = [](clk::time_point t0) {
     return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
@@ -586,6 +775,11 @@ void step(std::vector<Particle>& snow, const std::vector<Plane>& bodies,
   ms[4] += since(t0);
   t0 = clk::now();
   grid_collisions(grid, bodies, prm.dx);
+  if (imp && imp->beta > 0) {
+    const std::vector<Node*> nodes = index_nodes(grid);
+    imp->iterations = Conjugate_residual(grid, snow, nodes, prm.dx, prm.dt, prm.mu0, prm.lambda0, prm.xi, imp->beta,
+                                         imp->squared_tolerance, imp->max_iterations, &imp->residual);
+  }
   ms[5] += since(t0);
   t0 = clk::now();
 #pragma omp parallel for
@@ -687,6 +881,107 @@ void oracle_step(double* rec, int64_t n, const double* params, const double* pla
 void oracle_step_bodies(double* rec, int64_t n, const double* params, const double* bodies, int n_bodies,
                         int steps, double* stage_ms) {
   run_steps(rec, n, params, to_bodies(bodies, n_bodies), steps, stage_ms);
+}
+
+// Steps with the semi-implicit update (beta > 0); iterations[k] and
+// residual[k] report step k's solve.
+void oracle_step_implicit(double* rec, int64_t n, const double* params, const double* planes, int n_planes,
+                          int steps, double beta, double squared_tolerance, int max_iterations, int* iterations,
+                          double* residual) {
+  auto v = to_vec(rec, n);
+  StepParams p;
+  std::memcpy(&p, params, sizeof(StepParams));
+  const auto bodies = to_planes(planes, n_planes);
+  std::vector<Stencil> st(v.size());
+  double ms[10] = {0};
+  for (int k = 0; k < steps; ++k) {
+    ImplicitParams imp;
+    imp.beta = beta;
+    imp.squared_tolerance = squared_tolerance;
+    imp.max_iterations = max_iterations;
+    step(v, bodies, st, p, ms, &imp);
+    if (iterations) iterations[k] = imp.iterations;
+    if (residual) residual[k] = imp.residual;
+  }
+  from_vec(v, rec);
+}
+
+// constitutive_differential of one particle record; dF and dP column-major.
+void oracle_constitutive_differential(const double* rec, const double* dF, double mu0, double lambda0, double xi,
+                                      double* dP) {
+  const Particle p = to_vec(rec, 1)[0];
+  Mat3 d;
+  std::memcpy(d.a, dF, sizeof d.a);
+  const Mat3 out = constitutive_differential(p, d, mu0, lambda0, xi);
+  std::memcpy(dP, out.a, sizeof out.a);
+}
+void oracle_force_constitutive(const double* rec, double mu0, double lambda0, double xi, double* P) {
+  const Particle p = to_vec(rec, 1)[0];
+  const Mat3 out = force_constitutive(p, mu0, lambda0, xi);
+  std::memcpy(P, out.a, sizeof out.a);
+}
+
+// The grid that P2G + forces + grid_velocity + collisions of one step build
+// from the records (the state the implicit solve starts from), over its
+// nodes with mass in index_nodes' order: ijk[m][3] and fields[m][10] (mass,
+// momentum, velocity, force) when given; with q (m x 3): out = A q; without q
+// (out given): out = the Conjugate_residual solution.  Returns m (the node
+// count; nothing is written when out is NULL or m > cap).
+int64_t oracle_implicit_grid(const double* rec, int64_t n, const double* params, const double* planes,
+                             int n_planes, double beta, double squared_tolerance, int max_iterations,
+                             const double* q, double* out, int32_t* ijk, double* fields, int64_t cap,
+                             int* iterations) {
+  auto snow = to_vec(rec, n);
+  StepParams prm;
+  std::memcpy(&prm, params, sizeof(StepParams));
+  const auto bodies = to_planes(planes, n_planes);
+  Grid grid;
+  std::vector<Stencil> st(snow.size());
+  for (std::size_t i = 0; i < snow.size(); ++i) st[i] = build_stencil(snow[i], prm.dx);
+  for (std::size_t i = 0; i < snow.size(); ++i) p2g(grid, snow[i], st[i]);
+  for (std::size_t i = 0; i < snow.size(); ++i)
+    force_grid_accumulation(force_constitutive(snow[i], prm.mu0, prm.lambda0, prm.xi), snow[i], st[i]);
+  grid_velocity(grid, Vec3{prm.gravity[0], prm.gravity[1], prm.gravity[2]}, prm.dt);
+  grid_collisions(grid, bodies, prm.dx);
+  std::vector<Node*> nodes;
+  std::vector<NodeIdx> idx;
+  for (auto& [k, node] : grid)
+    if (node.mass > 0) {
+      nodes.push_back(&node);
+      idx.push_back(k);
+    }
+  const int64_t m = (int64_t)nodes.size();
+  if (!out || m > cap) return m;
+  for (int64_t i = 0; i < m; ++i) {
+    if (ijk) {
+      ijk[3 * i] = idx[i].i;
+      ijk[3 * i + 1] = idx[i].j;
+      ijk[3 * i + 2] = idx[i].k;
+    }
+    if (fields) {
+      double* f = fields + 10 * i;
+      f[0] = nodes[i]->mass;
+      for (int c = 0; c < 3; ++c) {
+        f[1 + c] = nodes[i]->momentum[c];
+        f[4 + c] = nodes[i]->velocity[c];
+        f[7 + c] = nodes[i]->force[c];
+      }
+    }
+  }
+  if (q) {
+    std::vector<Vec3> qq(m);
+    for (int64_t i = 0; i < m; ++i) qq[i] = Vec3{q[3 * i], q[3 * i + 1], q[3 * i + 2]};
+    const auto a = apply_A(grid, snow, nodes, qq, prm.dx, prm.dt, prm.mu0, prm.lambda0, prm.xi, beta);
+    for (int64_t i = 0; i < m; ++i)
+      for (int c = 0; c < 3; ++c) out[3 * i + c] = a[i][c];
+    return m;
+  }
+  const int it = Conjugate_residual(grid, snow, nodes, prm.dx, prm.dt, prm.mu0, prm.lambda0, prm.xi, beta,
+                                    squared_tolerance, max_iterations);
+  if (iterations) *iterations = it;
+  for (int64_t i = 0; i < m; ++i)
+    for (int c = 0; c < 3; ++c) out[3 * i + c] = nodes[i]->velocity[c];
+  return m;
 }
 
 double oracle_N(double a, double b) { return N(a, b); }

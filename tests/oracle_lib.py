@@ -97,6 +97,65 @@ class Oracle(_StepLib):
         L.oracle_position_update.argtypes = [_dp, ctypes.c_int64, ctypes.c_double]
         L.oracle_svd3.argtypes = [_dp, _dp, _dp, _dp]
 
+    def step_implicit(self, rec: np.ndarray, params, planes, steps: int, beta: float,
+                      squared_tolerance: float = 1e-12, max_iterations: int = 50):
+        """Steps with the semi-implicit update; returns (records, iterations[steps], residual[steps])."""
+        L = self.L
+        L.oracle_step_implicit.argtypes = [_dp, ctypes.c_int64, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip, _dp]
+        out = np.ascontiguousarray(rec, dtype=np.float64).copy()
+        prm = np.ascontiguousarray(params, dtype=np.float64)
+        pl = np.ascontiguousarray(np.asarray(planes, dtype=np.float64).reshape(-1, 7))
+        its = np.zeros(steps, np.int32)
+        res = np.zeros(steps)
+        L.oracle_step_implicit(_p(out), out.shape[0], _p(prm), _p(pl), pl.shape[0], int(steps), float(beta),
+                               float(squared_tolerance), int(max_iterations), _p(its, _ip), _p(res))
+        return out, its, res
+
+    def constitutive_differential(self, rec1: np.ndarray, dF: np.ndarray, mu0, lambda0, xi) -> np.ndarray:
+        """dP (3x3) of one particle record for the 3x3 dF (both as numpy 3x3 arrays)."""
+        self.L.oracle_constitutive_differential.argtypes = [_dp, _dp] + [ctypes.c_double] * 3 + [_dp]
+        r = np.ascontiguousarray(rec1, dtype=np.float64).reshape(26)
+        d = np.ascontiguousarray(np.asarray(dF, dtype=np.float64).T.reshape(9))  # column-major
+        out = np.zeros(9)
+        self.L.oracle_constitutive_differential(_p(r), _p(d), mu0, lambda0, xi, _p(out))
+        return out.reshape(3, 3).T
+
+    def force_constitutive(self, rec1: np.ndarray, mu0, lambda0, xi) -> np.ndarray:
+        self.L.oracle_force_constitutive.argtypes = [_dp] + [ctypes.c_double] * 3 + [_dp]
+        r = np.ascontiguousarray(rec1, dtype=np.float64).reshape(26)
+        out = np.zeros(9)
+        self.L.oracle_force_constitutive(_p(r), mu0, lambda0, xi, _p(out))
+        return out.reshape(3, 3).T
+
+    def implicit_grid(self, rec: np.ndarray, params, planes, beta: float, q: np.ndarray | None = None,
+                      squared_tolerance: float = 1e-24, max_iterations: int = 300):
+        """The grid one step of the records builds (its nodes with mass): returns
+        (ijk, fields[m][10] before the solve, A q -- or the solved velocities
+        when q is None --, iterations).  q is taken over the first m rows."""
+        L = self.L
+        L.oracle_implicit_grid.argtypes = [_dp, ctypes.c_int64, _dp, _dp, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int, _dp, _dp, _ip, _dp, ctypes.c_int64, _ip]
+        L.oracle_implicit_grid.restype = ctypes.c_int64
+        r = np.ascontiguousarray(rec, dtype=np.float64)
+        prm = np.ascontiguousarray(params, dtype=np.float64)
+        pl = np.ascontiguousarray(np.asarray(planes, dtype=np.float64).reshape(-1, 7))
+        m = L.oracle_implicit_grid(_p(r), r.shape[0], _p(prm), _p(pl), pl.shape[0], beta, squared_tolerance,
+                                   max_iterations, None, None, None, None, 0, None)
+        out = np.zeros((m, 3))
+        ijk = np.zeros((m, 3), np.int32)
+        fields = np.zeros((m, 10))
+        it = np.zeros(1, np.int32)
+        qq = None
+        if q is not None:
+            qq = np.zeros((m, 3))
+            qn = np.asarray(q, dtype=np.float64).reshape(-1, 3)
+            qq[: min(m, qn.shape[0])] = qn[:m]
+        L.oracle_implicit_grid(_p(r), r.shape[0], _p(prm), _p(pl), pl.shape[0], beta, squared_tolerance,
+                               max_iterations, None if qq is None else _p(qq), _p(out), _p(ijk, _ip), _p(fields), m,
+                               _p(it, _ip))
+        return ijk, fields, out, int(it[0])
+
     def N(self, a, b):
         return self.L.oracle_N(float(a), float(b))
 
