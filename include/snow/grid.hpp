@@ -17,8 +17,13 @@
 //  * N, N_dash and build_stencil are evaluated on the host from the same
 //    B-spline code the kernels use; they return host data.
 //  * constitutive_differential, index_nodes, deformation_differential,
-//    force_differential, apply_A and Conjugate_residual are declared, as in
-//    the reference, and defined nowhere (the reference solver is explicit only).
+//    force_differential, apply_A and Conjugate_residual, which the reference
+//    declares and never defines, implement Stomakhin et al.'s semi-implicit
+//    velocity update: the particle work on the GPU (snow_gpu_stage_*), the
+//    Krylov vectors over the nodes with mass.  Conjugate_residual solves
+//    (I + beta dt^2 M^-1 H) v = v* from the nodes' velocities, until
+//    <r, r>_M <= squared_tolerance <v*, v*>_M (mass-weighted) or
+//    maximum_iterations, and writes the velocities back.
 #pragma once
 
 #include <array>

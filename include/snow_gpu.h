@@ -198,6 +198,21 @@ int snow_gpu_batch_sort_mode(snow_gpu_batch* batch);
 int snow_gpu_batch_autotune(snow_gpu_batch* batch, int trial_steps, int* chosen, double* ms_per_step,
                             void* stream);
 
+/* Semi-implicit velocity update (Stomakhin et al. 2013, eq. 9).  The
+ * reference declares its pieces -- constitutive_differential, index_nodes,
+ * deformation_differential, force_differential, apply_A and
+ * Conjugate_residual (include/snow/grid.hpp:76,80,88-92) -- and defines none.
+ * beta = 0 (the default) is the reference's explicit step.  With beta in
+ * (0, 1], after the grid update and collisions the velocities of the nodes
+ * with mass solve (I + beta dt^2 M^-1 H) v = v*, H the Hessian of the elastic
+ * energy (F_P held fixed), by conjugate residuals in the mass-weighted inner
+ * product until the residual falls below `tolerance` relative to v*, or
+ * `max_iterations`.  Steps then run kernel by kernel (the solve reads its dot
+ * products back), not from a CUDA graph. */
+int snow_gpu_batch_set_implicit(snow_gpu_batch* batch, double beta, double tolerance, int max_iterations);
+/* Iterations and relative residual of the last step's solve. */
+int snow_gpu_batch_implicit_stats(snow_gpu_batch* batch, int* iterations, double* residual);
+
 /* ---- serving: continuous batching of independent scenes -----------------
  * No reference counterpart.  Requests are queued with an arrival time (seconds
  * on the server's clock, which starts when run() starts; a negative arrival_s
@@ -309,6 +324,29 @@ int snow_gpu_stage_stress(const double* records, int64_t n, double mu_0, double 
  * forces[n][64][3] is added to the stencil's nodes by the caller. */
 int snow_gpu_stage_force_scatter(const double* records, int64_t n, const double* P,
                                  const double* gradients, double* forces);
+/* The implicit update's differentials (Stomakhin et al. 2013; declared and not
+ * defined by the reference, include/snow/grid.hpp:76,88): per particle,
+ * dP[n][9] = the differential of the fixed-corotated stress at F_E for
+ * dF[n][9], and dF[n][9] = dt (sum_e delta_v[n][e] gradients[n][e]^T) F_E over
+ * the 64 stencil entries (delta_v, gradients: [n][64][3]).  Column-major. */
+int snow_gpu_stage_constitutive_differential(const double* records, int64_t n, const double* dF, double mu_0,
+                                             double lambda_0, double hardening_coefficient, double* dP);
+int snow_gpu_stage_deformation_differential(const double* records, int64_t n, double time_step,
+                                            const double* gradients, const double* delta_v, double* dF);
+/* apply_A and Conjugate_residual (declared at include/snow/grid.hpp:90-91 of
+ * the reference, defined nowhere there) on a host grid: nodes ijk[n][3] and
+ * fields[n][10] as above, the particles whose stencils the operator couples,
+ * and the step's parameters.  The unknowns are the nodes with mass.  With q
+ * (n_nodes x 3): out = A q = q - beta dt delta f(q) / m at nodes with mass and
+ * q elsewhere.  With q NULL: out = the solution of A v = velocity by conjugate
+ * residuals in the mass-weighted inner product, from v = velocity, until
+ * <r, r>_M <= squared_tolerance <velocity, velocity>_M or max_iterations
+ * (*iterations gets the count); massless nodes keep their velocity. */
+int snow_gpu_stage_implicit(const int32_t* ijk, const double* fields, int64_t n_nodes,
+                            const double* records, int64_t n, double grid_spacing, double time_step,
+                            double mu_0, double lambda_0, double hardening_coefficient, double beta,
+                            double squared_tolerance, int max_iterations, const double* q, double* out,
+                            int* iterations);
 int snow_gpu_stage_grid_velocity(double* fields, int64_t n_nodes, const double gravity[3],
                                  double time_step);
 int snow_gpu_stage_grid_collisions(const int32_t* ijk, double* fields, int64_t n_nodes,

@@ -204,6 +204,7 @@ Batch::~Batch() {
   free_bins();
   dfree(staging_);
   dfree(d_tmp_scene_);
+  free_implicit();
   for (auto& c : cache_) free_scene(c);
   for (int k = 0; k < 2; ++k) {
     if (pinned_ev_[k]) {
@@ -595,6 +596,7 @@ BatchDev Batch::dev(SceneDev* scenes, int num_scenes, int64_t total) const {
   b.acc = acc_;
   b.vel = vel_;
   b.ctr = d_ctr_;
+  b.imp_mass = imp_beta_ > 0.0 ? imp_nodes_ : nullptr;
   b.dense = dense_ ? 1 : 0;
   b.cap_bins = cap_bins_;
   b.bins = bins_;
@@ -692,6 +694,7 @@ void Batch::launch_step(const BatchDev& b, cudaStream_t s, cudaEvent_t* ev) {
   StepLaunch<R>::p2g(b, P2G_PRE, s);
   mark(2);
   StepLaunch<R>::grid_update(b, s);
+  if (b.imp_mass) implicit_solve<R>(b, s);
   mark(3);
   StepLaunch<R>::g2p(b, G2P_FULL, s);
   StepLaunch<R>::fixup(b, s);
@@ -735,6 +738,7 @@ void Batch::step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s)
   // own (blocking) stream instead, which orders itself with NULL-stream work.
   if (!s) s = own_stream_;
   prepare(s);
+  if (imp_beta_ > 0.0) ensure_implicit();  // sized for this step's grid and particles
   const BatchDev b = dev(d_scenes_, num_dev_scenes_, total_);
   if (force_dirty_) {
     // P2G reads each particle's force matrix, which G2P keeps current from step
@@ -774,7 +778,7 @@ void Batch::step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s)
       timings->stress_update += ms[3];
     }
     for (auto& e : ev) cudaEventDestroy(e);
-  } else if (use_graphs_) {
+  } else if (use_graphs_ && imp_beta_ == 0.0) {  // the implicit solve reads back scalars: no graph
     int k = 0;
     if (!gexec_) {
       // first step eagerly (initialises per-kernel launch settings), then capture
@@ -1231,6 +1235,18 @@ int snow_gpu_batch_set_chunk(snow_gpu_batch* batch, int chunk) {
 }
 int snow_gpu_batch_chunk(snow_gpu_batch* batch) {
   return batch && batch->impl ? batch->impl->chunk() : SNOW_E_ARG;
+}
+int snow_gpu_batch_set_implicit(snow_gpu_batch* batch, double beta, double tolerance, int max_iterations) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->set_implicit(beta, tolerance, max_iterations);
+  });
+}
+int snow_gpu_batch_implicit_stats(snow_gpu_batch* batch, int* iterations, double* residual) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    batch->impl->implicit_stats(iterations, residual);
+  });
 }
 int snow_gpu_batch_sort_mode(snow_gpu_batch* batch) {
   return batch && batch->impl ? (batch->impl->dense() ? 1 : 0) : SNOW_E_ARG;

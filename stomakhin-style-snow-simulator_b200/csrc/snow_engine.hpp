@@ -143,6 +143,28 @@ class Batch {
   bool dense() const { return dense_; }
   // Kernel launches in one replay of the captured step graph (0 before capture).
   int graph_kernels() const { return graph_kernels_; }
+  // Semi-implicit velocity update (snow_implicit.cu): beta = 0 is the explicit
+  // step; beta > 0 solves (I + beta dt^2 M^-1 H) v = v* by conjugate residuals
+  // to the relative `tolerance` or `max_iterations`.  Steps then run eagerly.
+  void set_implicit(double beta, double tolerance, int max_iterations) {
+    if (!(beta >= 0.0 && beta <= 1.0) || !(tolerance > 0.0) || max_iterations < 1)
+      throw Error(SNOW_E_ARG, "implicit update: beta in [0, 1], tolerance > 0, max_iterations >= 1");
+    imp_beta_ = beta;
+    imp_tol2_ = tolerance * tolerance;
+    imp_max_iter_ = max_iterations;
+    drop_graph();
+  }
+  void implicit_stats(int* iterations, double* residual) const {
+    if (iterations) *iterations = last_imp_iters_;
+    if (residual) *residual = last_imp_res_;
+  }
+  // Buffers of the solve for the current grid and particles, and the solve
+  // itself on the velocities in vel[0..2] (the grid update's output, or
+  // velocities loaded there); apply_only: vel[0..2] <- A vel[0..2] instead.
+  void ensure_implicit();
+  void free_implicit();
+  template <typename R>
+  void implicit_solve(const BatchDev& b, cudaStream_t s, bool apply_only = false);
   static constexpr int64_t kMaxDenseBins = int64_t(1) << 26;
   int64_t device_bytes() const;
   int precision() const { return prec_; }
@@ -249,6 +271,18 @@ class Batch {
   cudaStream_t own_stream_ = nullptr;
   uint32_t last_status_ = 0;
   int64_t last_blocks_ = 0;
+
+  // semi-implicit update
+  double imp_beta_ = 0.0, imp_tol2_ = 1e-12;
+  int imp_max_iter_ = 50;
+  void* imp_nodes_ = nullptr;   // R[16][imp_cap_nodes_]: mass, r, p, Ar, Ap, df
+  void* imp_parts_ = nullptr;   // R[17][imp_cap_p_]: polar factors and Lame parameters
+  double* imp_dots_ = nullptr;  // 4 dot-product accumulators, then the apply's item counter
+  double* imp_host_ = nullptr;  // page-locked copy of the accumulators
+  double imp_read_[4] = {0, 0, 0, 0};
+  int64_t imp_cap_nodes_ = 0, imp_cap_p_ = 0;
+  int last_imp_iters_ = 0;
+  double last_imp_res_ = 0.0;
 
  public:
   void ensure_grid_public(int64_t blocks) { ensure_grid(blocks); }

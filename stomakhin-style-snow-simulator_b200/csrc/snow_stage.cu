@@ -212,6 +212,50 @@ __global__ void k_force_scatter(const double* rec, int64_t n, const double* P, c
   for (int r = 0; r < 3; ++r) force[3 * t + r] = M[r][0] * g[0] + M[r][1] * g[1] + M[r][2] * g[2];
 }
 
+// dP[i] = the differential of the fixed-corotated stress at F_E of particle
+// i for dF[i] (corotated_differential; polar factors of F_E, hardening from
+// F_P), matrices column-major.
+__global__ void k_constitutive_differential(const double* rec, int64_t n, const double* dF, double mu0,
+                                            double lambda0, double xi, double* dP, uint32_t* bad) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* p = rec + 26 * i;
+  M3<double> F, FP, D;
+  for (int e = 0; e < 9; ++e) {
+    FP.a[e] = p[8 + e];
+    F.a[e] = p[17 + e];
+    D.a[e] = dF[9 * i + e];
+  }
+  M3<double> R;
+  Sym3<double> S;
+  if (!polar_factors(F, R, S)) {
+    atomicOr(bad, 1u);
+    return;
+  }
+  const double h = exp(xi * (1.0 - det3(FP)));
+  const M3<double> out = corotated_differential(F, R, S, mu0 * h, lambda0 * h, D);
+  for (int e = 0; e < 9; ++e) dP[9 * i + e] = out.a[e];
+}
+
+// dF[i] = dt (sum_e dv[i][e] grad[i][e]^T) F_E of particle i, over its 64
+// stencil entries (the implicit update's deformation differential).
+__global__ void k_deformation_differential(const double* rec, int64_t n, double dt, const double* grad,
+                                           const double* dv, double* dF) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // column-major sum of dv grad^T
+  for (int e = 0; e < 64; ++e) {
+    const double* g = grad + 192 * i + 3 * e;
+    const double* u = dv + 192 * i + 3 * e;
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r) G[c * 3 + r] += u[r] * g[c];
+  }
+  const double* F = rec + 26 * i + 17;
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r)
+      dF[9 * i + c * 3 + r] = dt * (G[r] * F[c * 3] + G[3 + r] * F[c * 3 + 1] + G[6 + r] * F[c * 3 + 2]);
+}
+
 // out[i][e] = (m w, m v w) for stencil weight w = weights[i][e] (grid.cpp:121-127).
 __global__ void k_p2g_stencil(const double* rec, int64_t n, const double* weights, double* out) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -350,6 +394,43 @@ int snow_gpu_stage_stress(const double* records, int64_t n, double mu_0, double 
     k_stress<<<blocks_for(n), 256>>>(d.p, n, mu_0, lambda_0, hardening_coefficient, dp.p);
     check_cuda(cudaGetLastError(), "stress");
     check_cuda(cudaMemcpy(P_out, dp.p, n * 72, cudaMemcpyDeviceToHost), "stress out");
+  });
+}
+
+int snow_gpu_stage_constitutive_differential(const double* records, int64_t n, const double* dF, double mu_0,
+                                             double lambda_0, double hardening_coefficient, double* dP) {
+  return guarded([&] {
+    check_records(records, n);
+    if (n > 0 && (!dF || !dP)) throw Error(SNOW_E_ARG, "NULL argument");
+    if (n == 0) return;
+    DBuf<double> d((size_t)n * 26), din((size_t)n * 9), dout((size_t)n * 9);
+    DBuf<uint32_t> bad(1);
+    check_cuda(cudaMemset(bad.p, 0, sizeof(uint32_t)), "flag");
+    check_cuda(cudaMemcpy(d.p, records, n * 208, cudaMemcpyHostToDevice), "records");
+    check_cuda(cudaMemcpy(din.p, dF, n * 72, cudaMemcpyHostToDevice), "dF");
+    k_constitutive_differential<<<blocks_for(n), 256>>>(d.p, n, din.p, mu_0, lambda_0, hardening_coefficient,
+                                                         dout.p, bad.p);
+    check_cuda(cudaGetLastError(), "constitutive differential");
+    uint32_t flag = 0;
+    check_cuda(cudaMemcpy(&flag, bad.p, sizeof flag, cudaMemcpyDeviceToHost), "flag");
+    if (flag) throw Error(SNOW_E_ARG, "constitutive_differential: a singular F_E");
+    check_cuda(cudaMemcpy(dP, dout.p, n * 72, cudaMemcpyDeviceToHost), "dP");
+  });
+}
+
+int snow_gpu_stage_deformation_differential(const double* records, int64_t n, double time_step,
+                                            const double* gradients, const double* delta_v, double* dF) {
+  return guarded([&] {
+    check_records(records, n);
+    if (n > 0 && (!gradients || !delta_v || !dF)) throw Error(SNOW_E_ARG, "NULL argument");
+    if (n == 0) return;
+    DBuf<double> d((size_t)n * 26), dg((size_t)n * 192), du((size_t)n * 192), dout((size_t)n * 9);
+    check_cuda(cudaMemcpy(d.p, records, n * 208, cudaMemcpyHostToDevice), "records");
+    check_cuda(cudaMemcpy(dg.p, gradients, n * 192 * 8, cudaMemcpyHostToDevice), "gradients");
+    check_cuda(cudaMemcpy(du.p, delta_v, n * 192 * 8, cudaMemcpyHostToDevice), "delta_v");
+    k_deformation_differential<<<blocks_for(n), 256>>>(d.p, n, time_step, dg.p, du.p, dout.p);
+    check_cuda(cudaGetLastError(), "deformation differential");
+    check_cuda(cudaMemcpy(dF, dout.p, n * 72, cudaMemcpyDeviceToHost), "dF");
   });
 }
 

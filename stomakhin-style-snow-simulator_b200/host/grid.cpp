@@ -259,6 +259,139 @@ void G2P(const Grid& grid, Particle& particle, double grid_spacing, double alpha
                              alpha));
 }
 
+// ---------------------------------------------------------- implicit update
+// The functions the reference declares for Stomakhin et al.'s semi-implicit
+// update (include/snow/grid.hpp:76,80,88-92) and defines nowhere: the
+// per-particle work runs in the GPU stage entry points, the bookkeeping of the
+// host Grid here.
+
+Eigen::Matrix3d constitutive_differential(const Particle& particle, const Eigen::Matrix3d& delta_f, double mu_0,
+                                          double lambda_0, double hardening_coefficient)
+{
+    Eigen::Matrix3d dP;
+    check(snow_gpu_stage_constitutive_differential(record(particle), 1, delta_f.data(), mu_0, lambda_0,
+                                                   hardening_coefficient, dP.data()));
+    return dP;
+}
+
+// The nodes with mass: the unknowns of the implicit solve.
+std::vector<GridNode*> index_nodes(Grid& grid)
+{
+    std::vector<GridNode*> out;
+    for (auto& [index, node] : grid)
+        if (node.mass > 0) out.push_back(&node);
+    return out;
+}
+
+// dt (sum_i delta_v_i grad w_i^T) F_E over the particle's stencil.
+Eigen::Matrix3d deformation_differential(const Grid& grid, const Particle& particle, double grid_spacing,
+                                         double time_step)
+{
+    const ParticleStencil st = build_stencil(particle, grid_spacing);
+    double grad[64 * 3], dv[64 * 3];
+    for (int e = 0; e < 64; ++e)
+    {
+        const auto it = grid.find(st[e].index);
+        for (int a = 0; a < 3; ++a)
+        {
+            grad[3 * e + a] = st[e].gradient[a];
+            dv[3 * e + a] = it == grid.end() ? 0.0 : it->second.delta_v[a];
+        }
+    }
+    Eigen::Matrix3d dF;
+    check(snow_gpu_stage_deformation_differential(record(particle), 1, time_step, grad, dv, dF.data()));
+    return dF;
+}
+
+// delta_force += -V_p0 dP F_E^T grad w at the particle's stencil nodes, dP the
+// constitutive differential of the deformation differential.
+void force_differential(Grid& grid, const Particle& particle, double grid_spacing, double time_step, double mu_0,
+                        double lambda_0, double hardening_coefficient)
+{
+    const Eigen::Matrix3d dP = constitutive_differential(
+        particle, deformation_differential(grid, particle, grid_spacing, time_step), mu_0, lambda_0,
+        hardening_coefficient);
+    const ParticleStencil st = build_stencil(particle, grid_spacing);
+    double grad[64 * 3], force[64 * 3];
+    for (int e = 0; e < 64; ++e)
+        for (int a = 0; a < 3; ++a) grad[3 * e + a] = st[e].gradient[a];
+    check(snow_gpu_stage_force_scatter(record(particle), 1, dP.data(), grad, force));
+    for (int e = 0; e < 64; ++e)
+    {
+        GridNode& node = grid[st[e].index];
+        for (int a = 0; a < 3; ++a) node.delta_force[a] += force[3 * e + a];
+    }
+}
+
+namespace
+{
+// The grid as a node list with each node's position in `krylov` (or -1).
+NodeList krylov_list(const Grid& grid, const std::vector<GridNode*>& krylov, std::vector<int64_t>& slot)
+{
+    std::unordered_map<const GridNode*, int64_t> pos;
+    for (std::size_t i = 0; i < krylov.size(); ++i) pos[krylov[i]] = static_cast<int64_t>(i);
+    NodeList nodes = to_nodes(grid);
+    slot.clear();
+    for (const auto& [index, node] : grid)
+    {
+        const auto it = pos.find(&node);
+        slot.push_back(it == pos.end() ? -1 : it->second);
+    }
+    return nodes;
+}
+
+std::vector<double> particle_records(const std::vector<Particle>& snow)
+{
+    std::vector<double> rec(snow.size() * SNOW_RECORD_DOUBLES);
+    if (!snow.empty()) std::memcpy(rec.data(), snow.data(), rec.size() * sizeof(double));
+    return rec;
+}
+}  // namespace
+
+// (A q)_i = q_i - beta dt delta f_i(q) / m_i over the Krylov nodes (the grid's
+// nodes with mass, as index_nodes gives them; other nodes take q = 0).
+KrylovVector apply_A(Grid& grid, const std::vector<Particle>& snow, const std::vector<GridNode*>& krylov_nodes,
+                     const KrylovVector& q, double grid_spacing, double time_step, double mu_0, double lambda_0,
+                     double hardening_coefficent, double beta)
+{
+    if (q.size() != krylov_nodes.size()) throw std::invalid_argument("apply_A: q and krylov_nodes differ in size");
+    std::vector<int64_t> slot;
+    const NodeList nodes = krylov_list(grid, krylov_nodes, slot);
+    std::vector<double> qq(static_cast<std::size_t>(nodes.size()) * 3, 0.0), out(qq.size());
+    for (int64_t r = 0; r < nodes.size(); ++r)
+        if (slot[r] >= 0)
+            for (int a = 0; a < 3; ++a) qq[3 * r + a] = q[slot[r]][a];
+    const std::vector<double> rec = particle_records(snow);
+    check(snow_gpu_stage_implicit(nodes.ijk.data(), nodes.f.data(), nodes.size(), rec.data(),
+                                  static_cast<int64_t>(snow.size()), grid_spacing, time_step, mu_0, lambda_0,
+                                  hardening_coefficent, beta, 1e-24, 1, qq.data(), out.data(), nullptr));
+    KrylovVector aq(krylov_nodes.size(), Eigen::Vector3d::Zero());
+    for (int64_t r = 0; r < nodes.size(); ++r)
+        if (slot[r] >= 0) aq[slot[r]] = Eigen::Vector3d(out[3 * r], out[3 * r + 1], out[3 * r + 2]);
+    return aq;
+}
+
+// Solves A v = velocity over the Krylov nodes, from v = velocity, until
+// <r, r>_M <= squared_tolerance <velocity, velocity>_M (mass-weighted) or
+// maximum_iterations, and writes the velocities back.
+void Conjugate_residual(Grid& grid, const std::vector<Particle>& snow, const std::vector<GridNode*>& krylov_nodes,
+                        double grid_spacing, double time_step, double mu_0, double lambda_0,
+                        double hardening_coefficent, double beta, double squared_tolerance, int maximum_iterations)
+{
+    std::vector<int64_t> slot;
+    const NodeList nodes = krylov_list(grid, krylov_nodes, slot);
+    std::vector<double> out(static_cast<std::size_t>(nodes.size()) * 3);
+    const std::vector<double> rec = particle_records(snow);
+    int iterations = 0;
+    check(snow_gpu_stage_implicit(nodes.ijk.data(), nodes.f.data(), nodes.size(), rec.data(),
+                                  static_cast<int64_t>(snow.size()), grid_spacing, time_step, mu_0, lambda_0,
+                                  hardening_coefficent, beta, squared_tolerance, maximum_iterations, nullptr,
+                                  out.data(), &iterations));
+    for (int64_t r = 0; r < nodes.size(); ++r)
+        if (slot[r] >= 0)
+            for (int a = 0; a < 3; ++a) krylov_nodes[slot[r]]->velocity[a] = out[3 * r + a];
+}
+
 void particle_collisions(Particle& particle, const std::vector<CollisionBody>& colliders)
 {
     const auto cols = to_colliders(colliders);

@@ -143,6 +143,12 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_batch_graph_kernels": (ctypes.c_int, [vp]),
         "snow_gpu_batch_sort_mode": (ctypes.c_int, [vp]),
         "snow_gpu_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, _dp, _dp, vp]),
+        "snow_gpu_batch_set_implicit": (ctypes.c_int, [vp, d, d, ctypes.c_int]),
+        "snow_gpu_batch_implicit_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), _dp]),
+        "snow_gpu_stage_constitutive_differential": (ctypes.c_int, [_dp, i64, _dp, d, d, d, _dp]),
+        "snow_gpu_stage_deformation_differential": (ctypes.c_int, [_dp, i64, d, _dp, _dp, _dp]),
+        "snow_gpu_stage_implicit": (ctypes.c_int, [_ip, _dp, i64, _dp, i64, d, d, d, d, d, d, d, ctypes.c_int,
+                                                   _dp, _dp, ctypes.POINTER(ctypes.c_int)]),
         "snow_gpu_batch_snapshot": (ctypes.c_int, [vp, ctypes.c_int32, vp]),
         "snow_gpu_batch_restore": (ctypes.c_int, [vp, ctypes.c_int32, vp]),
         "snow_gpu_setup": (ctypes.c_int, [_dp, i64, d]),
@@ -374,6 +380,16 @@ class Batch:
                                              ctypes.c_void_p(stream)))
         return c.value, ms.value
 
+    def set_implicit(self, beta: float, tolerance: float = 1e-10, max_iterations: int = 100) -> None:
+        """Semi-implicit velocity update (beta = 0: the explicit step)."""
+        _check(lib().snow_gpu_batch_set_implicit(self._h, float(beta), float(tolerance), int(max_iterations)))
+
+    def implicit_stats(self) -> tuple[int, float]:
+        """(iterations, relative residual) of the last step's implicit solve."""
+        it, res = ctypes.c_int(), ctypes.c_double()
+        _check(lib().snow_gpu_batch_implicit_stats(self._h, ctypes.byref(it), ctypes.byref(res)))
+        return it.value, res.value
+
     @property
     def fp64_projections(self) -> int:
         """Mixed form: projections redone in double during the last step."""
@@ -497,6 +513,33 @@ def stage_particle_collisions(records, planes) -> np.ndarray:
     col = colliders(planes)
     _check(lib().snow_gpu_stage_particle_collisions(_ptr(rec), rec.shape[0], col, len(planes)))
     return rec
+
+
+def stage_constitutive_differential(records, dF, mu0, lambda0, xi) -> np.ndarray:
+    """dP[n][3][3] for dF[n][3][3] (row-major numpy matrices)."""
+    rec = _records(records)
+    dfc = np.ascontiguousarray(np.transpose(np.asarray(dF, dtype=np.float64), (0, 2, 1)).reshape(-1, 9))
+    out = np.zeros_like(dfc)
+    _check(lib().snow_gpu_stage_constitutive_differential(_ptr(rec), rec.shape[0], _ptr(dfc), float(mu0),
+                                                          float(lambda0), float(xi), _ptr(out)))
+    return np.transpose(out.reshape(-1, 3, 3), (0, 2, 1))
+
+
+def stage_implicit(ijk, fields, records, dx, dt, mu0, lambda0, xi, beta, q=None, squared_tolerance=1e-24,
+                   max_iterations=300):
+    """A q (q given) or the conjugate-residual solution (q None) on a node list;
+    returns (n_nodes x 3 values, iterations)."""
+    ijk = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
+    f = np.ascontiguousarray(fields, dtype=np.float64).reshape(-1, 10)
+    rec = _records(records)
+    qq = None if q is None else np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((ijk.shape[0], 3))
+    it = ctypes.c_int()
+    _check(lib().snow_gpu_stage_implicit(_ptr(ijk, _ip), _ptr(f), ijk.shape[0], _ptr(rec), rec.shape[0], float(dx),
+                                         float(dt), float(mu0), float(lambda0), float(xi), float(beta),
+                                         float(squared_tolerance), int(max_iterations),
+                                         None if qq is None else _ptr(qq), _ptr(out), ctypes.byref(it)))
+    return out, it.value
 
 
 def stage_position_update(records, dt) -> np.ndarray:

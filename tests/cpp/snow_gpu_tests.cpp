@@ -3,6 +3,7 @@
 // call below runs on the device.  Plus API behaviour the reference relies on:
 // setup()+step() conservation, residency, CSV import errors and frame export.
 // Exit status 0 = all pass.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <filesystem>
@@ -357,6 +358,42 @@ int main()
              };
              expect(slurp("frame_000007.csv") == "x,y,z\n-0.1,-0.05,1\n0.2,-0.4,0.3\n", "export axes and format");
              expect(slurp("frame_000008.csv") == slurp("frame_000007.csv"), "asynchronous export writes the same file");
+         }},
+        {"implicit update: Conjugate_residual solves what apply_A applies", [] {
+             const double dx = 0.1, dt = 1e-3, mu = 1e4, lambda = 1.5e4, xi = 10;
+             std::vector<Particle> snow;
+             for (int i = 0; i < 4; ++i)
+             {
+                 Particle p({1.0 + 0.031 * i, 1.2 - 0.017 * i, 0.9 + 0.023 * i}, {0.3 * i, -0.2, 0.1}, 1.0, 1e-3);
+                 p.F_E = diag(1.02, 0.97, 1.01);
+                 p.F_E(0, 1) = 0.01 * i;
+                 p.F_P = diag(1.0, 1.0, 0.999);
+                 snow.push_back(p);
+             }
+             Grid g;
+             for (const Particle& p : snow) P2G(g, p, dx);
+             for (auto& [i, n] : g) n.velocity = n.momentum / n.mass;
+             const std::vector<GridNode*> nodes = index_nodes(g);
+             expect(nodes.size() == g.size(), "every node of a particle stencil has mass");
+             KrylovVector want(nodes.size());
+             for (std::size_t k = 0; k < nodes.size(); ++k) want[k] = nodes[k]->velocity;
+             Conjugate_residual(g, snow, nodes, dx, dt, mu, lambda, xi, 1.0, 1e-28, 400);
+             KrylovVector v(nodes.size());
+             double moved = 0;
+             for (std::size_t k = 0; k < nodes.size(); ++k)
+                 v[k] = nodes[k]->velocity, moved = std::max(moved, dist(v[k], want[k]));
+             expect(moved > 1e-9, "the implicit term changes the velocities");
+             const KrylovVector av = apply_A(g, snow, nodes, v, dx, dt, mu, lambda, xi, 1.0);
+             double err = 0;
+             for (std::size_t k = 0; k < nodes.size(); ++k) err = std::max(err, dist(av[k], want[k]));
+             expect(err < 1e-10, "A v = v* (" + std::to_string(err) + ")");
+             for (std::size_t k = 0; k < nodes.size(); ++k) nodes[k]->velocity = want[k];
+             Conjugate_residual(g, snow, nodes, dx, dt, mu, lambda, xi, 0.0, 1e-28, 400);
+             double still = 0;
+             for (std::size_t k = 0; k < nodes.size(); ++k) still = std::max(still, dist(nodes[k]->velocity, want[k]));
+             expect(still == 0, "beta 0 keeps v*");
+             const Eigen::Matrix3d dP = constitutive_differential(snow[1], Eigen::Matrix3d::Zero(), mu, lambda, xi);
+             expect(dP.norm() == 0, "zero dF gives zero dP");
          }},
     };
     int n = 0;

@@ -27,6 +27,8 @@ REFERENCE_API = [
     "force_grid_accumulation(", "force_calculation(", "grid_velocity(", "grid_collisions(", "stress_update(",
     "G2P(", "particle_collisions(", "import_particles(", "import_groups(", "import_particle_seeds(",
     "assemble_particles(", "export_particles(", "step(std::vector<Particle",
+    "constitutive_differential(", "index_nodes(", "deformation_differential(", "force_differential(",
+    "apply_A(", "Conjugate_residual(",
 ]
 
 
