@@ -219,10 +219,12 @@ def alg_bytes(n_p: int, nodes: int, real: int) -> dict:
         particle and writes the 7 accumulated channels of every grid node;
     g2p reads x, v, m, V_p0, F_E (17 `real`), F_P (9 doubles) and the particle id
         per particle and the 6 velocity channels per node, and writes the new
-        state: x, v, m, V_p0, F_E, the next force matrix (23 `real`), F_P and the id.
+        state: x, v, m, V_p0, F_E, the next force matrix (23 `real`), F_P and the id,
+        and the next step's sort key and position (8 B; in the steady state G2P
+        emits them and the keys kernel reads nothing).
     """
     return {"p2g": n_p * 13 * real + nodes * 7 * real,
-            "g2p": n_p * (17 * real + 72 + 4) + nodes * 6 * real + n_p * (23 * real + 72 + 4)}
+            "g2p": n_p * (17 * real + 72 + 4) + nodes * 6 * real + n_p * (23 * real + 72 + 4 + 8)}
 
 
 def errors(a, b) -> dict:
