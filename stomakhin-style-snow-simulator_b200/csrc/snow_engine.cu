@@ -288,6 +288,7 @@ void Batch::ensure_bins(int64_t bins) {
   bin_state_ = dalloc<unsigned long long>((size_t)(bins / kBinTile + 1));
   cap_bins_ = bins;
   bins_dirty_ = true;
+  boxes_dirty_ = true;  // the next step's counts G2P emitted into the old bins are gone
 }
 
 // Chooses the sort for the coming steps: dense bins with 2x headroom over
@@ -295,7 +296,9 @@ void Batch::ensure_bins(int64_t bins) {
 // Clears the counts if a step may have left some behind.
 void Batch::size_dense(int64_t key_blocks, cudaStream_t s) {
   const int64_t need = 2 * key_blocks * 64 + 16 * kBinTile;
+  const bool was = dense_;
   dense_ = want_dense_ && need <= kMaxDenseBins;
+  if (dense_ != was) boxes_dirty_ = true;  // keys G2P emitted for the other sort are not used
   if (!dense_) return;
   ensure_bins(need);
   if (bins_dirty_) {
@@ -529,6 +532,9 @@ void Batch::reserve(int64_t particles, int64_t staging, int scenes, int collider
 void Batch::ensure_particle_buffers(int64_t total) {
   if (total <= cap_p_) return;
   free_particle_buffers();
+  // The next step's keys G2P emitted lived in the old buffers: the next step
+  // measures the boxes and computes every key again.
+  boxes_dirty_ = true;
   const int64_t cap = std::max<int64_t>(total, 1024);
   for (int k = 0; k < 2; ++k) {
     keys_[k] = dalloc<uint32_t>((size_t)cap);

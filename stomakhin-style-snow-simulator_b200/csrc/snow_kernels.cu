@@ -205,12 +205,20 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
   if (kSwap)
     for (int s = threadIdx.x; s < b.num_scenes; s += blockDim.x) b.scenes[s].cur ^= 1;
   if (threadIdx.x == 0) {
-    const bool armed = b.ctr->emit_ok != 0;  // the last G2P may have written keys and counts
+    const bool armed = b.ctr->emit_ok != 0;  // the G2P that just ran may have written keys and counts
     const bool tried = kSwap && b.dense && armed;
     s_emitted = tried && !b.ctr->emit_fail;
-    const bool leftovers = kSwap ? tried && b.ctr->emit_fail : armed;
-    const unsigned long long eb = b.ctr->emit_blocks;
-    s_cleanup = leftovers && b.bins && b.occ && eb * 64 <= (unsigned long long)b.cap_bins ? (int)eb : 0;
+    // Block keys whose counts were written and will not be consumed: those of
+    // a G2P that gave up part way (its emission boxes), or, on a fresh start,
+    // those a finished step left for the next one (the current key boxes,
+    // which are then the emission boxes that G2P wrote against).
+    unsigned long long eb = 0;
+    if (kSwap) {
+      if (tried && b.ctr->emit_fail) eb = b.ctr->emit_blocks;
+    } else if (b.ctr->keys_ready) {
+      eb = b.ctr->key_blocks;
+    }
+    s_cleanup = eb && b.bins && b.occ && eb * 64 <= (unsigned long long)b.cap_bins ? (int)eb : 0;
   }
   __syncthreads();
   const bool emitted = s_emitted != 0;
@@ -218,7 +226,7 @@ __global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
     // Counts and occupancy G2P wrote that no step will consume: G2P gave up
     // part way (a particle left its emission box, which a particle moving less
     // than a block per step never does), or this is a fresh start (after an
-    // upload, setup or a change of scenes) and the keys kernel sorts.
+    // upload, setup, a change of scenes or of buffers) and the keys kernel sorts.
     uint4* bins4 = reinterpret_cast<uint4*>(b.bins);
     for (int64_t k = threadIdx.x; k < (int64_t)s_cleanup * 16; k += blockDim.x) bins4[k] = make_uint4(0, 0, 0, 0);
     for (int64_t k = threadIdx.x; k < (int64_t)s_cleanup; k += blockDim.x) b.occ[k] = 0;
@@ -1828,7 +1836,8 @@ int persistent_grid(K kernel, int threads, size_t smem) {
 
 template <typename K>
 void set_smem(K kernel, size_t smem) {
-  if (smem > 48 * 1024)
+  // always: without it static + dynamic shared memory is held to 48 KB
+  if (smem > 0)
     check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                "shared memory size");
 }

@@ -158,3 +158,29 @@ def test_snapshot_and_restore(snow):
         finally:
             b2.close()
     assert other >= 0
+
+
+def test_fresh_start_after_emitted_keys(snow, oracle):
+    """G2P writes the next step's sort keys and counts as it goes; a change of
+    scenes between two steps makes the next step sort afresh and must clear
+    every count the finished step left behind, also when the scene's block box
+    shrank in between (a fast-moving scene loses a block column at one end
+    while it gains one at the other).  A tiny scene added and removed after
+    every step forces the fresh start; the result equals the oracle's."""
+    from snow_b200 import scenes
+
+    sc = scenes.cube_scene(10)
+    rec = oracle.setup(sc.particles, sc.dx)
+    rec[:, 3] = -300.0  # 3 cm per step: a block column every few steps
+    want, _ = oracle.step(rec, sc.params(), sc.plane_array(), 12)
+    tiny = scenes.cube_scene(2)
+    b = snow.Batch(snow.SNOW_FP64)
+    sid = b.add_scene(rec, sc.params(), sc.planes)
+    for _ in range(12):
+        b.step(1)
+        t = b.add_scene(tiny.particles, tiny.params(), tiny.planes)
+        b.remove_scene(t)
+    got = b.download(sid)
+    b.close()
+    e = errors(got, want)
+    assert max(e.values()) < 1e-10, e

@@ -164,3 +164,42 @@ def test_requests_submitted_while_running(snow, prec, tol):
         e = errors(got, _alone(snow, prec, sc, steps))
         assert max(e.values()) < tol, (sc.name, e)
     srv.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 1e-5)])
+def test_reservation_grows_under_a_live_scene(snow, prec, tol):
+    """A long-running scene is live (its steps write the next step's sort keys
+    as they go) when a much larger request arrives: the server grows the live
+    batch's particle and sort buffers between two ticks, and the next tick must
+    sort afresh instead of reading keys from the replaced buffers.  Both results
+    equal their scenes alone."""
+    import threading
+    import time
+
+    from snow_b200 import scenes
+
+    (long_sc, _, _), = scenes.served_requests(count=1, rate=2000.0, lo=1500, hi=2500, seed=41)
+    (big_sc, _, _), = scenes.served_requests(count=1, rate=2000.0, lo=40000, hi=60000, seed=42)
+    srv = snow.Server(prec, max_steps_per_tick=4)
+    srv.set_streaming(True)
+    ids = [(srv.submit(long_sc, 400, 0.0), long_sc, 400)]
+    failure = []
+
+    def serve():
+        try:
+            srv.run()
+        except Exception as e:  # reported by the main thread
+            failure.append(e)
+
+    th = threading.Thread(target=serve)
+    th.start()
+    time.sleep(0.02)
+    ids.append((srv.submit(big_sc, 20), big_sc, 20))
+    srv.end_of_stream()
+    th.join(timeout=120)
+    assert not th.is_alive() and not failure, failure
+    assert srv.stats()["reservations"] >= 2
+    for rid, sc, steps in ids:
+        got, _ = srv.result(rid)
+        e = errors(got, _alone(snow, prec, sc, steps))
+        assert max(e.values()) < tol, (sc.name, e)
