@@ -302,8 +302,24 @@ def serve_stream(snow_b200, sp, reqs, precision, streaming: bool = True) -> dict
         if failure:
             raise failure[0]
     st = srv.stats()
+    st.update(tick_summary(srv.ticks(), st["wall_s"]))
     srv.close()
     return st
+
+
+def tick_summary(ticks, wall_s: float) -> dict:
+    """Where a served run's time went, from its per-tick trace: the device's
+    busy share of the wall time, the mean steps and device milliseconds per
+    tick, and the mean device gap between two ticks (admission, retirement and
+    the host's launch of the next tick)."""
+    if not ticks:
+        return {}
+    busy = sum(t["device_end_s"] - t["device_start_s"] for t in ticks)
+    gaps = [b["device_start_s"] - a["device_end_s"] for a, b in zip(ticks, ticks[1:])]
+    return {"device_busy_frac": busy / wall_s if wall_s > 0 else None,
+            "mean_steps_per_tick": sum(t["steps"] for t in ticks) / len(ticks),
+            "mean_tick_device_ms": 1e3 * busy / len(ticks),
+            "mean_gap_ms": 1e3 * sum(gaps) / len(gaps) if gaps else 0.0}
 
 
 def measure_served(snow_b200, torch, sp, count: int, fp64_rate: float | None = None, grounded: bool = False,
@@ -332,6 +348,8 @@ def measure_served(snow_b200, torch, sp, count: int, fp64_rate: float | None = N
            "particle_steps_per_s": med["particle_steps_per_s"], "completed": med["completed"],
            "rejected": med["rejected"], "peak_concurrent_scenes": med["peak_scenes"], "ticks": med["ticks"],
            "reservations": med["reservations"], "wall_s": med["wall_s"],
+           "ticks_summary": {k: med.get(k) for k in ("device_busy_frac", "mean_steps_per_tick",
+                                                     "mean_tick_device_ms", "mean_gap_ms")},
            "host_phases_s": {"admit": med["admit_s"], "step": med["step_s"], "retire": med["retire_s"]}}
     if fp64_rate:
         out["served_vs_plain_fp64_headline"] = med["particle_steps_per_s"] / fp64_rate
@@ -693,7 +711,8 @@ def kernel_roofline(kernel: str, ms: float, alg_bytes: float, n_particles: int, 
             tf = per * n_particles / (ms * 1e-3) / 1e12
             roofs[pipe] = {"achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
                            "peak_source": "measured (snow_gpu_measure_fma_peak)",
-                           "flops_per_launch": per * n_particles}
+                           "flops_per_launch": per * n_particles,
+                           "pipe_active_pct_ncu": fl.get(f"{'fp64' if pipe == 'fp64' else 'fma'}_pipe_active_pct")}
     bound = max(roofs, key=lambda k: roofs[k]["frac"])
     return {"kernel": kernel, "launch_ms": ms, "alg_bytes_per_launch": alg_bytes, "bound": bound,
             "frac": roofs[bound]["frac"], "roofs": roofs,
@@ -1000,8 +1019,9 @@ def run_served(args, ws, rank, local):
             "config": {"workload": f"served-{len(reqs)}-requests", "precision": "mixed",
                        "parallelism": f"request shards x{ws}" if ws > 1 else "single GPU",
                        "submission": "streaming"},
-            "rank0": {k: st[k] for k in ("p50_s", "p99_s", "mean_s", "completed", "ticks", "peak_scenes",
-                                          "reservations", "particle_steps_per_s")},
+            "rank0": {k: st.get(k) for k in ("p50_s", "p99_s", "mean_s", "completed", "ticks", "peak_scenes",
+                                              "reservations", "particle_steps_per_s", "device_busy_frac",
+                                              "mean_steps_per_tick", "mean_tick_device_ms", "mean_gap_ms")},
             "clocks": clk}
     if dist is not None:
         dist.barrier()
