@@ -139,6 +139,11 @@ int snow_gpu_batch_upload(snow_gpu_batch* batch, int32_t scene_id, const double*
 /* Copies a scene's particles back in their original order. */
 int snow_gpu_batch_download(snow_gpu_batch* batch, int32_t scene_id, double* records, int64_t n,
                             void* stream);
+/* Copies only a scene's particle positions back, x y z per particle in their
+ * original order (n x 3 doubles): what a frame export (export_particles,
+ * src/export.cpp:10-22) reads, an eighth of the records' bytes. */
+int snow_gpu_batch_download_positions(snow_gpu_batch* batch, int32_t scene_id, double* xyz, int64_t n,
+                                      void* stream);
 /* A device copy of a scene's particle state (one per scene, replaced by the
  * next call), and putting it back so the scene continues from there: for
  * pre-empting or retrying served work.  No reference counterpart (the

@@ -108,6 +108,15 @@ __global__ void k_planes_to_records(double* rec, int64_t n, const R* r, const do
   for (int k = 0; k < 9; ++k) p[17 + k] = (double)r[(PFE + k) * st + i];
 }
 
+template <typename R>
+__global__ void k_planes_to_positions(double* xyz, int64_t n, const R* r, const int32_t* id, int64_t st) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* p = xyz + 3 * (int64_t)id[i];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) p[a] = (double)r[(PX + a) * st + i];
+}
+
 int64_t pad32(int64_t n) { return (n + 31) / 32 * 32; }
 
 // True for host memory that is page-locked (registered or cudaHostAlloc'd).
@@ -472,6 +481,23 @@ void Batch::download(int32_t id, double* records, int64_t n, cudaStream_t s, boo
   copy_out(records, staging_, (size_t)n * 26 * sizeof(double), s, wait);
 }
 
+void Batch::download_positions(int32_t id, double* xyz, int64_t n, cudaStream_t s) {
+  step_complete();
+  Scene* sc = find(id);
+  if (n != sc->n) throw Error(SNOW_E_ARG, "download_positions: particle count differs from the scene's");
+  if (n == 0) return;
+  ensure_staging(n);
+  const unsigned g = (unsigned)((n + 255) / 256);
+  if (prec_ == SNOW_FP64)
+    k_planes_to_positions<double><<<g, 256, 0, s>>>(staging_, n, (const double*)sc->r[sc->cur], sc->id[sc->cur],
+                                                     sc->stride);
+  else
+    k_planes_to_positions<float><<<g, 256, 0, s>>>(staging_, n, (const float*)sc->r[sc->cur], sc->id[sc->cur],
+                                                    sc->stride);
+  check_cuda(cudaGetLastError(), "download kernel");
+  copy_out(xyz, staging_, (size_t)n * 3 * sizeof(double), s, true);
+}
+
 SceneDev Batch::scene_dev(const Scene& sc, int64_t begin) const {
   SceneDev d{};
   for (int k = 0; k < 2; ++k) {
@@ -786,11 +812,14 @@ void Batch::step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s)
     for (auto& e : ev) cudaEventDestroy(e);
   } else if (use_graphs_ && imp_beta_ == 0.0) {  // the implicit solve reads back scalars: no graph
     int k = 0;
-    if (!gexec_) {
-      // first step eagerly (initialises per-kernel launch settings), then capture
+    if (!gexec_ && !graph_warm_) {
+      // the batch's first step eagerly (initialises per-kernel launch
+      // settings); every later call captures or replays, also one step at a
+      // time as the drop-in step() calls it
       one(nullptr);
       check_cuda(cudaGetLastError(), "step launch");
       ++k;
+      graph_warm_ = true;
     }
     if (k < n_steps && (!gexec_ || std::memcmp(&graph_args_, &b, sizeof b) != 0)) {
       cudaGraph_t g;
@@ -1179,6 +1208,14 @@ int snow_gpu_batch_download(snow_gpu_batch* batch, int32_t scene_id, double* rec
   return guarded([&] {
     SNOW_BATCH_OR_FAIL;
     batch->impl->download(scene_id, records, n, as_stream(stream));
+  });
+}
+int snow_gpu_batch_download_positions(snow_gpu_batch* batch, int32_t scene_id, double* xyz, int64_t n,
+                                      void* stream) {
+  return guarded([&] {
+    SNOW_BATCH_OR_FAIL;
+    if (n > 0 && !xyz) throw Error(SNOW_E_ARG, "NULL position buffer");
+    batch->impl->download_positions(scene_id, xyz, n, as_stream(stream));
   });
 }
 int snow_gpu_batch_snapshot(snow_gpu_batch* batch, int32_t scene_id, void* stream) {

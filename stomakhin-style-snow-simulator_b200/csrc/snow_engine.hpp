@@ -71,6 +71,7 @@ class Batch {
   void set_params(int32_t id, const snow_step_params* params, const snow_collider* c, int n);
   void upload(int32_t id, const double* records, int64_t n, cudaStream_t s, bool wait = true);
   void download(int32_t id, double* records, int64_t n, cudaStream_t s, bool wait = true);
+  void download_positions(int32_t id, double* xyz, int64_t n, cudaStream_t s);
   // box_blocks >= 0: an upper bound on the scene's block box at dx (in 4^3
   // blocks, halo included) known to the caller, which sizes the grid without
   // reading the box back.  wait = false: the setup is left in flight on s and
@@ -265,6 +266,7 @@ class Batch {
   int64_t cached_bytes_ = 0;
 
   cudaGraphExec_t gexec_ = nullptr;
+  bool graph_warm_ = false;  // a step ran eagerly: later steps may be captured
   BatchDev graph_args_{};
   std::vector<SceneDev> table_;
   std::vector<Collider> coll_;

@@ -4,12 +4,14 @@
 // one piece and converts numbers with std::from_chars where the text is a
 // plain decimal (falling back to std::stoi/std::stod, the reference's
 // conversions, for anything else), instead of a stringstream per field.
+#include <algorithm>
 #include <charconv>
 #include <cstdint>
 #include <cstring>
 #include <fstream>
 #include <iomanip>
 #include <iterator>
+#include <memory>
 #include <mutex>
 #include <sstream>
 #include <stdexcept>
@@ -177,21 +179,13 @@ char* put_number(char* at, double v)
     return std::to_chars(at, at + 32, v, std::chars_format::general, 6).ptr;
 }
 
-// output/frame_<frame>.csv with header "x,y,z" and rows (x, -z, y), default
-// stream formatting (export.cpp:10-22), formatted into one buffer and written
-// in one piece.
-void write_frame(const double* rec, std::size_t n, int frame_no)
+// Rows [lo, hi) of a frame: "x,-z,y\n" per particle; `stride` doubles from one
+// particle's x to the next one's (26 for records, 3 for positions).
+char* put_rows(char* at, const double* xyz, std::size_t stride, std::size_t lo, std::size_t hi)
 {
-    std::ostringstream name;
-    name << "output/frame_" << std::setw(6) << std::setfill('0') << frame_no << ".csv";
-    std::ofstream file{name.str(), std::ios::binary};
-    std::string out(6 + n * 3 * 32, '\0');
-    char* at = out.data();
-    std::memcpy(at, "x,y,z\n", 6);
-    at += 6;
-    for (std::size_t i = 0; i < n; ++i)
+    for (std::size_t i = lo; i < hi; ++i)
     {
-        const double* p = rec + SNOW_RECORD_DOUBLES * i;
+        const double* p = xyz + stride * i;
         at = put_number(at, p[0]);
         *at++ = ',';
         at = put_number(at, p[2] * -1);
@@ -199,7 +193,33 @@ void write_frame(const double* rec, std::size_t n, int frame_no)
         at = put_number(at, p[1]);
         *at++ = '\n';
     }
-    file.write(out.data(), at - out.data());
+    return at;
+}
+
+// output/frame_<frame>.csv with header "x,y,z" and rows (x, -z, y), default
+// stream formatting (export.cpp:10-22).  Large frames are formatted by several
+// threads, each into its own buffer, and written in order in one pass.
+void write_frame(const double* xyz, std::size_t stride, std::size_t n, int frame_no)
+{
+    std::ostringstream name;
+    name << "output/frame_" << std::setw(6) << std::setfill('0') << frame_no << ".csv";
+    std::ofstream file{name.str(), std::ios::binary};
+    constexpr std::size_t kRowBytes = 3 * 32, kRowsPerThread = 16384;
+    const std::size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const std::size_t parts = std::max<std::size_t>(1, std::min<std::size_t>({hw, 32, n / kRowsPerThread}));
+    std::vector<std::string> out(parts);
+    std::vector<std::size_t> used(parts, 0);
+    auto work = [&](std::size_t k) {
+        const std::size_t lo = n * k / parts, hi = n * (k + 1) / parts;
+        out[k].resize((hi - lo) * kRowBytes);
+        used[k] = put_rows(out[k].data(), xyz, stride, lo, hi) - out[k].data();
+    };
+    std::vector<std::thread> pool;
+    for (std::size_t k = 1; k < parts; ++k) pool.emplace_back(work, k);
+    work(0);
+    for (auto& t : pool) t.join();
+    file.write("x,y,z\n", 6);
+    for (std::size_t k = 0; k < parts; ++k) file.write(out[k].data(), static_cast<std::streamsize>(used[k]));
 }
 
 std::mutex g_export_mu;
@@ -208,27 +228,33 @@ std::vector<std::thread> g_exports;
 
 void export_particles(const std::vector<Particle>& particles, int frame_no)
 {
-    // A vector kept on the GPU by resident stepping is read back first.
-    std::vector<double> fresh;
-    const double* rec = reinterpret_cast<const double*>(particles.data());
-    if (!particles.empty())
+    // A vector kept on the GPU by resident stepping: its positions are read back.
+    const std::size_t n = particles.size();
+    std::unique_ptr<double[]> fresh;
+    if (n > 0)
     {
-        fresh.resize(particles.size() * SNOW_RECORD_DOUBLES);
-        if (snow_host_resident_copy(particles, fresh.data())) rec = fresh.data();
+        fresh.reset(new double[3 * n]);
+        if (snow_host_resident_positions(particles, fresh.get()))
+        {
+            write_frame(fresh.get(), 3, n, frame_no);
+            return;
+        }
     }
-    write_frame(rec, particles.size(), frame_no);
+    write_frame(reinterpret_cast<const double*>(particles.data()), SNOW_RECORD_DOUBLES, n, frame_no);
 }
 
 namespace snow::gpu
 {
 void export_particles_async(const std::vector<Particle>& particles, int frame_no)
 {
-    std::vector<double> state(particles.size() * SNOW_RECORD_DOUBLES);
-    if (!particles.empty() && !snow_host_resident_copy(particles, state.data()))
-        std::memcpy(state.data(), particles.data(), state.size() * sizeof(double));
+    // the positions now (from the GPU when the vector is resident), the file later
     const std::size_t n = particles.size();
+    std::shared_ptr<double[]> xyz(new double[3 * std::max<std::size_t>(n, 1)]);
+    if (n > 0 && !snow_host_resident_positions(particles, xyz.get()))
+        for (std::size_t i = 0; i < n; ++i)
+            std::memcpy(&xyz[3 * i], &particles[i].x_p[0], 3 * sizeof(double));
     std::lock_guard<std::mutex> lock(g_export_mu);
-    g_exports.emplace_back([state = std::move(state), n, frame_no] { write_frame(state.data(), n, frame_no); });
+    g_exports.emplace_back([xyz, n, frame_no] { write_frame(xyz.get(), 3, n, frame_no); });
 }
 
 void wait_exports()
@@ -278,7 +304,7 @@ extern "C" int snow_io_export(const double* records, int64_t n, int frame_no)
     try
     {
         if (n < 0 || (n > 0 && !records)) throw std::runtime_error("snow_io_export: bad record array");
-        write_frame(records, static_cast<std::size_t>(n), frame_no);
+        write_frame(records, SNOW_RECORD_DOUBLES, static_cast<std::size_t>(n), frame_no);
         return 0;
     }
     catch (const std::exception& e)

@@ -126,6 +126,15 @@ void snow_host_resident_step(std::vector<Particle>& snow, const snow_step_params
     r.host_stale = true;
 }
 
+bool snow_host_resident_positions(const std::vector<Particle>& snow, double* xyz)
+{
+    auto& r = state();
+    std::lock_guard<std::mutex> lk(r.mu);
+    if (!r.batch || r.data != snow.data() || r.size != snow.size() || !r.host_stale) return false;
+    check(snow_gpu_batch_download_positions(r.batch, r.scene, xyz, static_cast<int64_t>(snow.size()), nullptr));
+    return true;
+}
+
 bool snow_host_resident_copy(const std::vector<Particle>& snow, double* out)
 {
     auto& r = state();

@@ -20,3 +20,6 @@ void snow_host_invalidate_resident();
 // If `snow` is the resident vector, copies the GPU state into `out` (n records)
 // and returns true.
 bool snow_host_resident_copy(const std::vector<Particle>& snow, double* out);
+// The positions only (x y z per particle) of a vector kept on the GPU; false
+// when `snow` is not the resident vector or the host copy is current.
+bool snow_host_resident_positions(const std::vector<Particle>& snow, double* xyz);

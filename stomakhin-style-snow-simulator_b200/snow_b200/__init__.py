@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
                                                      ctypes.POINTER(Collider), ctypes.c_int]),
         "snow_gpu_batch_upload": (ctypes.c_int, [vp, i32, _dp, i64, vp]),
         "snow_gpu_batch_download": (ctypes.c_int, [vp, i32, _dp, i64, vp]),
+        "snow_gpu_batch_download_positions": (ctypes.c_int, [vp, i32, _dp, i64, vp]),
         "snow_gpu_batch_setup": (ctypes.c_int, [vp, i32, d, vp]),
         "snow_gpu_batch_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(StepTimings), vp]),
         "snow_gpu_batch_scene_count": (ctypes.c_int, [vp]),
@@ -328,6 +329,13 @@ class Batch:
         if out is None:
             out = np.empty((n, 26), dtype=np.float64)
         _check(lib().snow_gpu_batch_download(self._h, sid, _ptr(out), n, ctypes.c_void_p(stream)))
+        return out
+
+    def download_positions(self, sid: int) -> np.ndarray:
+        """Particle positions (n x 3) in their original order (snow_gpu_batch_download_positions)."""
+        n = self.sizes[sid]
+        out = np.empty((n, 3))
+        _check(lib().snow_gpu_batch_download_positions(self._h, sid, _ptr(out), n, None))
         return out
 
     def snapshot(self, sid: int, stream: int | None = None) -> None:

@@ -184,3 +184,20 @@ def test_fresh_start_after_emitted_keys(snow, oracle):
     b.close()
     e = errors(got, want)
     assert max(e.values()) < 1e-10, e
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_download_positions_match_records(snow, prec):
+    """The positions-only read-back (what a frame export reads) equals the
+    position columns of the full records, in the particles' original order."""
+    from snow_b200 import scenes
+
+    sc = scenes.cube_scene(8)
+    b = snow.Batch(prec)
+    sid = b.add_scene(snow.setup(sc.particles.copy(), sc.dx), sc.params(), sc.planes)
+    b.step(3)
+    pos = b.download_positions(sid)
+    rec = b.download(sid)
+    b.close()
+    assert pos.shape == (rec.shape[0], 3)
+    assert np.array_equal(pos, rec[:, 0:3])

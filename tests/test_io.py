@@ -89,3 +89,32 @@ def test_export_matches_reference_export_byte_for_byte(tmp_path):
     a = (tmp_path / "a" / "output" / "frame_000007.csv").read_bytes()
     b = (tmp_path / "b" / "output" / "frame_000007.csv").read_bytes()
     assert a == b and a.startswith(b"x,y,z\n") and a.count(b"\n") == rec.shape[0] + 1
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference build (oracle/_ref) not present")
+def test_large_export_is_formatted_in_parts_and_matches_reference(tmp_path):
+    """A frame of 100,003 particles is formatted by several threads (16,384
+    rows or more each) and written in order: still byte for byte the
+    reference's export of the same records."""
+    rng = np.random.default_rng(9)
+    n = 100_003
+    rec = np.zeros((n, 26))
+    mags = 10.0 ** rng.uniform(-8, 8, (n, 3))
+    rec[:, 0:3] = mags * rng.choice([-1.0, 1.0], mags.shape)
+    L = _io()
+    R = ctypes.CDLL(REF_SO)
+    R.ref_export.argtypes = [_dp, ctypes.c_int64, ctypes.c_int]
+    cwd = os.getcwd()
+    try:
+        for who, d in (("ours", tmp_path / "a"), ("ref", tmp_path / "b")):
+            (d / "output").mkdir(parents=True)
+            os.chdir(d)
+            if who == "ours":
+                assert L.snow_io_export(rec.ctypes.data_as(_dp), n, 3) == 0
+            else:
+                R.ref_export(rec.ctypes.data_as(_dp), n, 3)
+    finally:
+        os.chdir(cwd)
+    a = (tmp_path / "a" / "output" / "frame_000003.csv").read_bytes()
+    b = (tmp_path / "b" / "output" / "frame_000003.csv").read_bytes()
+    assert a.count(b"\n") == n + 1 and a == b
