@@ -314,6 +314,14 @@ int snow_gpu_stage_p2g(const double* records, int64_t n, double grid_spacing, in
 int snow_gpu_stage_force(const double* records, int64_t n, double grid_spacing, double mu_0,
                          double lambda_0, double hardening_coefficient, int32_t* ijk,
                          double* fields, int64_t cap_nodes, int64_t* n_nodes);
+/* The kernels' own stencil weights along one axis (the branch-free form of
+ * N and N_dash, src/grid.cpp:24-58, that P2G and G2P evaluate): for each
+ * coordinate x[i], base[i] = floor(x / dx) - 1 and, for the nodes base + k,
+ * k = 0..3, w[4 i + k] = N(base + k, x / dx) and dw[4 i + k] =
+ * N_dash(base + k, x / dx) / dx, computed on the device in double
+ * (precision SNOW_FP64) or in float (SNOW_MIXED, results widened). */
+int snow_gpu_stage_weights(const double* x, int64_t n, double grid_spacing, int precision, int32_t* base,
+                           double* w, double* dw);
 /* P2G with a caller's stencil (src/grid.cpp:119-129): for each particle and
  * each of its 64 stencil weights, the mass and momentum contributions
  * out[n][64][4] = (m w, m v w); the caller adds them to the stencil's nodes. */

@@ -691,6 +691,14 @@ void Batch::prepare(cudaStream_t s) {
   else
     StepLaunch<float>::bbox_init(b, s);
   check_cuda(cudaGetLastError(), "bbox");
+  if (host_sized_ && !boxes_dirty_ && cap_blocks_ > 0) {
+    // the boxes are measured on the device for the key space; the grid and
+    // bins are the caller's reservation
+    ensure_items();
+    num_dev_scenes_ = (int)table_.size();
+    dirty_ = params_dirty_ = false;
+    return;
+  }
   std::vector<SceneDev> measured(table_.size());
   if (!measured.empty())
     check_cuda(cudaMemcpyAsync(measured.data(), d_scenes_, measured.size() * sizeof(SceneDev),
@@ -978,8 +986,20 @@ void Batch::reserve_scenes(const std::vector<int64_t>& sizes, int64_t max_bytes)
   std::vector<int64_t> strides;
   size_t total = 0;
   int64_t bytes = 0;
+  // sizes that a cached buffer set would serve (add_scene's rule: the
+  // smallest at most twice the size), each cached set counted once
+  std::vector<bool> taken(cache_.size(), false);
   for (int64_t n : sizes) {
     const int64_t st = pad32(std::max<int64_t>(n, 1));
+    int best = -1;
+    for (int c = 0; c < (int)cache_.size(); ++c)
+      if (!taken[c] && cache_[c].stride >= st && cache_[c].stride <= 2 * st &&
+          (best < 0 || cache_[c].stride < cache_[best].stride))
+        best = c;
+    if (best >= 0) {
+      taken[best] = true;
+      continue;
+    }
     if (bytes + scene_bytes(st) > max_bytes) break;
     bytes += scene_bytes(st);
     strides.push_back(st);

@@ -122,6 +122,11 @@ class Batch {
   int64_t capacity_blocks() const { return cap_blocks_; }
   // Particles per P2G/G2P work item (a power of two, 32..1024).  Until set
   // (here or by autotune) it follows the batch's particle count: auto_chunk.
+  // Host-sized batches (the server's live batch): the caller reserves the grid
+  // and the key bins for the scenes it adds (reserve_grid), so a change of
+  // scenes alone does not read the measured boxes back to size them; growth
+  // past the reservation's headroom (step_complete) still does.
+  void set_host_sized(bool on) { host_sized_ = on; }
   void set_chunk(int chunk) {
     if (chunk < 32 || chunk > 1024 || (chunk & (chunk - 1))) throw Error(SNOW_E_ARG, "chunk must be a power of two in [32, 1024]");
     chunk_ = chunk;
@@ -253,6 +258,7 @@ class Batch {
   int32_t cap_items_ = 0;
   int32_t chunk_ = 256;
   bool chunk_auto_ = true;
+  bool host_sized_ = false;
 
   double* staging_ = nullptr;
   int64_t staging_cap_ = 0;

@@ -211,6 +211,7 @@ class Server {
     bool base_recorded = false;
     double t_phase = now();
     batch_.set_chunk(work_item_ ? work_item_ : auto_work_item(order));
+    batch_.set_host_sized(true);
     reserve(order, s);
     admit_s_ += now() - t_phase;
     for (;;) {
@@ -508,6 +509,14 @@ class Server {
   // allocations out of the ticks and batches them.
   void grow_for(const std::vector<Request*>& fresh, const std::vector<Request*>& live,
                 const std::vector<Request*>& admitting, cudaStream_t s) {
+    // Particle buffers for the fresh requests, carved from one allocation:
+    // admitting them then allocates nothing, and the buffers of finished
+    // scenes stay cached for later ones instead of being freed (a cudaFree
+    // inside the loop waits for the tick in flight).
+    std::vector<int64_t> sizes;
+    for (Request* r : fresh)
+      if (r->bytes <= budget_) sizes.push_back((int64_t)r->records.size() / 26);
+    admit_.reserve_scenes(sizes, budget_);
     Need need;
     for (const auto* group : {&live, &admitting})
       for (Request* r : *group) need.add(*r);

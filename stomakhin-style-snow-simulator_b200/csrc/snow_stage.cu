@@ -256,6 +256,20 @@ __global__ void k_deformation_differential(const double* rec, int64_t n, double 
       dF[9 * i + c * 3 + r] = dt * (G[r] * F[c * 3] + G[3 + r] * F[c * 3 + 1] + G[6 + r] * F[c * 3 + 2]);
 }
 
+// axis_weights of every coordinate, in precision R (widened to double).
+template <typename R>
+__global__ void k_axis_weights(const double* x, int64_t n, double dx, int32_t* base, double* w, double* dw) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const AxisWeights<R> a = axis_weights((R)x[i], (R)dx);
+  base[i] = a.base;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    w[4 * i + k] = (double)a.w[k];
+    dw[4 * i + k] = (double)a.dw[k];
+  }
+}
+
 // out[i][e] = (m w, m v w) for stencil weight w = weights[i][e] (grid.cpp:121-127).
 __global__ void k_p2g_stencil(const double* rec, int64_t n, const double* weights, double* out) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -521,6 +535,27 @@ int snow_gpu_stage_particle_collisions(double* records, int64_t n, const snow_co
     k_particle_collide<<<blocks_for(n), 256>>>(d.p, n, dc.p, (int)c.size());
     check_cuda(cudaGetLastError(), "particle collisions");
     check_cuda(cudaMemcpy(records, d.p, n * 208, cudaMemcpyDeviceToHost), "records");
+  });
+}
+
+int snow_gpu_stage_weights(const double* x, int64_t n, double grid_spacing, int precision, int32_t* base,
+                           double* w, double* dw) {
+  return guarded([&] {
+    if (n < 0 || (n > 0 && (!x || !base || !w || !dw))) throw Error(SNOW_E_ARG, "NULL argument");
+    if (!(grid_spacing > 0.0)) throw Error(SNOW_E_ARG, "grid_spacing must be positive");
+    if (precision != SNOW_FP64 && precision != SNOW_MIXED) throw Error(SNOW_E_ARG, "unknown precision");
+    if (n == 0) return;
+    DBuf<double> dx_((size_t)n), dw_((size_t)n * 4), ddw((size_t)n * 4);
+    DBuf<int32_t> db((size_t)n);
+    check_cuda(cudaMemcpy(dx_.p, x, n * sizeof(double), cudaMemcpyHostToDevice), "x");
+    if (precision == SNOW_FP64)
+      k_axis_weights<double><<<blocks_for(n), 256>>>(dx_.p, n, grid_spacing, db.p, dw_.p, ddw.p);
+    else
+      k_axis_weights<float><<<blocks_for(n), 256>>>(dx_.p, n, grid_spacing, db.p, dw_.p, ddw.p);
+    check_cuda(cudaGetLastError(), "weights");
+    check_cuda(cudaMemcpy(base, db.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost), "base");
+    check_cuda(cudaMemcpy(w, dw_.p, n * 4 * sizeof(double), cudaMemcpyDeviceToHost), "w");
+    check_cuda(cudaMemcpy(dw, ddw.p, n * 4 * sizeof(double), cudaMemcpyDeviceToHost), "dw");
   });
 }
 

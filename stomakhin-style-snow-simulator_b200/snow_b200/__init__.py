@@ -116,6 +116,7 @@ def lib() -> ctypes.CDLL:
         "snow_gpu_batch_upload": (ctypes.c_int, [vp, i32, _dp, i64, vp]),
         "snow_gpu_batch_download": (ctypes.c_int, [vp, i32, _dp, i64, vp]),
         "snow_gpu_batch_download_positions": (ctypes.c_int, [vp, i32, _dp, i64, vp]),
+        "snow_gpu_stage_weights": (ctypes.c_int, [_dp, i64, ctypes.c_double, ctypes.c_int, _ip, _dp, _dp]),
         "snow_gpu_batch_setup": (ctypes.c_int, [vp, i32, d, vp]),
         "snow_gpu_batch_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(StepTimings), vp]),
         "snow_gpu_batch_scene_count": (ctypes.c_int, [vp]),
@@ -548,6 +549,17 @@ def stage_implicit(ijk, fields, records, dx, dt, mu0, lambda0, xi, beta, q=None,
                                          float(squared_tolerance), int(max_iterations),
                                          None if qq is None else _ptr(qq), _ptr(out), ctypes.byref(it)))
     return out, it.value
+
+
+def stage_weights(x, dx, precision: int = 0):
+    """The device stencil weights along one axis: (base[n], w[n][4], dw[n][4])."""
+    xs = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    n = xs.shape[0]
+    base = np.zeros(n, np.int32)
+    w = np.zeros((n, 4))
+    dw = np.zeros((n, 4))
+    _check(lib().snow_gpu_stage_weights(_ptr(xs), n, float(dx), int(precision), _ptr(base, _ip), _ptr(w), _ptr(dw)))
+    return base, w, dw
 
 
 def stage_position_update(records, dt) -> np.ndarray:

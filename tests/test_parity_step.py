@@ -102,3 +102,40 @@ def test_negative_coordinates(snow, oracle):
     got = _run_batch(snow, r0, sc.params(), sc.planes, 5)
     e = errors(got, want)
     assert max(e.values()) < TOL, e
+
+
+def test_device_stencil_weights_match_reference_spline(snow, oracle):
+    """The kernels' own branch-free weights and slopes (axis_weights, run on
+    the device in double) against the reference's N and N_dash (grid.cpp:24-58,
+    through the oracle) at random positions, on the grid knots and one ulp to
+    either side: the same stencil base, weights within 2e-15 and slopes within
+    2e-15 / dx; the weights sum to 1 and the slopes to 0.  The float form
+    (the mixed path) against the same functions at |x / dx| <= 5, away from
+    the knots: its single-precision grid position x / dx may differ from the
+    double one by two ulp, so within 4e-6."""
+    rng = np.random.default_rng(17)
+    dx = 0.02
+    knots = np.arange(-50, 50) * dx
+    xs = np.concatenate([rng.uniform(-1.0, 1.0, 2000), knots, np.nextafter(knots, 10), np.nextafter(knots, -10)])
+    base, w, dw = snow.stage_weights(xs, dx, 0)
+    tol = 2e-15
+    for i, x in enumerate(xs):
+        gp = x / dx
+        b = int(np.floor(gp)) - 1
+        assert base[i] == b, (x, base[i], b)
+        for k in range(4):
+            assert abs(w[i, k] - oracle.N(b + k, gp)) <= tol, (x, k)
+            assert abs(dw[i, k] - oracle.N_dash(b + k, gp) / dx) <= tol / dx, (x, k)
+    assert np.abs(w.sum(axis=1) - 1).max() <= 4 * tol
+    assert np.abs(dw.sum(axis=1)).max() <= 8 * tol / dx
+    xf = rng.uniform(-0.1, 0.1, 2000)
+    fr = xf / dx - np.floor(xf / dx)
+    xf = xf[(fr > 1e-4) & (fr < 1 - 1e-4)]
+    base, w, dw = snow.stage_weights(xf, dx, 1)
+    for i, x in enumerate(xf):
+        gp = x / dx
+        b = int(np.floor(gp)) - 1
+        assert base[i] == b, (x, base[i], b)
+        for k in range(4):
+            assert abs(w[i, k] - oracle.N(b + k, gp)) <= 4e-6, (x, k)
+            assert abs(dw[i, k] - oracle.N_dash(b + k, gp) / dx) <= 4e-6 / dx, (x, k)
