@@ -440,9 +440,12 @@ __global__ void __launch_bounds__(256) k_bins(const BatchDev b) {
     const int64_t bin0 = tile * kBinTile + threadIdx.x * 16;
     const int64_t bk = bin0 >> 6;
     const bool live = bk < K;
+    // A block key without particles (occupancy 0) has zero counts: its counts
+    // are neither read nor cleared, and its offsets are never looked up.
+    const bool occupied = live && b.occ[bk] != 0;
     uint32_t c[16];
     uint32_t sum = 0;
-    if (live) {
+    if (occupied) {
       const uint4* src = reinterpret_cast<const uint4*>(b.bins + bin0);
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
@@ -547,7 +550,7 @@ __global__ void __launch_bounds__(256) k_bins(const BatchDev b) {
     __syncthreads();
     const unsigned long long run = s_prefix + before + x - v;
     uint32_t pos = (uint32_t)(run & kPartMask);
-    if (live) {
+    if (occupied) {
       uint4* off = reinterpret_cast<uint4*>(b.bin_off + bin0);
       uint4* zero = reinterpret_cast<uint4*>(b.bins + bin0);
 #pragma unroll
