@@ -186,7 +186,8 @@ int snow_gpu_batch_chunk(snow_gpu_batch* batch);
  * step up to the order of floating-point sums.  No reference counterpart. */
 int snow_gpu_batch_set_dense(snow_gpu_batch* batch, int enable);
 /* Kernels launched by one replay of the batch's captured step graph (0 until
- * a multi-step call captured it).  No reference counterpart. */
+ * a step was captured: the batch's first step runs eagerly, later steps, one
+ * per call or several, are captured and replayed).  No reference counterpart. */
 int snow_gpu_batch_graph_kernels(snow_gpu_batch* batch);
 /* Particle ordering in use: 1 counting sort over dense key bins, 0 radix sort
  * (set by set_dense, the autotuner, or the size of the key boxes).  No
