@@ -760,11 +760,15 @@ __device__ __forceinline__ uint32_t num_blocks(const BatchDev& b) {
 }
 
 // Work-item queue of a persistent CTA.  Warp 0 claims the next item and loads
-// its header into registers while the CTA works on the current one, so the
-// claim costs one barrier and no dependent global loads.
+// its header into registers while the CTA works on the current one, so a claim
+// costs no dependent global loads.  claim() stores the header in one shared
+// buffer between two barriers; claim_buffered() stores it in the other of two
+// buffers (the one of the item before, which nobody reads any more) and needs
+// one barrier.
 struct ItemQueue {
-  int next;   // item claimed ahead (warp 0)
-  int word;   // header word `lane` of that item (lanes 0..15 of warp 0)
+  int next;     // item claimed ahead (warp 0)
+  int word;     // header word `lane` of that item (lanes 0..15 of warp 0)
+  int cur = 0;  // header buffer of the current item
   __device__ void fetch(const BatchDev& b, uint32_t* counter, uint32_t items) {
     if (threadIdx.x >= 32) return;
     int n = 0;
@@ -781,6 +785,20 @@ struct ItemQueue {
     if ((uint32_t)s_next >= items) return false;
     fetch(b, counter, items);
     return true;
+  }
+  // The next item's header (hdr[2], s_next[2] in shared memory), or null when
+  // the queue is empty.
+  __device__ const BlockHeader* claim_buffered(const BatchDev& b, uint32_t* counter, BlockHeader* hdr,
+                                               int* s_next) {
+    const uint32_t items = min(b.ctr->n_items, (uint32_t)b.cap_items);
+    const int nb = cur ^ 1;
+    if (threadIdx.x < 16) reinterpret_cast<int*>(&hdr[nb])[threadIdx.x] = word;
+    if (threadIdx.x == 0) s_next[nb] = next;
+    __syncthreads();  // everyone is done with the previous item's tile; its successor's header is stored
+    cur = nb;
+    if ((uint32_t)s_next[cur] >= items) return nullptr;
+    fetch(b, counter, items);
+    return &hdr[cur];
   }
 };
 
@@ -954,7 +972,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile = reinterpret_cast<R*>(smem_raw);  // [NCH][TileShape<R>::N]
   R* recs = tile + NCH * TileShape<R>::N;              // [warps][32][kRec]
-  __shared__ BlockHeader h;
+  __shared__ BlockHeader hbuf[2];
+  __shared__ int s_next[2];
   R* acc_g = (R*)b.acc;
   const int64_t plane = (int64_t)b.cap_blocks * 64;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -962,12 +981,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
   const int qi = lane >> 4, qj = (lane >> 2) & 3, qk = lane & 3;
   const int col = tile_index<R>(0, qj, qk);
 
-  __shared__ int s_item;
+  // The tile is zeroed once here; each item's flush clears what it adds (the
+  // barrier at the next claim orders that before the next item's walk).
+  for (int e = threadIdx.x; e < NCH * TileShape<R>::N; e += blockDim.x) tile[e] = R(0);
   ItemQueue q;
   q.fetch(b, &b.ctr->work_p2g, min(b.ctr->n_items, (uint32_t)b.cap_items));
-  while (q.claim(b, &b.ctr->work_p2g, h, s_item)) {
-    for (int e = threadIdx.x; e < NCH * TileShape<R>::N; e += blockDim.x) tile[e] = R(0);
-    __syncthreads();
+  while (const BlockHeader* hp = q.claim_buffered(b, &b.ctr->work_p2g, hbuf, s_next)) {
+    const BlockHeader& h = *hp;
     const SceneDev& sc = b.scenes[h.scene];
     const R dx = (R)sc.dx;
     const PlaneView<R> pv{(const R*)sc.r[sc.cur], sc.fp[sc.cur], sc.id[sc.cur], sc.stride};
@@ -1131,23 +1151,28 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_p2g(const Batch
       __syncwarp();
     }
     __syncthreads();
-    // Flush: one global atomic per touched node and channel.
+    // Flush: one global atomic per touched node and channel, clearing the
+    // tile as it goes.
     for (int e = threadIdx.x; e < 8 * 64; e += blockDim.x) {
       const int d = e >> 6, node = e & 63;
       int t;
       if (!tile_of<R>(d, node, t)) continue;
       const int32_t nb = h.nbr[d];
-      if (nb < 0) continue;
-      const int64_t g = (int64_t)nb * 64 + node;
+      R v[NCH];
       bool any = false;
 #pragma unroll
-      for (int ch = 0; ch < NCH; ++ch) any |= tile[ch * TileShape<R>::N + t] != R(0);
+      for (int ch = 0; ch < NCH; ++ch) {
+        v[ch] = tile[ch * TileShape<R>::N + t];
+        any |= v[ch] != R(0);
+      }
       if (!any) continue;
 #pragma unroll
-      for (int ch = 0; ch < NCH; ++ch) {
-        const R v = tile[ch * TileShape<R>::N + t];
-        if (v != R(0)) atomicAdd(&acc_g[ch * plane + g], v);
-      }
+      for (int ch = 0; ch < NCH; ++ch) tile[ch * TileShape<R>::N + t] = R(0);
+      if (nb < 0) continue;
+      const int64_t g = (int64_t)nb * 64 + node;
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch)
+        if (v[ch] != R(0)) atomicAdd(&acc_g[ch * plane + g], v[ch]);
     }
   }
 }
