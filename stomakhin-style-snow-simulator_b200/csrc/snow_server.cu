@@ -92,6 +92,12 @@ class Server {
       batch_.step_complete();
     } catch (...) {
     }
+    // Copies into the requests' page-locked records may still be in flight
+    // when run() left by an exception: let them finish before the records are
+    // unregistered and the streams destroyed.
+    for (cudaStream_t st : {admit_s_stream_, retire_s_stream_, main_s_})
+      if (st) cudaStreamSynchronize(st);
+    cudaGetLastError();
     for (auto& r : reqs_) {
       if (r->pinned) cudaHostUnregister(r->records.data());
       if (r->done) cudaEventDestroy(r->done);
