@@ -151,17 +151,21 @@ __global__ void __launch_bounds__(256) k_bbox_init(const BatchDev b) {
 }
 
 // ------------------------------------------------------------------ keyspace
-// Exclusive prefix of one count per scene over the block (256 threads, scenes
-// in rounds of 256): writes each scene's base and count through `put` and
-// returns the total (to every thread).
+// One CTA sets up the key space of a step: 1024 threads take up to 1024
+// scenes in one round of each prefix (a served batch holds hundreds).
+constexpr int kKeyspaceThreads = 1024;
+
+// Exclusive prefix of one count per scene over the block (up to 1024 threads,
+// scenes in rounds of blockDim.x): writes each scene's base and count through
+// `put` and returns the total (to every thread).
 template <typename Count, typename Put>
 __device__ unsigned long long scene_prefix(const BatchDev& b, Count&& count, Put&& put) {
   __shared__ unsigned long long s_carry;
-  __shared__ unsigned long long s_warp[8];
+  __shared__ unsigned long long s_warp[32];
   if (threadIdx.x == 0) s_carry = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int base = 0; base < b.num_scenes; base += 256) {
+  for (int base = 0; base < b.num_scenes; base += blockDim.x) {
     const int s = base + threadIdx.x;
     const unsigned long long cnt = s < b.num_scenes ? count(s) : 0ull;
     unsigned long long x = cnt;
@@ -176,7 +180,7 @@ __device__ unsigned long long scene_prefix(const BatchDev& b, Count&& count, Put
     const unsigned long long incl = s_carry + before + x;
     if (s < b.num_scenes) put(s, incl - cnt, cnt);
     __syncthreads();
-    if (threadIdx.x == 255) s_carry = incl;
+    if (threadIdx.x == blockDim.x - 1) s_carry = incl;
     __syncthreads();
   }
   const unsigned long long total = s_carry;
@@ -200,7 +204,7 @@ __device__ __forceinline__ uint32_t clamp32(unsigned long long v) {
 // is the particles' block box grown by one block on every side, plus the same
 // high margin: emit_ok when those boxes fit the dense bins.
 template <bool kSwap>
-__global__ void __launch_bounds__(256) k_keyspace(const BatchDev b) {
+__global__ void __launch_bounds__(kKeyspaceThreads) k_keyspace(const BatchDev b) {
   __shared__ int s_emitted, s_cleanup;
   if (kSwap)
     for (int s = threadIdx.x; s < b.num_scenes; s += blockDim.x) b.scenes[s].cur ^= 1;
@@ -1888,7 +1892,7 @@ void StepLaunch<R>::bbox_init(const BatchDev& b, cudaStream_t s) {
 }
 template <typename R>
 void StepLaunch<R>::keyspace(const BatchDev& b, cudaStream_t s, bool) {
-  k_keyspace<false><<<1, 256, 0, s>>>(b);
+  k_keyspace<false><<<1, kKeyspaceThreads, 0, s>>>(b);
 }
 template <typename R>
 void StepLaunch<R>::keys(const BatchDev& b, cudaStream_t s) {
@@ -1983,7 +1987,7 @@ void StepLaunch<R>::finish(const BatchDev& b, cudaStream_t s) {
 }
 template <typename R>
 void StepLaunch<R>::finish_and_keyspace(const BatchDev& b, cudaStream_t s) {
-  k_keyspace<true><<<1, 256, 0, s>>>(b);
+  k_keyspace<true><<<1, kKeyspaceThreads, 0, s>>>(b);
 }
 
 template struct StepLaunch<double>;
