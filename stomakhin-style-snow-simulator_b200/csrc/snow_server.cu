@@ -183,7 +183,8 @@ class Server {
   // streams, events and every buffer that scales with them are made before it
   // (a cudaMalloc or cudaFree inside it can wait for the tick in flight).
   // Requests submitted while it runs are reserved for between ticks
-  // (grow_for), in doublings.  Each pass launches a tick of steps for
+  // (grow_for), in doublings, and their particle buffers allocated while a
+  // tick runs (carve_for).  Each pass launches a tick of steps for
   // the live scenes, then, while it runs, issues the setup of newly arrived
   // requests in a second batch on a second stream and the result copies of
   // finished scenes on a third, without waiting for either; after the tick it
@@ -211,7 +212,7 @@ class Server {
     if (!s) s = main_stream();
     std::stable_sort(order.begin(), order.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
     std::deque<Request*> pending(order.begin(), order.end());
-    std::vector<Request*> live, admitting, leaving;
+    std::vector<Request*> live, admitting, leaving, carve;
     int64_t used = 0;
     ticks_log_.clear();
     bool base_recorded = false;
@@ -232,6 +233,7 @@ class Server {
       if (!fresh.empty()) {
         t_phase = now();
         grow_for(fresh, live, admitting, s);
+        carve.insert(carve.end(), fresh.begin(), fresh.end());
         std::stable_sort(fresh.begin(), fresh.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
         std::deque<Request*> merged;
         std::merge(pending.begin(), pending.end(), fresh.begin(), fresh.end(), std::back_inserter(merged),
@@ -266,8 +268,14 @@ class Server {
         check_cuda(cudaEventRecord(ev_end_, s), "cudaEventRecord");
       }
       step_s_ += now() - t_phase;
-      // issue the setup of every arrived request that fits, in arrival order
+      // particle buffers for the requests that arrived since the last pass,
+      // allocated while the tick runs
       t_phase = now();
+      if (!carve.empty()) {
+        carve_for(carve);
+        carve.clear();
+      }
+      // issue the setup of every arrived request that fits, in arrival order
       while (!pending.empty() && pending.front()->arrival <= now()) {
         Request* r = pending.front();
         if (r->bytes > budget_) {  // can never fit
@@ -515,14 +523,6 @@ class Server {
   // allocations out of the ticks and batches them.
   void grow_for(const std::vector<Request*>& fresh, const std::vector<Request*>& live,
                 const std::vector<Request*>& admitting, cudaStream_t s) {
-    // Particle buffers for the fresh requests, carved from one allocation:
-    // admitting them then allocates nothing, and the buffers of finished
-    // scenes stay cached for later ones instead of being freed (a cudaFree
-    // inside the loop waits for the tick in flight).
-    std::vector<int64_t> sizes;
-    for (Request* r : fresh)
-      if (r->bytes <= budget_) sizes.push_back((int64_t)r->records.size() / 26);
-    admit_.reserve_scenes(sizes, budget_);
     Need need;
     for (const auto* group : {&live, &admitting})
       for (Request* r : *group) need.add(*r);
@@ -541,6 +541,18 @@ class Server {
     twice.box_max = std::max(need.box_max, have.box_max);
     twice.grid_max = std::max(need.grid_max, have.grid_max);
     reserve_need(twice, s, false);
+  }
+
+  // Particle buffers for fresh requests, carved from one allocation: admitting
+  // them then allocates nothing, and the buffers of finished scenes stay
+  // cached for later ones instead of being freed (a cudaFree inside the loop
+  // waits for the tick in flight).  The allocation issues no stream work, so
+  // the loop makes it while a tick runs.
+  void carve_for(const std::vector<Request*>& fresh) {
+    std::vector<int64_t> sizes;
+    for (Request* r : fresh)
+      if (r->bytes <= budget_) sizes.push_back((int64_t)r->records.size() / 26);
+    admit_.reserve_scenes(sizes, budget_);
   }
 
   cudaStream_t main_stream() {
