@@ -249,6 +249,28 @@ def timed_steps(batch, steps, sp, torch) -> float:
     return e0.elapsed_time(e1)
 
 
+def copy_bound(torch, host, n: int, rate: float) -> dict:
+    """The host-link bound of one drop-in call: the same record bytes copied
+    host -> device and back from the same page-locked buffer, with no step
+    between (best of three, CUDA events), and the share of the measured call
+    time it takes."""
+    dev = torch.empty(host.shape, dtype=torch.float64, device="cuda")
+    src = torch.from_numpy(host)
+    best = float("inf")
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        dev.copy_(src, non_blocking=True)
+        src.copy_(dev, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    call_ms = 1e3 * n / rate
+    return {"copy_only_ms": best, "call_ms": call_ms, "copy_share_of_call": best / call_ms,
+            "link_gbs_each_way": 2 * host.nbytes / (best * 1e-3) / 2e9}
+
+
 def plain_fp64_rate(snow_b200, torch, sp, items, settle: int = 0) -> float:
     """Particle-steps/s of the plain FP64 path on the given scenes: each scene
     alone in its own one-scene batch (the drop-in step on resident state, with
@@ -816,6 +838,7 @@ def run_ours(args, ws, rank, local):
         e2e = {"value": ws * sc.n * ke / dt_e, "unit": "particle-steps/s",
                "h2d_bytes_per_step": sc.n * 208, "d2h_bytes_per_step": sc.n * 208,
                "steps": ke, "api": "snow_gpu_step (upload, step, download per call)"}
+        e2e.update(copy_bound(torch, host, sc.n, e2e["value"] / ws))
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

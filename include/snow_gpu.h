@@ -280,7 +280,10 @@ int snow_gpu_server_ticks(snow_gpu_server* server, snow_server_tick* out, int64_
 /* ---- one scene: setup() / step() of the reference ------------------------ */
 /* setup() on host records: records[i].V_p0 is overwritten. */
 int snow_gpu_setup(double* records, int64_t n, double grid_spacing);
-/* n_steps of step() on host records, in place (upload, steps, download). */
+/* n_steps of step() on host records, in place (upload, steps, download).  A
+ * call on as many records as the last completed call places them in the
+ * block-sorted order that call's step left, so its first step reads sorted
+ * particles; the results do not depend on it. */
 int snow_gpu_step(double* records, int64_t n, const snow_step_params* params,
                   const snow_collider* colliders, int n_colliders, int n_steps,
                   snow_step_timings* timings);

@@ -94,6 +94,29 @@ __global__ void k_records_to_planes(const double* rec, int64_t n, R* r, double* 
   id[i] = (int32_t)i;
 }
 
+// The same into the slots the scene's particles already occupy: slot j takes
+// record id[j].  After a step the slots are block-sorted, so the next step
+// reads its particles in sorted order instead of the caller's.  An id outside
+// [0, n) is never read through; it sets a status bit instead.
+template <typename R>
+__global__ void k_records_to_planes_ordered(const double* rec, int64_t n, R* r, double* fp, const int32_t* id,
+                                            int64_t st, uint32_t* status) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int64_t src = id[j];
+  if (src < 0 || src >= n) {
+    atomicOr(status, ST_LOOKUP_MISS);
+    return;
+  }
+  const double* p = rec + 26 * src;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k * st + j] = (R)p[k];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) fp[k * st + j] = p[8 + k];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) r[(PFE + k) * st + j] = (R)p[17 + k];
+}
+
 template <typename R>
 __global__ void k_planes_to_records(double* rec, int64_t n, const R* r, const double* fp,
                                     const int32_t* id, int64_t st) {
@@ -445,7 +468,7 @@ void Batch::set_params(int32_t id, const snow_step_params* params, const snow_co
   force_dirty_ = true;
 }
 
-void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s, bool wait) {
+void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s, bool wait, bool keep_order) {
   step_complete();
   Scene* sc = find(id);
   if (n != sc->n) throw Error(SNOW_E_ARG, "upload: particle count differs from the scene's");
@@ -453,7 +476,13 @@ void Batch::upload(int32_t id, const double* records, int64_t n, cudaStream_t s,
   ensure_staging(n);
   copy_in(staging_, records, (size_t)n * 26 * sizeof(double), s, wait);
   const unsigned g = (unsigned)((n + 255) / 256);
-  if (prec_ == SNOW_FP64)
+  if (keep_order && prec_ == SNOW_FP64)
+    k_records_to_planes_ordered<double><<<g, 256, 0, s>>>(staging_, n, (double*)sc->r[sc->cur], sc->fp[sc->cur],
+                                                           sc->id[sc->cur], sc->stride, &d_ctr_->status);
+  else if (keep_order)
+    k_records_to_planes_ordered<float><<<g, 256, 0, s>>>(staging_, n, (float*)sc->r[sc->cur], sc->fp[sc->cur],
+                                                          sc->id[sc->cur], sc->stride, &d_ctr_->status);
+  else if (prec_ == SNOW_FP64)
     k_records_to_planes<double><<<g, 256, 0, s>>>(staging_, n, (double*)sc->r[sc->cur],
                                                    sc->fp[sc->cur], sc->id[sc->cur], sc->stride);
   else
@@ -1334,6 +1363,10 @@ int snow_gpu_batch_set_graphs(snow_gpu_batch* batch, int enable) {
 // upload, run, download on every call).
 static std::mutex g_single_mu;
 static std::unique_ptr<Batch> g_single;
+// True while the one-scene batch's id plane is a permutation of its records
+// (the last call on it completed): the next step call uploads into the slots
+// the last step left, in block-sorted order.
+static bool g_single_ordered = false;
 
 static Batch& single_batch() {
   if (!g_single) g_single = std::make_unique<Batch>(SNOW_FP64);
@@ -1346,12 +1379,14 @@ int snow_gpu_setup(double* records, int64_t n, double grid_spacing) {
     if (n < 0 || (n > 0 && !records)) throw Error(SNOW_E_ARG, "bad particle array");
     if (n == 0) return;
     Batch& b = single_batch();
+    g_single_ordered = false;
     b.clear();
     snow_step_params p{};
     p.grid_spacing = grid_spacing;
     const int32_t id = b.add_scene(records, n, &p, nullptr, 0, nullptr);
     b.setup(id, grid_spacing, nullptr);
     b.download(id, records, n, nullptr);
+    g_single_ordered = true;
   });
 }
 
@@ -1364,16 +1399,19 @@ int snow_gpu_step(double* records, int64_t n, const snow_step_params* params,
     if (n == 0 || n_steps == 0) return;
     Batch& b = single_batch();
     int32_t id;
+    const bool ordered = g_single_ordered;
+    g_single_ordered = false;
     if (b.scene_count() == 1 && b.particles() == n) {
       id = b.first_id();
       b.set_params(id, params, colliders, n_colliders);
-      b.upload(id, records, n, nullptr);
+      b.upload(id, records, n, nullptr, true, ordered);
     } else {
       b.clear();
       id = b.add_scene(records, n, params, colliders, n_colliders, nullptr);
     }
     b.step(n_steps, timings, nullptr);
     b.download(id, records, n, nullptr);
+    g_single_ordered = true;
   });
 }
 

@@ -69,7 +69,12 @@ class Batch {
                     const snow_collider* colliders, int n_colliders, cudaStream_t s, bool wait = true);
   void remove_scene(int32_t id);
   void set_params(int32_t id, const snow_step_params* params, const snow_collider* c, int n);
-  void upload(int32_t id, const double* records, int64_t n, cudaStream_t s, bool wait = true);
+  // keep_order: slot j of the scene takes record id[j], the order its last
+  // step left (block-sorted), instead of record j; only valid while the
+  // scene's id plane is a permutation of [0, n), i.e. after a step or upload
+  // that completed without an error.
+  void upload(int32_t id, const double* records, int64_t n, cudaStream_t s, bool wait = true,
+              bool keep_order = false);
   void download(int32_t id, double* records, int64_t n, cudaStream_t s, bool wait = true);
   void download_positions(int32_t id, double* xyz, int64_t n, cudaStream_t s);
   // box_blocks >= 0: an upper bound on the scene's block box at dx (in 4^3

@@ -77,6 +77,30 @@ def test_literal_step_entry_point(snow, oracle):
     assert max(e.values()) < TOL, e
 
 
+def test_step_calls_in_sorted_order(snow, oracle):
+    """Consecutive snow_gpu_step calls on as many records place them in the
+    order the last step left (block-sorted).  Results follow the caller's
+    records: chained calls equal the oracle's steps, and a call on the same
+    records shuffled equals the oracle on the shuffled records, row for row."""
+    from snow_b200 import scenes
+
+    sc = scenes.tori_scene(n_per_torus=6000, steps=4)
+    sc.particles[:, 0] += np.where(sc.particles[:, 3] > 0, 0.12, -0.12)  # start in contact
+    rec = oracle.setup(sc.particles, sc.dx)
+    want, _ = oracle.step(rec, sc.params(), sc.plane_array(), 3)
+    got = rec.copy()
+    snow.step(got, sc.params(), sc.planes, 1)
+    snow.step(got, sc.params(), sc.planes, 2)
+    e = errors(got, want)
+    assert max(e.values()) < TOL, e
+    perm = np.random.default_rng(5).permutation(got.shape[0])
+    mixed = got[perm].copy()
+    want2, _ = oracle.step(mixed, sc.params(), sc.plane_array(), 1)
+    snow.step(mixed, sc.params(), sc.planes, 1)
+    e = errors(mixed, want2)
+    assert max(e.values()) < TOL, e
+
+
 def test_colliding_tori_small(snow, oracle):
     """Two small tori at +-8 m/s meeting over a few steps, against the oracle."""
     from snow_b200 import scenes
