@@ -271,6 +271,9 @@ int snow_gpu_server_close(snow_gpu_server* server);
  * snow_gpu_batch_set_chunk, else a power of two in [32, 1024].  Results do not depend on it beyond the
  * order of atomic sums.  No reference counterpart. */
 int snow_gpu_server_set_work_item(snow_gpu_server* server, int particles);
+/* One tick of run(): host and device seconds on the server clock, steps,
+ * live scenes and particles, the scenes that joined the live batch just before
+ * it and those that finish with it. */
 typedef struct snow_server_tick {
   double host_start_s, host_end_s, device_start_s, device_end_s;
   int64_t steps, scenes, particles, admitted, retired;

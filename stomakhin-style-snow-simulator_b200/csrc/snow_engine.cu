@@ -218,19 +218,30 @@ Batch::Batch(int precision) : prec_(precision) {
   rsize_ = precision == SNOW_FP64 ? sizeof(double) : sizeof(float);
   d_ctr_ = dalloc<Counters>(1);
   check_cuda(cudaMemset(d_ctr_, 0, sizeof(Counters)), "cudaMemset");
-  check_cuda(cudaMallocHost((void**)&h_ctr_, sizeof(Counters)), "cudaMallocHost");
-  std::memset(h_ctr_, 0, sizeof(Counters));
+  check_cuda(cudaMallocHost((void**)&h_ctr_buf_, 2 * sizeof(Counters)), "cudaMallocHost");
+  std::memset(h_ctr_buf_, 0, 2 * sizeof(Counters));
+  h_ctr_ = h_ctr_buf_;
   check_cuda(cudaStreamCreate(&own_stream_), "cudaStreamCreate");
 }
 
 Batch::~Batch() {
   if (pending_) cudaStreamSynchronize(pending_stream_);
+  if (detached_) cudaEventSynchronize(det_ev_);
+  if (det_ev_) cudaEventDestroy(det_ev_);
+  for (HostStage& st : stage_)
+    for (int k = 0; k < 2; ++k) {
+      if (st.ev[k]) {
+        cudaEventSynchronize(st.ev[k]);
+        cudaEventDestroy(st.ev[k]);
+      }
+      if (st.p[k]) cudaFreeHost(st.p[k]);
+    }
   drop_graph();
   for (auto& s : scenes_) free_scene(*s);
   dfree(d_scenes_);
   dfree(d_coll_);
   dfree(d_ctr_);
-  if (h_ctr_) cudaFreeHost(h_ctr_);
+  if (h_ctr_buf_) cudaFreeHost(h_ctr_buf_);
   free_particle_buffers();
   free_grid();
   free_bins();
@@ -245,7 +256,20 @@ Batch::~Batch() {
     }
     if (pinned_[k]) cudaFreeHost(pinned_[k]);
   }
+  defer_free_ = false;
+  flush_released();
   if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+void Batch::release_ptr(void* p) {
+  if (!p) return;
+  if (defer_free_) released_.push_back(p);
+  else cudaFree(p);
+}
+
+void Batch::flush_released() {
+  for (void* p : released_) cudaFree(p);
+  released_.clear();
 }
 
 void Batch::free_scene(Scene& s) {
@@ -289,21 +313,21 @@ void Batch::restore(int32_t id, cudaStream_t s) {
 
 void Batch::free_particle_buffers() {
   for (int k = 0; k < 2; ++k) {
-    dfree(keys_[k]);
-    dfree(vals_[k]);
+    release(keys_[k]);
+    release(vals_[k]);
   }
-  dfree(hist_);
-  dfree(fixups_);
-  dfree(digit_total_);
+  release(hist_);
+  release(fixups_);
+  release(digit_total_);
   cap_p_ = 0;
 }
 
 void Batch::free_bins() {
-  dfree(bins_);
-  dfree(bin_off_);
-  dfree(occ_);
-  dfree(idmap_);
-  dfree(bin_state_);
+  release(bins_);
+  release(bin_off_);
+  release(occ_);
+  release(idmap_);
+  release(bin_state_);
   cap_bins_ = 0;
 }
 
@@ -320,7 +344,10 @@ void Batch::ensure_bins(int64_t bins) {
   bin_state_ = dalloc<unsigned long long>((size_t)(bins / kBinTile + 1));
   cap_bins_ = bins;
   bins_dirty_ = true;
-  boxes_dirty_ = true;  // the next step's counts G2P emitted into the old bins are gone
+  // the next step's counts G2P emitted into the old bins are gone: a fresh key
+  // space (and a re-measure unless the caller sizes the bins)
+  keyspace_ready_ = false;
+  if (!host_sized_) boxes_dirty_ = true;
 }
 
 // Chooses the sort for the coming steps: dense bins with 2x headroom over
@@ -343,11 +370,11 @@ void Batch::size_dense(int64_t key_blocks, cudaStream_t s) {
 }
 
 void Batch::free_grid() {
-  dfree(htab_);
-  dfree(blk_);
-  dfree(acc_);
-  dfree(vel_);
-  dfree(item_hdr_);
+  release(htab_);
+  release(blk_);
+  release(acc_);
+  release(vel_);
+  release(item_hdr_);
   cap_items_ = 0;
   cap_blocks_ = 0;
   hcap_ = 0;
@@ -366,7 +393,7 @@ Scene* Batch::find(int32_t id) {
 
 void Batch::ensure_staging(int64_t n) {
   if (n <= staging_cap_) return;
-  dfree(staging_);
+  release(staging_);
   staging_ = dalloc<double>((size_t)std::max<int64_t>(n, 1) * 26);
   staging_cap_ = n;
 }
@@ -571,13 +598,13 @@ void Batch::reserve(int64_t particles, int64_t staging, int scenes, int collider
   if (staging > 0) ensure_staging(staging);
   if (!d_tmp_scene_) d_tmp_scene_ = dalloc<SceneDev>(1);
   if (scenes > d_scenes_cap_) {
-    dfree(d_scenes_);
+    release(d_scenes_);
     d_scenes_cap_ = scenes;
     d_scenes_ = dalloc<SceneDev>(d_scenes_cap_);
     dirty_ = true;  // the tables are written again before the next step
   }
   if (colliders > d_coll_cap_) {
-    dfree(d_coll_);
+    release(d_coll_);
     d_coll_cap_ = colliders;
     d_coll_ = dalloc<Collider>(d_coll_cap_);
     dirty_ = true;
@@ -588,8 +615,10 @@ void Batch::ensure_particle_buffers(int64_t total) {
   if (total <= cap_p_) return;
   free_particle_buffers();
   // The next step's keys G2P emitted lived in the old buffers: the next step
-  // measures the boxes and computes every key again.
-  boxes_dirty_ = true;
+  // computes every key again (a fresh key space), and measures the boxes
+  // again unless the caller sizes the grid and bins (host-sized).
+  keyspace_ready_ = false;
+  if (!host_sized_) boxes_dirty_ = true;
   const int64_t cap = std::max<int64_t>(total, 1024);
   for (int k = 0; k < 2; ++k) {
     keys_[k] = dalloc<uint32_t>((size_t)cap);
@@ -607,7 +636,7 @@ void Batch::ensure_particle_buffers(int64_t total) {
 void Batch::ensure_items() {
   const int64_t need = cap_p_ / chunk_ + cap_blocks_ + 64;
   if (need <= cap_items_) return;
-  dfree(item_hdr_);
+  release(item_hdr_);
   item_hdr_ = dalloc<BlockHeader>((size_t)need);
   cap_items_ = (int32_t)need;
 }
@@ -627,8 +656,11 @@ void Batch::ensure_grid(int64_t blocks) {
   blk_ = dalloc<int4>((size_t)cap);
   acc_ = dalloc<unsigned char>((size_t)cap * 64 * kAccCh * rsize_);
   vel_ = dalloc<unsigned char>((size_t)cap * 64 * kVelCh * rsize_);
-  check_cuda(cudaMemset(acc_, 0, (size_t)cap * 64 * kAccCh * rsize_), "cudaMemset");
-  check_cuda(cudaMemset(vel_, 0, (size_t)cap * 64 * kVelCh * rsize_), "cudaMemset");
+  // zeroed on the batch's own stream and waited for alone: launches left in
+  // flight on other streams (which use the old grid) are not waited for
+  check_cuda(cudaMemsetAsync(acc_, 0, (size_t)cap * 64 * kAccCh * rsize_, own_stream_), "cudaMemset");
+  check_cuda(cudaMemsetAsync(vel_, 0, (size_t)cap * 64 * kVelCh * rsize_, own_stream_), "cudaMemset");
+  check_cuda(cudaStreamSynchronize(own_stream_), "cudaMemset");
   ensure_items();
 }
 
@@ -696,23 +728,17 @@ void Batch::prepare(cudaStream_t s) {
     }
   }
   if ((int)table_.size() > d_scenes_cap_) {
-    dfree(d_scenes_);
+    release(d_scenes_);
     d_scenes_cap_ = std::max<int>(16, (int)table_.size() * 2);
     d_scenes_ = dalloc<SceneDev>(d_scenes_cap_);
   }
   if ((int)coll_.size() > d_coll_cap_ || !d_coll_) {
-    dfree(d_coll_);
+    release(d_coll_);
     d_coll_cap_ = std::max<int>(16, (int)coll_.size() * 2);
     d_coll_ = dalloc<Collider>(d_coll_cap_);
   }
-  if (!table_.empty())
-    check_cuda(cudaMemcpyAsync(d_scenes_, table_.data(), table_.size() * sizeof(SceneDev),
-                               cudaMemcpyHostToDevice, s),
-               "scene table");
-  if (!coll_.empty())
-    check_cuda(cudaMemcpyAsync(d_coll_, coll_.data(), coll_.size() * sizeof(Collider),
-                               cudaMemcpyHostToDevice, s),
-               "colliders");
+  if (!table_.empty()) staged_upload(stage_[0], d_scenes_, table_.data(), table_.size() * sizeof(SceneDev), s, "scene table");
+  if (!coll_.empty()) staged_upload(stage_[1], d_coll_, coll_.data(), coll_.size() * sizeof(Collider), s, "colliders");
   ensure_particle_buffers(total_);
   const BatchDev b = dev(d_scenes_, (int)table_.size(), total_);
   if (prec_ == SNOW_FP64)
@@ -911,14 +937,54 @@ void Batch::step_complete() {
   if (!pending_) return;
   pending_ = false;
   check_cuda(cudaStreamSynchronize(pending_stream_), "step");
-  last_status_ = h_ctr_->status;
-  last_blocks_ = (int64_t)h_ctr_->last_blocks;
-  last_key_blocks_ = (int64_t)h_ctr_->key_blocks;
+  detached_ = false;  // the stream sync covered a launch left behind too
+  absorb(*h_ctr_);
+}
+
+void Batch::step_detach() {
+  if (!pending_) return;
+  if (detached_) complete_detached();
+  if (!det_ev_) check_cuda(cudaEventCreateWithFlags(&det_ev_, cudaEventDisableTiming), "cudaEventCreate");
+  check_cuda(cudaEventRecord(det_ev_, pending_stream_), "cudaEventRecord");
+  det_ctr_ = h_ctr_;
+  h_ctr_ = h_ctr_ == h_ctr_buf_ ? h_ctr_buf_ + 1 : h_ctr_buf_;
+  detached_ = true;
+  pending_ = false;
+}
+
+void Batch::complete_detached() {
+  if (!detached_) return;
+  detached_ = false;
+  check_cuda(cudaEventSynchronize(det_ev_), "step");
+  absorb(*det_ctr_);
+}
+
+void Batch::absorb(const Counters& c) {
+  last_status_ = c.status;
+  last_blocks_ = (int64_t)c.last_blocks;
+  last_key_blocks_ = (int64_t)c.key_blocks;
   // Keep 2x headroom: grow the grid and the bins before the next call if the
   // last step came close.
   if (last_blocks_ * 2 > cap_blocks_) boxes_dirty_ = true;
   if (dense_ && last_key_blocks_ * 64 * 2 > cap_bins_) boxes_dirty_ = true;
   check_status();
+}
+
+void Batch::staged_upload(HostStage& st, void* dst, const void* src, size_t bytes, cudaStream_t s, const char* what) {
+  const int k = st.next;
+  st.next ^= 1;
+  if (st.ev[k]) check_cuda(cudaEventSynchronize(st.ev[k]), what);  // its last copy has passed
+  else check_cuda(cudaEventCreateWithFlags(&st.ev[k], cudaEventDisableTiming), "cudaEventCreate");
+  if (st.cap[k] < bytes) {
+    if (st.p[k]) cudaFreeHost(st.p[k]);
+    st.p[k] = nullptr;
+    st.cap[k] = 0;
+    check_cuda(cudaMallocHost(&st.p[k], 2 * bytes), "cudaMallocHost");
+    st.cap[k] = 2 * bytes;
+  }
+  std::memcpy(st.p[k], src, bytes);
+  check_cuda(cudaMemcpyAsync(dst, st.p[k], bytes, cudaMemcpyHostToDevice, s), what);
+  check_cuda(cudaEventRecord(st.ev[k], s), what);
 }
 
 void Batch::check_status() {

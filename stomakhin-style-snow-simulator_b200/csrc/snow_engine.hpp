@@ -91,6 +91,18 @@ class Batch {
   void step(int n_steps, snow_step_timings* timings, cudaStream_t s);
   void step_launch(int n_steps, snow_step_timings* timings, cudaStream_t s);
   void step_complete();
+  // Leaves the launched steps in flight without waiting for them, so that
+  // scenes can join and leave and the next steps be launched behind them on
+  // the same stream (their status goes to a second counter slot);
+  // complete_detached() waits for them and checks their status.  At most one
+  // launch is left behind: detaching another first completes it.
+  void step_detach();
+  void complete_detached();
+  // Deferred frees: buffers that growth replaces are kept until
+  // flush_released() instead of freed at once (a cudaFree waits for the whole
+  // device, launches left in flight included, which may still read them).
+  void set_deferred_free(bool on) { defer_free_ = on; }
+  void flush_released();
   int32_t adopt_scene(Batch& from, int32_t id);
   // Sizes the particle-indexed step buffers for `particles` in total, the
   // host-transfer staging for scenes of up to `staging` particles and the
@@ -225,6 +237,30 @@ class Batch {
   bool keyspace_ready_ = false;  // the device holds the next step's key boxes
   bool pending_ = false;  // steps launched, status not read yet
   cudaStream_t pending_stream_ = nullptr;
+  bool detached_ = false;  // steps left in flight by step_detach()
+  cudaEvent_t det_ev_ = nullptr;
+  Counters* det_ctr_ = nullptr;  // their counter slot
+  void absorb(const Counters& c);
+  bool defer_free_ = false;
+  std::vector<void*> released_;
+  void release_ptr(void* p);
+  template <typename T>
+  void release(T*& p) {
+    release_ptr((void*)p);
+    p = nullptr;
+  }
+  // Page-locked staging of the scene and collider tables prepare() uploads,
+  // two per table used in turn, each reused only once its last copy passed:
+  // an upload queued behind a detached launch reads one while the next
+  // prepare() writes the other.
+  struct HostStage {
+    void* p[2] = {nullptr, nullptr};
+    size_t cap[2] = {0, 0};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int next = 0;
+  };
+  HostStage stage_[2];
+  void staged_upload(HostStage& st, void* dst, const void* src, size_t bytes, cudaStream_t s, const char* what);
   int64_t total_ = 0;
   int num_dev_scenes_ = 0;
 
@@ -234,7 +270,8 @@ class Batch {
   Collider* d_coll_ = nullptr;
   int d_coll_cap_ = 0;
   Counters* d_ctr_ = nullptr;
-  Counters* h_ctr_ = nullptr;
+  Counters* h_ctr_ = nullptr;      // the slot the next launch's counters go to
+  Counters* h_ctr_buf_ = nullptr;  // two page-locked slots
 
   uint32_t* keys_[2] = {nullptr, nullptr};
   uint32_t* vals_[2] = {nullptr, nullptr};

@@ -102,7 +102,7 @@ class Server {
       if (r->pinned) cudaHostUnregister(r->records.data());
       if (r->done) cudaEventDestroy(r->done);
     }
-    for (cudaEvent_t e : {ev_base_, ev_start_, ev_end_})
+    for (cudaEvent_t e : {ev_base_, ev_start_[0], ev_start_[1], ev_end_[0], ev_end_[1]})
       if (e) cudaEventDestroy(e);
     if (main_s_) cudaStreamDestroy(main_s_);
     if (admit_s_stream_) cudaStreamDestroy(admit_s_stream_);
@@ -184,13 +184,15 @@ class Server {
   // (a cudaMalloc or cudaFree inside it can wait for the tick in flight).
   // Requests submitted while it runs are reserved for between ticks
   // (grow_for), in doublings, and their particle buffers allocated while a
-  // tick runs (carve_for).  Each pass launches a tick of steps for
-  // the live scenes, then, while it runs, issues the setup of newly arrived
-  // requests in a second batch on a second stream and the result copies of
-  // finished scenes on a third, without waiting for either; after the tick it
-  // moves the set-up scenes whose work has passed into the live batch
-  // (without copying their particles), finished scenes out of it, and
-  // releases scenes whose results have arrived.
+  // tick runs (carve_for).  Each pass leaves the tick launched by the last
+  // pass in flight, moves the scenes that finish with it out of the live batch
+  // (their result copies queued on a third stream behind it) and the set-up
+  // scenes whose work has passed into it (without copying their particles),
+  // and queues the next tick behind the one in flight on the same stream;
+  // then, while the ticks run, it issues the setup of newly arrived requests
+  // in a second batch on a second stream, releases scenes whose results have
+  // arrived, and last waits for the older tick.  The device thus finds the
+  // next tick queued when one ends.
   void run(cudaStream_t s) {
     std::vector<Request*> order;
     {
@@ -213,15 +215,43 @@ class Server {
     std::stable_sort(order.begin(), order.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
     std::deque<Request*> pending(order.begin(), order.end());
     std::vector<Request*> live, admitting, leaving, carve;
+    // the tick in flight: launched by the last pass, completed by this one
+    struct Flight {
+      bool on = false;
+      int64_t k = 0;
+      int ev = 0;  // its pair of ev_start_ / ev_end_
+      snow_server_tick tick{};
+    } flying;
+    int ev_next = 0;
     int64_t used = 0;
     ticks_log_.clear();
     bool base_recorded = false;
     double t_phase = now();
     batch_.set_chunk(work_item_ ? work_item_ : auto_work_item(order));
     batch_.set_host_sized(true);
+    // buffers that a reservation replaces while ticks, setups or result copies
+    // are in flight stay allocated until the loop is idle (a cudaFree would
+    // wait for the whole device)
+    struct Released {
+      Server* sv;
+      void flush() {
+        for (Batch* b : {&sv->batch_, &sv->admit_, &sv->retired_}) b->flush_released();
+      }
+      ~Released() {
+        flush();
+        for (Batch* b : {&sv->batch_, &sv->admit_, &sv->retired_}) b->set_deferred_free(false);
+      }
+    } released{this};
+    for (Batch* b : {&batch_, &admit_, &retired_}) b->set_deferred_free(true);
     reserve(order, s);
     admit_s_ += now() - t_phase;
     for (;;) {
+      // The tick launched by the last pass stays in flight while this pass
+      // reserves for new requests, moves scenes in and out and queues the next
+      // tick behind it on the same stream; only then does the host wait for
+      // the older tick, so the device runs tick after tick without a gap for
+      // the host's work.
+      batch_.step_detach();
       // requests submitted since the last pass join the queue in arrival order
       std::vector<Request*> fresh;
       bool more_may_come;
@@ -241,35 +271,83 @@ class Server {
         pending.swap(merged);
         admit_s_ += now() - t_phase;
       }
-      if (pending.empty() && live.empty() && admitting.empty() && leaving.empty()) {
+      if (pending.empty() && live.empty() && admitting.empty() && leaving.empty() && !flying.on) {
         if (!more_may_come) break;
+        released.flush();  // idle: nothing in flight reads the replaced buffers
         std::unique_lock<std::mutex> lk(mu_);
         cv_.wait_for(lk, std::chrono::milliseconds(5),
                      [&] { return !incoming_.empty() || closed_ || !streaming_; });
         continue;
       }
-      // launch this tick (the steps run while the host admits and retires below)
-      int64_t k = 0;
+      // scenes that finish with the tick in flight leave the live batch now
+      // (without a copy); their results are copied back on the retire stream
+      // once that tick has passed, while the next one runs
       t_phase = now();
-      snow_server_tick tick{};
-      tick.host_start_s = t_phase;
-      if (!live.empty()) {
-        k = max_tick_;
-        for (Request* r : live) {
-          k = std::min(k, r->remaining);
-          tick.particles += (int64_t)r->records.size() / 26;
+      int64_t admitted_now = 0;
+      for (size_t i = 0; i < live.size();) {
+        Request* r = live[i];
+        if (r->remaining > 0) {
+          ++i;
+          continue;
         }
+        r->scene = retired_.adopt_scene(batch_, r->scene);
+        if (flying.on) check_cuda(cudaStreamWaitEvent(retire_stream(), ev_end_[flying.ev], 0), "cudaStreamWaitEvent");
+        retired_.download(r->scene, r->records.data(), (int64_t)r->records.size() / 26, retire_stream(),
+                          /*wait=*/!r->pinned);
+        check_cuda(cudaEventRecord(r->done, retire_stream()), "cudaEventRecord");
+        leaving.push_back(r);
+        live.erase(live.begin() + i);
+      }
+      retire_s_ += now() - t_phase;
+      // set-up scenes join the live batch
+      t_phase = now();
+      bool joined = false;
+      for (size_t i = 0; i < admitting.size();) {
+        Request* r = admitting[i];
+        const cudaError_t q = cudaEventQuery(r->done);
+        if (q == cudaErrorNotReady) {
+          ++i;
+          continue;
+        }
+        check_cuda(q, "admission");
+        if (!joined) admit_.collect_status();  // flags of every setup that has passed
+        joined = true;
+        r->scene = batch_.adopt_scene(admit_, r->scene);
+        live.push_back(r);
+        admitting.erase(admitting.begin() + i);
+        ++admitted_now;
+      }
+      admit_s_ += now() - t_phase;
+      // launch the next tick (it runs while the host admits and retires below)
+      Flight next;
+      t_phase = now();
+      int64_t k = max_tick_;
+      for (Request* r : live) k = std::min(k, r->remaining);
+      if (!live.empty() && k > 0) {
+        next.on = true;
+        next.k = k;
+        next.ev = ev_next;
+        ev_next ^= 1;
+        next.tick.host_start_s = t_phase;
+        next.tick.steps = k;
+        next.tick.scenes = (int64_t)live.size();
+        next.tick.admitted = admitted_now;
+        for (Request* r : live) next.tick.particles += (int64_t)r->records.size() / 26;
         if (!base_recorded) {
           check_cuda(cudaEventRecord(ev_base_, s), "cudaEventRecord");
           base_recorded = true;
         }
-        check_cuda(cudaEventRecord(ev_start_, s), "cudaEventRecord");
+        check_cuda(cudaEventRecord(ev_start_[next.ev], s), "cudaEventRecord");
         batch_.step_launch((int)k, nullptr, s);
-        check_cuda(cudaEventRecord(ev_end_, s), "cudaEventRecord");
+        check_cuda(cudaEventRecord(ev_end_[next.ev], s), "cudaEventRecord");
+        for (Request* r : live) {
+          r->remaining -= k;
+          next.tick.retired += r->remaining == 0;  // these finish with this tick
+        }
       }
       step_s_ += now() - t_phase;
       // particle buffers for the requests that arrived since the last pass,
-      // allocated while the tick runs
+      // allocated while the ticks run
       t_phase = now();
       if (!carve.empty()) {
         carve_for(carve);
@@ -303,74 +381,35 @@ class Server {
       t_phase = now();
       collect_results(leaving, used, now, false);
       retire_s_ += now() - t_phase;
-      // complete the tick
-      if (k > 0) {
+      // complete the older tick; the new one is queued behind it
+      if (flying.on) {
         t_phase = now();
-        batch_.step_complete();
-        step_s_ += now() - t_phase;
-        ++ticks_;
-        for (Request* r : live) {
-          r->remaining -= k;
-          particle_steps_ += k * ((int64_t)r->records.size() / 26);
-        }
+        batch_.complete_detached();
+        check_cuda(cudaEventSynchronize(ev_end_[flying.ev]), "cudaEventSynchronize");
         float a = 0.f, b = 0.f;
-        check_cuda(cudaEventSynchronize(ev_end_), "cudaEventSynchronize");
-        check_cuda(cudaEventElapsedTime(&a, ev_base_, ev_start_), "cudaEventElapsedTime");
-        check_cuda(cudaEventElapsedTime(&b, ev_base_, ev_end_), "cudaEventElapsedTime");
-        tick.host_end_s = now();
-        tick.device_start_s = a * 1e-3;
-        tick.device_end_s = b * 1e-3;
-        tick.steps = k;
-        tick.scenes = (int64_t)live.size();
+        check_cuda(cudaEventElapsedTime(&a, ev_base_, ev_start_[flying.ev]), "cudaEventElapsedTime");
+        check_cuda(cudaEventElapsedTime(&b, ev_base_, ev_end_[flying.ev]), "cudaEventElapsedTime");
+        flying.tick.host_end_s = now();
+        flying.tick.device_start_s = a * 1e-3;
+        flying.tick.device_end_s = b * 1e-3;
+        ++ticks_;
+        particle_steps_ += flying.k * flying.tick.particles;
+        ticks_log_.push_back(flying.tick);
+        step_s_ += now() - t_phase;
       }
-      if (live.empty() && !admitting.empty())  // nothing to step: wait for the first setup
+      flying = next;
+      if (!flying.on && live.empty() && !admitting.empty())  // nothing to step: wait for the first setup
         check_cuda(cudaEventSynchronize(admitting.front()->done), "cudaEventSynchronize");
-      // set-up scenes join the live batch
-      t_phase = now();
-      bool joined = false;
-      for (size_t i = 0; i < admitting.size();) {
-        Request* r = admitting[i];
-        const cudaError_t q = cudaEventQuery(r->done);
-        if (q == cudaErrorNotReady) {
-          ++i;
-          continue;
-        }
-        check_cuda(q, "admission");
-        if (!joined) admit_.collect_status();  // flags of every setup that has passed
-        joined = true;
-        r->scene = batch_.adopt_scene(admit_, r->scene);
-        live.push_back(r);
-        admitting.erase(admitting.begin() + i);
-        ++tick.admitted;
-      }
-      admit_s_ += now() - t_phase;
-      // finished scenes leave the live batch without a copy; their results are
-      // copied back on the retire stream while the next tick runs
-      t_phase = now();
-      for (size_t i = 0; i < live.size();) {
-        Request* r = live[i];
-        if (r->remaining > 0) {
-          ++i;
-          continue;
-        }
-        r->scene = retired_.adopt_scene(batch_, r->scene);
-        retired_.download(r->scene, r->records.data(), (int64_t)r->records.size() / 26, retire_stream(),
-                          /*wait=*/!r->pinned);
-        check_cuda(cudaEventRecord(r->done, retire_stream()), "cudaEventRecord");
-        leaving.push_back(r);
-        live.erase(live.begin() + i);
-        ++tick.retired;
-      }
-      if (live.empty() && admitting.empty()) {
+      if (!flying.on && live.empty() && admitting.empty()) {
         // nothing runs: finish the copies back, or wait for the next arrival
+        t_phase = now();
         collect_results(leaving, used, now, true);
         if (!pending.empty()) {
           const double wait = pending.front()->arrival - now();
           if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
         }
+        retire_s_ += now() - t_phase;
       }
-      retire_s_ += now() - t_phase;
-      if (k > 0) ticks_log_.push_back(tick);
     }
     wall_ += now();
   }
@@ -483,7 +522,8 @@ class Server {
   };
 
   // Reserves `need` (capped by the budget and the scene slots) in the live,
-  // admission and retirement batches.  Called with no tick in flight.
+  // admission and retirement batches.  A tick may be in flight (detached from
+  // the live batch): it keeps the buffers it was launched with.
   void reserve_need(const Need& need, cudaStream_t s, bool carve_scenes) {
     const int64_t live_n = std::min(need.live_n, budget_ / per_particle_bytes());
     const int slots = (int)std::min<int64_t>(need.slots, max_scenes_);
@@ -494,8 +534,9 @@ class Server {
     admit_.reserve_grid(need.grid_max, need.box_max, admit_stream());
     if (carve_scenes) admit_.reserve_scenes(need.sizes, budget_);
     retired_.reserve(0, need.scene_max);
-    check_cuda(cudaStreamSynchronize(s), "reserve");
-    check_cuda(cudaStreamSynchronize(admit_stream()), "reserve");
+    // no wait: the clears above are ordered on the streams that use the new
+    // buffers, and the replaced ones stay allocated (deferred frees) while
+    // the ticks, setups and copies in flight still read them
     reserved_ = need;
     ++reservations_;
   }
@@ -507,7 +548,7 @@ class Server {
   void reserve(const std::vector<Request*>& order, cudaStream_t s) {
     admit_stream();
     retire_stream();
-    for (cudaEvent_t* e : {&ev_base_, &ev_start_, &ev_end_})
+    for (cudaEvent_t* e : {&ev_base_, &ev_start_[0], &ev_start_[1], &ev_end_[0], &ev_end_[1]})
       if (!*e) check_cuda(cudaEventCreate(e), "cudaEventCreate");
     Need need;
     for (Request* r : order)
@@ -582,7 +623,7 @@ class Server {
   Batch admit_;    // new scenes are set up here while batch_ steps
   Batch retired_;  // finished scenes are copied back from here while batch_ steps
   cudaStream_t main_s_ = nullptr, admit_s_stream_ = nullptr, retire_s_stream_ = nullptr;
-  cudaEvent_t ev_base_ = nullptr, ev_start_ = nullptr, ev_end_ = nullptr;
+  cudaEvent_t ev_base_ = nullptr, ev_start_[2] = {nullptr, nullptr}, ev_end_[2] = {nullptr, nullptr};
   std::vector<snow_server_tick> ticks_log_;
   int prec_;
   int64_t budget_;
