@@ -252,8 +252,8 @@ def timed_steps(batch, steps, sp, torch) -> float:
 def copy_bound(torch, host, n: int, rate: float) -> dict:
     """The host-link bound of one drop-in call: the same record bytes copied
     host -> device and back from the same page-locked buffer, with no step
-    between (best of three, CUDA events), and the share of the measured call
-    time it takes."""
+    between (best of three, CUDA events), the share of the measured call time
+    it takes, and the link rate of the two copies (bytes moved / their time)."""
     dev = torch.empty(host.shape, dtype=torch.float64, device="cuda")
     src = torch.from_numpy(host)
     best = float("inf")
@@ -268,7 +268,7 @@ def copy_bound(torch, host, n: int, rate: float) -> dict:
         best = min(best, e0.elapsed_time(e1))
     call_ms = 1e3 * n / rate
     return {"copy_only_ms": best, "call_ms": call_ms, "copy_share_of_call": best / call_ms,
-            "link_gbs_each_way": 2 * host.nbytes / (best * 1e-3) / 2e9}
+            "link_gbs": 2 * host.nbytes / (best * 1e-3) / 1e9}
 
 
 def plain_fp64_rate(snow_b200, torch, sp, items, settle: int = 0) -> float:
