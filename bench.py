@@ -338,10 +338,13 @@ def tick_summary(ticks, wall_s: float) -> dict:
         return {}
     busy = sum(t["device_end_s"] - t["device_start_s"] for t in ticks)
     gaps = [b["device_start_s"] - a["device_end_s"] for a, b in zip(ticks, ticks[1:])]
+    big = [g for g in gaps if g > 1e-3]
     return {"device_busy_frac": busy / wall_s if wall_s > 0 else None,
             "mean_steps_per_tick": sum(t["steps"] for t in ticks) / len(ticks),
             "mean_tick_device_ms": 1e3 * busy / len(ticks),
-            "mean_gap_ms": 1e3 * sum(gaps) / len(gaps) if gaps else 0.0}
+            "mean_gap_ms": 1e3 * sum(gaps) / len(gaps) if gaps else 0.0,
+            "median_gap_ms": 1e3 * statistics.median(gaps) if gaps else 0.0,
+            "gaps_over_1ms": len(big), "gap_ms_in_those": 1e3 * sum(big)}
 
 
 def measure_served(snow_b200, torch, sp, count: int, fp64_rate: float | None = None, grounded: bool = False,
@@ -371,7 +374,8 @@ def measure_served(snow_b200, torch, sp, count: int, fp64_rate: float | None = N
            "rejected": med["rejected"], "peak_concurrent_scenes": med["peak_scenes"], "ticks": med["ticks"],
            "reservations": med["reservations"], "wall_s": med["wall_s"],
            "ticks_summary": {k: med.get(k) for k in ("device_busy_frac", "mean_steps_per_tick",
-                                                     "mean_tick_device_ms", "mean_gap_ms")},
+                                                     "mean_tick_device_ms", "mean_gap_ms", "median_gap_ms",
+                                                     "gaps_over_1ms", "gap_ms_in_those")},
            "host_phases_s": {"admit": med["admit_s"], "step": med["step_s"], "retire": med["retire_s"]}}
     if fp64_rate:
         out["served_vs_plain_fp64_headline"] = med["particle_steps_per_s"] / fp64_rate
@@ -1044,7 +1048,8 @@ def run_served(args, ws, rank, local):
                        "submission": "streaming"},
             "rank0": {k: st.get(k) for k in ("p50_s", "p99_s", "mean_s", "completed", "ticks", "peak_scenes",
                                               "reservations", "particle_steps_per_s", "device_busy_frac",
-                                              "mean_steps_per_tick", "mean_tick_device_ms", "mean_gap_ms")},
+                                              "mean_steps_per_tick", "mean_tick_device_ms", "mean_gap_ms",
+                                              "median_gap_ms", "gaps_over_1ms", "gap_ms_in_those")},
             "clocks": clk}
     if dist is not None:
         dist.barrier()
