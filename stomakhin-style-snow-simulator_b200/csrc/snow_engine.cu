@@ -218,18 +218,21 @@ Batch::Batch(int precision) : prec_(precision) {
   rsize_ = precision == SNOW_FP64 ? sizeof(double) : sizeof(float);
   d_ctr_ = dalloc<Counters>(1);
   check_cuda(cudaMemset(d_ctr_, 0, sizeof(Counters)), "cudaMemset");
-  check_cuda(cudaMallocHost((void**)&h_ctr_buf_, 2 * sizeof(Counters)), "cudaMallocHost");
-  std::memset(h_ctr_buf_, 0, 2 * sizeof(Counters));
+  check_cuda(cudaMallocHost((void**)&h_ctr_buf_, kCtrSlots * sizeof(Counters)), "cudaMallocHost");
+  std::memset(h_ctr_buf_, 0, kCtrSlots * sizeof(Counters));
   h_ctr_ = h_ctr_buf_;
   check_cuda(cudaStreamCreate(&own_stream_), "cudaStreamCreate");
 }
 
 Batch::~Batch() {
   if (pending_) cudaStreamSynchronize(pending_stream_);
-  if (detached_) cudaEventSynchronize(det_ev_);
-  if (det_ev_) cudaEventDestroy(det_ev_);
+  for (const Detached& d : detached_) {
+    cudaEventSynchronize(d.ev);
+    cudaEventDestroy(d.ev);
+  }
+  for (cudaEvent_t e : det_events_) cudaEventDestroy(e);
   for (HostStage& st : stage_)
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kStageBufs; ++k) {
       if (st.ev[k]) {
         cudaEventSynchronize(st.ev[k]);
         cudaEventDestroy(st.ev[k]);
@@ -937,26 +940,44 @@ void Batch::step_complete() {
   if (!pending_) return;
   pending_ = false;
   check_cuda(cudaStreamSynchronize(pending_stream_), "step");
-  detached_ = false;  // the stream sync covered a launch left behind too
+  // the stream sync covered the launches left behind too
+  for (const Detached& d : detached_) det_events_.push_back(d.ev);
+  detached_.clear();
   absorb(*h_ctr_);
 }
 
 void Batch::step_detach() {
   if (!pending_) return;
-  if (detached_) complete_detached();
-  if (!det_ev_) check_cuda(cudaEventCreateWithFlags(&det_ev_, cudaEventDisableTiming), "cudaEventCreate");
-  check_cuda(cudaEventRecord(det_ev_, pending_stream_), "cudaEventRecord");
-  det_ctr_ = h_ctr_;
-  h_ctr_ = h_ctr_ == h_ctr_buf_ ? h_ctr_buf_ + 1 : h_ctr_buf_;
-  detached_ = true;
+  if ((int)detached_.size() >= kCtrSlots - 1) complete_detached();
+  cudaEvent_t ev = nullptr;
+  if (!det_events_.empty()) {
+    ev = det_events_.back();
+    det_events_.pop_back();
+  } else {
+    check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  check_cuda(cudaEventRecord(ev, pending_stream_), "cudaEventRecord");
+  detached_.push_back(Detached{ev, h_ctr_});
+  // the next launch's counters go to a slot no launch in flight writes
+  for (int k = 0; k < kCtrSlots; ++k) {
+    Counters* c = h_ctr_buf_ + k;
+    bool used = false;
+    for (const Detached& d : detached_) used |= d.ctr == c;
+    if (!used) {
+      h_ctr_ = c;
+      break;
+    }
+  }
   pending_ = false;
 }
 
 void Batch::complete_detached() {
-  if (!detached_) return;
-  detached_ = false;
-  check_cuda(cudaEventSynchronize(det_ev_), "step");
-  absorb(*det_ctr_);
+  if (detached_.empty()) return;
+  const Detached d = detached_.front();
+  detached_.pop_front();
+  det_events_.push_back(d.ev);
+  check_cuda(cudaEventSynchronize(d.ev), "step");
+  absorb(*d.ctr);
 }
 
 void Batch::absorb(const Counters& c) {
@@ -972,7 +993,7 @@ void Batch::absorb(const Counters& c) {
 
 void Batch::staged_upload(HostStage& st, void* dst, const void* src, size_t bytes, cudaStream_t s, const char* what) {
   const int k = st.next;
-  st.next ^= 1;
+  st.next = (st.next + 1) % kStageBufs;
   if (st.ev[k]) check_cuda(cudaEventSynchronize(st.ev[k]), what);  // its last copy has passed
   else check_cuda(cudaEventCreateWithFlags(&st.ev[k], cudaEventDisableTiming), "cudaEventCreate");
   if (st.cap[k] < bytes) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <deque>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -93,9 +94,10 @@ class Batch {
   void step_complete();
   // Leaves the launched steps in flight without waiting for them, so that
   // scenes can join and leave and the next steps be launched behind them on
-  // the same stream (their status goes to a second counter slot);
-  // complete_detached() waits for them and checks their status.  At most one
-  // launch is left behind: detaching another first completes it.
+  // the same stream (each launch's status goes to its own counter slot);
+  // complete_detached() waits for the oldest launch left in flight and checks
+  // its status.  At most kCtrSlots - 1 launches are left behind: detaching
+  // another first completes the oldest.
   void step_detach();
   void complete_detached();
   // Deferred frees: buffers that growth replaces are kept until
@@ -237,9 +239,15 @@ class Batch {
   bool keyspace_ready_ = false;  // the device holds the next step's key boxes
   bool pending_ = false;  // steps launched, status not read yet
   cudaStream_t pending_stream_ = nullptr;
-  bool detached_ = false;  // steps left in flight by step_detach()
-  cudaEvent_t det_ev_ = nullptr;
-  Counters* det_ctr_ = nullptr;  // their counter slot
+  // launches left in flight by step_detach(), oldest first: the event after
+  // each and its counter slot
+  struct Detached {
+    cudaEvent_t ev;
+    Counters* ctr;
+  };
+  std::deque<Detached> detached_;
+  std::vector<cudaEvent_t> det_events_;  // events of completed ones, for reuse
+  static constexpr int kCtrSlots = 4;
   void absorb(const Counters& c);
   bool defer_free_ = false;
   std::vector<void*> released_;
@@ -250,13 +258,14 @@ class Batch {
     p = nullptr;
   }
   // Page-locked staging of the scene and collider tables prepare() uploads,
-  // two per table used in turn, each reused only once its last copy passed:
-  // an upload queued behind a detached launch reads one while the next
-  // prepare() writes the other.
+  // kStageBufs per table used in turn, each reused only once its last copy
+  // passed: uploads queued behind detached launches read theirs while the
+  // next prepare() writes another.
+  static constexpr int kStageBufs = 4;
   struct HostStage {
-    void* p[2] = {nullptr, nullptr};
-    size_t cap[2] = {0, 0};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    void* p[kStageBufs] = {};
+    size_t cap[kStageBufs] = {};
+    cudaEvent_t ev[kStageBufs] = {};
     int next = 0;
   };
   HostStage stage_[2];
@@ -271,7 +280,7 @@ class Batch {
   int d_coll_cap_ = 0;
   Counters* d_ctr_ = nullptr;
   Counters* h_ctr_ = nullptr;      // the slot the next launch's counters go to
-  Counters* h_ctr_buf_ = nullptr;  // two page-locked slots
+  Counters* h_ctr_buf_ = nullptr;  // kCtrSlots page-locked slots
 
   uint32_t* keys_[2] = {nullptr, nullptr};
   uint32_t* vals_[2] = {nullptr, nullptr};

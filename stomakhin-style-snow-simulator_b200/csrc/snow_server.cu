@@ -102,8 +102,10 @@ class Server {
       if (r->pinned) cudaHostUnregister(r->records.data());
       if (r->done) cudaEventDestroy(r->done);
     }
-    for (cudaEvent_t e : {ev_base_, ev_start_[0], ev_start_[1], ev_end_[0], ev_end_[1]})
-      if (e) cudaEventDestroy(e);
+    if (ev_base_) cudaEventDestroy(ev_base_);
+    for (int k = 0; k < kTickEvents; ++k)
+      for (cudaEvent_t e : {ev_start_[k], ev_end_[k]})
+        if (e) cudaEventDestroy(e);
     if (main_s_) cudaStreamDestroy(main_s_);
     if (admit_s_stream_) cudaStreamDestroy(admit_s_stream_);
     if (retire_s_stream_) cudaStreamDestroy(retire_s_stream_);
@@ -188,11 +190,12 @@ class Server {
   // pass in flight, moves the scenes that finish with it out of the live batch
   // (their result copies queued on a third stream behind it) and the set-up
   // scenes whose work has passed into it (without copying their particles),
-  // and queues the next tick behind the one in flight on the same stream;
+  // and queues the next tick behind the ones in flight on the same stream;
   // then, while the ticks run, it issues the setup of newly arrived requests
   // in a second batch on a second stream, releases scenes whose results have
-  // arrived, and last waits for the older tick.  The device thus finds the
-  // next tick queued when one ends.
+  // arrived, and last waits for the oldest tick beyond kQueuedTicks.  The
+  // device thus finds ticks queued when one ends, also while a pass of host
+  // work takes longer than a tick.
   void run(cudaStream_t s) {
     std::vector<Request*> order;
     {
@@ -215,13 +218,16 @@ class Server {
     std::stable_sort(order.begin(), order.end(), [](Request* a, Request* b) { return a->arrival < b->arrival; });
     std::deque<Request*> pending(order.begin(), order.end());
     std::vector<Request*> live, admitting, leaving, carve;
-    // the tick in flight: launched by the last pass, completed by this one
+    // ticks in flight, oldest first: up to kQueuedTicks are queued on the
+    // device ahead of the host, so that a pass of host work longer than one
+    // tick does not leave the device idle
     struct Flight {
       bool on = false;
       int64_t k = 0;
       int ev = 0;  // its pair of ev_start_ / ev_end_
       snow_server_tick tick{};
-    } flying;
+    };
+    std::deque<Flight> flights;
     int ev_next = 0;
     int64_t used = 0;
     ticks_log_.clear();
@@ -248,9 +254,9 @@ class Server {
     for (;;) {
       // The tick launched by the last pass stays in flight while this pass
       // reserves for new requests, moves scenes in and out and queues the next
-      // tick behind it on the same stream; only then does the host wait for
-      // the older tick, so the device runs tick after tick without a gap for
-      // the host's work.
+      // tick behind it on the same stream; only then does the host wait, for
+      // the oldest tick beyond the kQueuedTicks it keeps queued, so the device
+      // runs tick after tick without a gap for the host's work.
       batch_.step_detach();
       // requests submitted since the last pass join the queue in arrival order
       std::vector<Request*> fresh;
@@ -271,7 +277,7 @@ class Server {
         pending.swap(merged);
         admit_s_ += now() - t_phase;
       }
-      if (pending.empty() && live.empty() && admitting.empty() && leaving.empty() && !flying.on) {
+      if (pending.empty() && live.empty() && admitting.empty() && leaving.empty() && flights.empty()) {
         if (!more_may_come) break;
         released.flush();  // idle: nothing in flight reads the replaced buffers
         std::unique_lock<std::mutex> lk(mu_);
@@ -291,7 +297,9 @@ class Server {
           continue;
         }
         r->scene = retired_.adopt_scene(batch_, r->scene);
-        if (flying.on) check_cuda(cudaStreamWaitEvent(retire_stream(), ev_end_[flying.ev], 0), "cudaStreamWaitEvent");
+        // their last tick is the newest in flight
+        if (!flights.empty())
+          check_cuda(cudaStreamWaitEvent(retire_stream(), ev_end_[flights.back().ev], 0), "cudaStreamWaitEvent");
         retired_.download(r->scene, r->records.data(), (int64_t)r->records.size() / 26, retire_stream(),
                           /*wait=*/!r->pinned);
         check_cuda(cudaEventRecord(r->done, retire_stream()), "cudaEventRecord");
@@ -327,7 +335,7 @@ class Server {
         next.on = true;
         next.k = k;
         next.ev = ev_next;
-        ev_next ^= 1;
+        ev_next = (ev_next + 1) % kTickEvents;
         next.tick.host_start_s = t_phase;
         next.tick.steps = k;
         next.tick.scenes = (int64_t)live.size();
@@ -381,26 +389,29 @@ class Server {
       t_phase = now();
       collect_results(leaving, used, now, false);
       retire_s_ += now() - t_phase;
-      // complete the older tick; the new one is queued behind it
-      if (flying.on) {
+      // complete the oldest ticks, keeping kQueuedTicks queued behind them
+      // (all of them when this pass queued none: nothing is left to run)
+      if (next.on) flights.push_back(next);
+      while (flights.size() > (next.on ? (size_t)kQueuedTicks : 0)) {
+        Flight& f = flights.front();
         t_phase = now();
         batch_.complete_detached();
-        check_cuda(cudaEventSynchronize(ev_end_[flying.ev]), "cudaEventSynchronize");
+        check_cuda(cudaEventSynchronize(ev_end_[f.ev]), "cudaEventSynchronize");
         float a = 0.f, b = 0.f;
-        check_cuda(cudaEventElapsedTime(&a, ev_base_, ev_start_[flying.ev]), "cudaEventElapsedTime");
-        check_cuda(cudaEventElapsedTime(&b, ev_base_, ev_end_[flying.ev]), "cudaEventElapsedTime");
-        flying.tick.host_end_s = now();
-        flying.tick.device_start_s = a * 1e-3;
-        flying.tick.device_end_s = b * 1e-3;
+        check_cuda(cudaEventElapsedTime(&a, ev_base_, ev_start_[f.ev]), "cudaEventElapsedTime");
+        check_cuda(cudaEventElapsedTime(&b, ev_base_, ev_end_[f.ev]), "cudaEventElapsedTime");
+        f.tick.host_end_s = now();
+        f.tick.device_start_s = a * 1e-3;
+        f.tick.device_end_s = b * 1e-3;
         ++ticks_;
-        particle_steps_ += flying.k * flying.tick.particles;
-        ticks_log_.push_back(flying.tick);
+        particle_steps_ += f.k * f.tick.particles;
+        ticks_log_.push_back(f.tick);
         step_s_ += now() - t_phase;
+        flights.pop_front();
       }
-      flying = next;
-      if (!flying.on && live.empty() && !admitting.empty())  // nothing to step: wait for the first setup
+      if (flights.empty() && live.empty() && !admitting.empty())  // nothing to step: wait for the first setup
         check_cuda(cudaEventSynchronize(admitting.front()->done), "cudaEventSynchronize");
-      if (!flying.on && live.empty() && admitting.empty()) {
+      if (flights.empty() && live.empty() && admitting.empty()) {
         // nothing runs: finish the copies back, or wait for the next arrival
         t_phase = now();
         collect_results(leaving, used, now, true);
@@ -548,8 +559,10 @@ class Server {
   void reserve(const std::vector<Request*>& order, cudaStream_t s) {
     admit_stream();
     retire_stream();
-    for (cudaEvent_t* e : {&ev_base_, &ev_start_[0], &ev_start_[1], &ev_end_[0], &ev_end_[1]})
-      if (!*e) check_cuda(cudaEventCreate(e), "cudaEventCreate");
+    if (!ev_base_) check_cuda(cudaEventCreate(&ev_base_), "cudaEventCreate");
+    for (int k = 0; k < kTickEvents; ++k)
+      for (cudaEvent_t* e : {&ev_start_[k], &ev_end_[k]})
+        if (!*e) check_cuda(cudaEventCreate(e), "cudaEventCreate");
     Need need;
     for (Request* r : order)
       if (r->bytes <= budget_) need.add(*r);
@@ -623,7 +636,11 @@ class Server {
   Batch admit_;    // new scenes are set up here while batch_ steps
   Batch retired_;  // finished scenes are copied back from here while batch_ steps
   cudaStream_t main_s_ = nullptr, admit_s_stream_ = nullptr, retire_s_stream_ = nullptr;
-  cudaEvent_t ev_base_ = nullptr, ev_start_[2] = {nullptr, nullptr}, ev_end_[2] = {nullptr, nullptr};
+  // ticks queued on the device ahead of the host (the engine keeps up to three
+  // launches in flight), and the event pairs of the ticks in flight
+  static constexpr int kQueuedTicks = 2;
+  static constexpr int kTickEvents = kQueuedTicks + 2;
+  cudaEvent_t ev_base_ = nullptr, ev_start_[kTickEvents] = {}, ev_end_[kTickEvents] = {};
   std::vector<snow_server_tick> ticks_log_;
   int prec_;
   int64_t budget_;
