@@ -8,6 +8,8 @@
 #include <charconv>
 #include <cstdint>
 #include <cstring>
+#include <exception>
+#include <fcntl.h>
 #include <fstream>
 #include <iomanip>
 #include <iterator>
@@ -20,6 +22,10 @@
 #include <thread>
 #include <vector>
 
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include "snow/export.hpp"
 #include "snow/import.hpp"
 #include "snow_host_detail.hpp"
@@ -29,9 +35,61 @@ namespace
 {
 std::string read_file(const std::string& filename)
 {
-    std::ifstream file(filename, std::ios::binary);
+    std::ifstream file(filename, std::ios::binary | std::ios::ate);
     if (!file.is_open()) throw std::runtime_error{"File not open: " + filename};
-    return std::string(std::istreambuf_iterator<char>(file), std::istreambuf_iterator<char>());
+    const std::streamoff size = file.tellg();
+    if (size < 0)  // not seekable (a pipe): read it as a stream
+    {
+        file.clear();
+        return std::string(std::istreambuf_iterator<char>(file), std::istreambuf_iterator<char>());
+    }
+    std::string text(static_cast<std::size_t>(size), '\0');
+    file.seekg(0);
+    file.read(text.data(), size);
+    text.resize(static_cast<std::size_t>(file.gcount()));
+    return text;
+}
+
+// Runs parse_line over lines [1, size) (line 0 is the header) in contiguous
+// parts on several threads, each into its own vector, and returns the
+// results in file order.  An exception is rethrown from the first line that
+// raised one in file order -- the one a sequential read stops at -- so the
+// error is the reference's.
+template <typename T, typename F>
+std::vector<T> parse_body(const std::vector<std::string_view>& lines, F&& parse_line)
+{
+    constexpr std::size_t kLinesPerPart = 32768;
+    const std::size_t body = lines.size() - 1;
+    const std::size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const std::size_t parts = std::max<std::size_t>(1, std::min<std::size_t>({hw, 32, body / kLinesPerPart}));
+    std::vector<std::vector<T>> out(parts);
+    std::vector<std::exception_ptr> err(parts);
+    auto work = [&](std::size_t k) {
+        const std::size_t lo = 1 + body * k / parts, hi = 1 + body * (k + 1) / parts;
+        try
+        {
+            out[k].reserve(hi - lo);
+            for (std::size_t i = lo; i < hi; ++i)
+                if (!lines[i].empty()) out[k].push_back(parse_line(lines[i]));
+        }
+        catch (...)
+        {
+            err[k] = std::current_exception();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (std::size_t k = 1; k < parts; ++k) pool.emplace_back(work, k);
+    work(0);
+    for (auto& t : pool) t.join();
+    for (const auto& e : err)
+        if (e) std::rethrow_exception(e);
+    if (parts == 1) return std::move(out[0]);
+    std::size_t total = 0;
+    for (const auto& v : out) total += v.size();
+    std::vector<T> all;
+    all.reserve(total);
+    for (auto& v : out) all.insert(all.end(), v.begin(), v.end());
+    return all;
 }
 
 // Lines as std::getline yields them: split at '\n', no empty final segment.
@@ -132,19 +190,14 @@ std::vector<ParticleSeed> import_particle_seeds(const std::string& filename)
     const std::string text = read_file(filename);
     const auto lines = lines_of(text);
     if (lines.empty()) throw std::runtime_error{"Particle data file is empty: " + filename};
-    std::vector<ParticleSeed> seeds;
-    seeds.reserve(lines.size());
-    for (std::size_t k = 1; k < lines.size(); ++k)
-    {
-        if (lines[k].empty()) continue;
-        Fields row(lines[k]);
+    return parse_body<ParticleSeed>(lines, [](std::string_view line) {
+        Fields row(line);
         const int id = to_int(row.next("group_ID"));
         const double x = to_double(row.next("x"));
         const double y = to_double(row.next("y"));
         const double z = to_double(row.next("z"));
-        seeds.push_back(ParticleSeed{id, Eigen::Vector3d{x, y, z}});
-    }
-    return seeds;
+        return ParticleSeed{id, Eigen::Vector3d{x, y, z}};
+    });
 }
 
 std::vector<Particle> assemble_particles(const std::vector<ParticleSeed>& seeds,
@@ -162,11 +215,167 @@ std::vector<Particle> assemble_particles(const std::vector<ParticleSeed>& seeds,
     return particles;
 }
 
+namespace
+{
+// A file's bytes for parsing: a regular file is mapped read-only, so its pages
+// are read in by the threads that parse them; anything else is read whole.
+class FileBytes
+{
+public:
+    explicit FileBytes(const std::string& filename)
+    {
+        const int fd = ::open(filename.c_str(), O_RDONLY);
+        if (fd < 0) throw std::runtime_error{"File not open: " + filename};
+        struct stat st{};
+        if (::fstat(fd, &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0)
+        {
+            void* m = ::mmap(nullptr, static_cast<std::size_t>(st.st_size), PROT_READ, MAP_PRIVATE, fd, 0);
+            if (m != MAP_FAILED)
+            {
+                map_ = m;
+                size_ = static_cast<std::size_t>(st.st_size);
+            }
+        }
+        ::close(fd);
+        if (!map_) buf_ = read_file(filename);
+    }
+    ~FileBytes()
+    {
+        if (map_) ::munmap(map_, size_);
+    }
+    FileBytes(const FileBytes&) = delete;
+    FileBytes& operator=(const FileBytes&) = delete;
+    std::string_view view() const { return map_ ? std::string_view(static_cast<const char*>(map_), size_) : buf_; }
+
+private:
+    void* map_ = nullptr;
+    std::size_t size_ = 0;
+    std::string buf_;
+};
+}  // namespace
+
+// import_particles (src/import.cpp:131-136) in one parallel pass over
+// particles.csv: the body after the header line is cut into byte ranges at
+// line starts, and each thread parses its lines and builds their particles
+// from the groups into its own vector; the vectors are joined in file order.
+// The errors are the sequential ones: a malformed line anywhere comes before
+// an undefined group id (the reference reads every seed before assembling),
+// and of each kind the first in file order is reported.
 std::vector<Particle> import_particles(const std::string& filename_group, const std::string& filename_particle_seed)
 {
     const auto groups = import_groups(filename_group);
-    const auto seeds = import_particle_seeds(filename_particle_seed);
-    return assemble_particles(seeds, groups);
+    const FileBytes file(filename_particle_seed);
+    const std::string_view text = file.view();
+    if (text.empty()) throw std::runtime_error{"Particle data file is empty: " + filename_particle_seed};
+    const std::size_t header_end = text.find('\n');
+    const std::size_t body = header_end == std::string_view::npos ? text.size() : header_end + 1;
+    // one particle per group, copied for each of its particles
+    std::map<int, Particle> proto;
+    for (const auto& [id, g] : groups) proto.emplace(id, Particle(Eigen::Vector3d::Zero(), g.velocity, g.mass, 0.0));
+
+    constexpr std::size_t kBytesPerPart = std::size_t(1) << 20;
+    const std::size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const std::size_t parts =
+        std::max<std::size_t>(1, std::min<std::size_t>({hw, 32, (text.size() - body) / kBytesPerPart}));
+    std::vector<std::size_t> cut(parts + 1, text.size());
+    cut[0] = body;
+    for (std::size_t k = 1; k < parts; ++k)
+    {
+        std::size_t b = std::max(body + (text.size() - body) * k / parts, cut[k - 1]);
+        if (b > body && b < text.size() && text[b - 1] != '\n')
+        {
+            const std::size_t nl = text.find('\n', b);
+            b = nl == std::string_view::npos ? text.size() : nl + 1;
+        }
+        cut[k] = b;
+    }
+    struct Seed
+    {
+        const Particle* proto;
+        double x, y, z;
+    };
+    struct Part
+    {
+        std::vector<Seed> particles;
+        std::exception_ptr parse_error;
+        bool undefined = false;
+        int undefined_id = 0;
+    };
+    std::vector<Part> out(parts);
+    auto work = [&](std::size_t k) {
+        Part& part = out[k];
+        part.particles.reserve((cut[k + 1] - cut[k]) / 24 + 1);
+        try
+        {
+            for (std::size_t pos = cut[k]; pos < cut[k + 1];)
+            {
+                const std::size_t nl = text.find('\n', pos);
+                const std::size_t end = std::min(nl == std::string_view::npos ? text.size() : nl, cut[k + 1]);
+                const std::string_view line = text.substr(pos, end - pos);
+                pos = end + 1;
+                if (line.empty()) continue;
+                Fields row(line);
+                const int id = to_int(row.next("group_ID"));
+                const double x = to_double(row.next("x"));
+                const double y = to_double(row.next("y"));
+                const double z = to_double(row.next("z"));
+                const auto it = proto.find(id);
+                if (it == proto.end())
+                {
+                    if (!part.undefined) part.undefined_id = id;
+                    part.undefined = true;
+                    continue;
+                }
+                part.particles.push_back(Seed{&it->second, x, y, z});
+            }
+        }
+        catch (...)
+        {
+            part.parse_error = std::current_exception();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (std::size_t k = 1; k < parts; ++k) pool.emplace_back(work, k);
+    work(0);
+    for (auto& t : pool) t.join();
+    for (const Part& part : out)
+        if (part.parse_error) std::rethrow_exception(part.parse_error);
+    for (const Part& part : out)
+        if (part.undefined)
+            throw std::runtime_error{"Particle references undefined group id: " + std::to_string(part.undefined_id)};
+    std::size_t total = 0;
+    for (const Part& part : out) total += part.particles.size();
+    std::vector<Particle> all;
+    all.reserve(total);
+    if (total > 0)
+    {
+        // fault the storage in on all threads before the one-pass fill
+        unsigned char* raw = reinterpret_cast<unsigned char*>(all.data());
+        const std::size_t bytes = total * sizeof(Particle);
+        {
+            const std::uintptr_t a = (reinterpret_cast<std::uintptr_t>(raw) + 4095) & ~std::uintptr_t(4095);
+            const std::uintptr_t e = (reinterpret_cast<std::uintptr_t>(raw) + bytes) & ~std::uintptr_t(4095);
+            if (e > a) ::madvise(reinterpret_cast<void*>(a), e - a, MADV_HUGEPAGE);
+        }
+        auto touch = [&](std::size_t k) {
+            const std::size_t lo = bytes * k / parts, hi = bytes * (k + 1) / parts;
+            std::memset(raw + lo, 0, hi - lo);
+        };
+        std::vector<std::thread> tp;
+        for (std::size_t k = 1; k < parts; ++k) tp.emplace_back(touch, k);
+        touch(0);
+        for (auto& t : tp) t.join();
+    }
+    for (const Part& part : out)
+        for (const Seed& sd : part.particles)
+        {
+            all.push_back(*sd.proto);
+            Particle& q = all.back();
+            q.x_p[0] = sd.x;
+            q.x_p[1] = sd.y;
+            q.x_p[2] = sd.z;
+        }
+    return all;
 }
 
 namespace

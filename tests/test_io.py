@@ -62,6 +62,68 @@ def test_import_capacity_and_missing_file(tmp_path):
     assert L.snow_io_last_error().decode() == "File not open: " + missing
 
 
+def _reference():
+    R = ctypes.CDLL(REF_SO)
+    R.ref_import.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _dp, ctypes.c_int64]
+    R.ref_import.restype = ctypes.c_int64
+    R.ref_last_error.restype = ctypes.c_char_p
+    return R
+
+
+def _large_input(tmp_path, n=200_000, edits=None, seed=11):
+    """groups.csv with 5 groups and a particles.csv of n lines (about 12 MB, so
+    the importer parses it in several parts), some lines ending in CRLF and
+    some blank lines between them; `edits` replaces particle lines by index."""
+    rng = np.random.default_rng(seed)
+    g = tmp_path / "groups.csv"
+    g.write_text("group_id,vx,vy,vz,mass\n" + "".join(
+        f"{i},{float(rng.normal())!r},{float(rng.normal())!r},{float(rng.normal())!r},"
+        f"{float(rng.uniform(1e-4, 1e-3))!r}\n" for i in range(5)))
+    gid = rng.integers(0, 5, n).tolist()
+    x = rng.uniform(-1, 1, (n, 3)).tolist()
+    lines = [f"{gid[i]},{x[i][0]!r},{x[i][1]!r},{x[i][2]!r}" for i in range(n)]
+    for i, text in (edits or {}).items():
+        lines[i] = text
+    body = []
+    for i, line in enumerate(lines):
+        body.append(line + ("\r\n" if i % 997 == 0 else "\n"))
+        if i % 1231 == 0:
+            body.append("\n")
+    p = tmp_path / "particles.csv"
+    p.write_text("group_id,x,y,z\n" + "".join(body))
+    return str(g), str(p)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference build (oracle/_ref) not present")
+def test_import_of_a_large_input_matches_the_reference(tmp_path):
+    """The importer parses large files in parallel parts: the records are the
+    reference's, in file order, CRLF lines and blank lines included."""
+    g, p = _large_input(tmp_path)
+    n, got = _import(_io(), g, p)
+    R = _reference()
+    want = np.zeros((n, 26))
+    assert R.ref_import(g.encode(), p.encode(), want.ctypes.data_as(_dp), n) == n == 200_000
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("edits", [
+    {10: "9,0.1,0.2,0.3", 180_000: "1,0.1,0.2"},      # undefined group early, missing field late
+    {10: "9,0.1,0.2,0.3", 150_000: "8,0.1,0.2,0.3"},  # two undefined groups
+    {5_000: "1,,0.2,0.3", 190_000: "1,0.1,0.2"},      # empty field early, missing field late
+    {190_000: "1,abc,0.2,0.3"},                       # not a number
+], ids=["parse-error-wins", "first-undefined-group", "first-parse-error", "not-a-number"])
+def test_import_errors_of_a_large_input_match_the_reference(tmp_path, edits):
+    """Errors of a file parsed in parallel parts are the reference's sequential
+    ones: a malformed line anywhere before an undefined group, and of each kind
+    the first in file order, with the reference's message."""
+    g, p = _large_input(tmp_path, edits=edits)
+    L, R = _io(), _reference()
+    assert R.ref_import(g.encode(), p.encode(), None, 0) == -1
+    assert L.snow_io_import(g.encode(), p.encode(), None, 0) == -1
+    assert L.snow_io_last_error() == R.ref_last_error()
+
+
 @pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference build (oracle/_ref) not present")
 def test_export_matches_reference_export_byte_for_byte(tmp_path):
     g = np.load(GOLDEN)
