@@ -646,13 +646,16 @@ def measure_io(sc) -> dict:
         n_ours = L.snow_io_import(g.encode(), p.encode(), None, 0)
         if n_ours != sc.n:
             raise RuntimeError(f"snow_io_import read {n_ours} particles, expected {sc.n}")
-        out["import_ms"] = {"ours": best(lambda: L.snow_io_import(g.encode(), p.encode(), None, 0))}
+        # both importers fill the caller's records (the reference's through its vector)
+        dst = np.zeros((sc.n, 26))
+        dptr = dst.ctypes.data_as(dp)
+        out["import_ms"] = {"ours": best(lambda: L.snow_io_import(g.encode(), p.encode(), dptr, sc.n))}
         os.makedirs(os.path.join(d, "output"), exist_ok=True)
         os.chdir(d)
         try:
             out["export_ms"] = {"ours": best(lambda: L.snow_io_export(rec.ctypes.data_as(dp), sc.n, 1))}
             if R is not None:
-                out["import_ms"]["reference"] = best(lambda: R.ref_import(g.encode(), p.encode(), None, 0))
+                out["import_ms"]["reference"] = best(lambda: R.ref_import(g.encode(), p.encode(), dptr, sc.n))
                 out["export_ms"]["reference"] = best(lambda: R.ref_export(rec.ctypes.data_as(dp), sc.n, 2))
         finally:
             os.chdir(cwd)

@@ -254,24 +254,49 @@ private:
 };
 }  // namespace
 
-// import_particles (src/import.cpp:131-136) in one parallel pass over
-// particles.csv: the body after the header line is cut into byte ranges at
-// line starts, and each thread parses its lines and builds their particles
-// from the groups into its own vector; the vectors are joined in file order.
-// The errors are the sequential ones: a malformed line anywhere comes before
-// an undefined group id (the reference reads every seed before assembling),
-// and of each kind the first in file order is reported.
-std::vector<Particle> import_particles(const std::string& filename_group, const std::string& filename_particle_seed)
+namespace
 {
+// A particle line's group prototype and position.
+struct Seed
+{
+    const Particle* proto;
+    double x, y, z;
+};
+// particles.csv parsed in parts: each part's seeds in file order.
+struct ParsedParticles
+{
+    std::map<int, Particle> proto;  // one particle per group, copied for each of its particles
+    std::vector<std::vector<Seed>> parts;
+    std::size_t total = 0;
+};
+
+// Runs work(k) for k in [0, parts) on that many threads (k = 0 on this one).
+template <typename F>
+void run_parts(std::size_t parts, F&& work)
+{
+    std::vector<std::thread> pool;
+    for (std::size_t k = 1; k < parts; ++k) pool.emplace_back(work, k);
+    work(0);
+    for (auto& t : pool) t.join();
+}
+
+// import_particles (src/import.cpp:131-136) up to the assembly, in one
+// parallel pass over particles.csv: the body after the header line is cut
+// into byte ranges at line starts, and each thread parses its lines into its
+// own part.  The errors are the sequential ones: a malformed line anywhere
+// comes before an undefined group id (the reference reads every seed before
+// assembling), and of each kind the first in file order is reported.
+ParsedParticles parse_particles(const std::string& filename_group, const std::string& filename_particle_seed)
+{
+    ParsedParticles res;
     const auto groups = import_groups(filename_group);
     const FileBytes file(filename_particle_seed);
     const std::string_view text = file.view();
     if (text.empty()) throw std::runtime_error{"Particle data file is empty: " + filename_particle_seed};
     const std::size_t header_end = text.find('\n');
     const std::size_t body = header_end == std::string_view::npos ? text.size() : header_end + 1;
-    // one particle per group, copied for each of its particles
-    std::map<int, Particle> proto;
-    for (const auto& [id, g] : groups) proto.emplace(id, Particle(Eigen::Vector3d::Zero(), g.velocity, g.mass, 0.0));
+    for (const auto& [id, g] : groups)
+        res.proto.emplace(id, Particle(Eigen::Vector3d::Zero(), g.velocity, g.mass, 0.0));
 
     constexpr std::size_t kBytesPerPart = std::size_t(1) << 20;
     const std::size_t hw = std::max(1u, std::thread::hardware_concurrency());
@@ -289,22 +314,14 @@ std::vector<Particle> import_particles(const std::string& filename_group, const 
         }
         cut[k] = b;
     }
-    struct Seed
-    {
-        const Particle* proto;
-        double x, y, z;
-    };
-    struct Part
-    {
-        std::vector<Seed> particles;
-        std::exception_ptr parse_error;
-        bool undefined = false;
-        int undefined_id = 0;
-    };
-    std::vector<Part> out(parts);
-    auto work = [&](std::size_t k) {
-        Part& part = out[k];
-        part.particles.reserve((cut[k + 1] - cut[k]) / 24 + 1);
+    res.parts.resize(parts);
+    std::vector<std::exception_ptr> parse_error(parts);
+    std::vector<char> undefined(parts, 0);
+    std::vector<int> undefined_id(parts, 0);
+    const auto& proto = res.proto;
+    run_parts(parts, [&](std::size_t k) {
+        std::vector<Seed>& seeds = res.parts[k];
+        seeds.reserve((cut[k + 1] - cut[k]) / 24 + 1);
         try
         {
             for (std::size_t pos = cut[k]; pos < cut[k + 1];)
@@ -322,52 +339,70 @@ std::vector<Particle> import_particles(const std::string& filename_group, const 
                 const auto it = proto.find(id);
                 if (it == proto.end())
                 {
-                    if (!part.undefined) part.undefined_id = id;
-                    part.undefined = true;
+                    if (!undefined[k]) undefined_id[k] = id;
+                    undefined[k] = 1;
                     continue;
                 }
-                part.particles.push_back(Seed{&it->second, x, y, z});
+                seeds.push_back(Seed{&it->second, x, y, z});
             }
         }
         catch (...)
         {
-            part.parse_error = std::current_exception();
+            parse_error[k] = std::current_exception();
         }
-    };
-    std::vector<std::thread> pool;
-    for (std::size_t k = 1; k < parts; ++k) pool.emplace_back(work, k);
-    work(0);
-    for (auto& t : pool) t.join();
-    for (const Part& part : out)
-        if (part.parse_error) std::rethrow_exception(part.parse_error);
-    for (const Part& part : out)
-        if (part.undefined)
-            throw std::runtime_error{"Particle references undefined group id: " + std::to_string(part.undefined_id)};
-    std::size_t total = 0;
-    for (const Part& part : out) total += part.particles.size();
-    std::vector<Particle> all;
-    all.reserve(total);
-    if (total > 0)
-    {
-        // fault the storage in on all threads before the one-pass fill
-        unsigned char* raw = reinterpret_cast<unsigned char*>(all.data());
-        const std::size_t bytes = total * sizeof(Particle);
+    });
+    for (const auto& e : parse_error)
+        if (e) std::rethrow_exception(e);
+    for (std::size_t k = 0; k < parts; ++k)
+        if (undefined[k])
+            throw std::runtime_error{"Particle references undefined group id: " + std::to_string(undefined_id[k])};
+    for (const auto& seeds : res.parts) res.total += seeds.size();
+    return res;
+}
+
+// Writes the parsed particles as records into `out` (total x 26 doubles), each
+// part on its own thread.
+void fill_records(const ParsedParticles& pp, double* out)
+{
+    std::vector<std::size_t> offset(pp.parts.size() + 1, 0);
+    for (std::size_t k = 0; k < pp.parts.size(); ++k) offset[k + 1] = offset[k] + pp.parts[k].size();
+    run_parts(pp.parts.size(), [&](std::size_t k) {
+        double* rec = out + SNOW_RECORD_DOUBLES * offset[k];
+        for (const Seed& sd : pp.parts[k])
         {
-            const std::uintptr_t a = (reinterpret_cast<std::uintptr_t>(raw) + 4095) & ~std::uintptr_t(4095);
-            const std::uintptr_t e = (reinterpret_cast<std::uintptr_t>(raw) + bytes) & ~std::uintptr_t(4095);
-            if (e > a) ::madvise(reinterpret_cast<void*>(a), e - a, MADV_HUGEPAGE);
+            std::memcpy(rec, sd.proto, sizeof(Particle));
+            rec[0] = sd.x;
+            rec[1] = sd.y;
+            rec[2] = sd.z;
+            rec += SNOW_RECORD_DOUBLES;
         }
-        auto touch = [&](std::size_t k) {
+    });
+}
+}  // namespace
+
+// The parsed particles, assembled into the vector in file order; its storage
+// is faulted in on all threads first, so that the one pass that fills it runs
+// at memory speed.
+std::vector<Particle> import_particles(const std::string& filename_group, const std::string& filename_particle_seed)
+{
+    const ParsedParticles pp = parse_particles(filename_group, filename_particle_seed);
+    std::vector<Particle> all;
+    all.reserve(pp.total);
+    if (pp.total > 0)
+    {
+        unsigned char* raw = reinterpret_cast<unsigned char*>(all.data());
+        const std::size_t bytes = pp.total * sizeof(Particle);
+        const std::uintptr_t a = (reinterpret_cast<std::uintptr_t>(raw) + 4095) & ~std::uintptr_t(4095);
+        const std::uintptr_t e = (reinterpret_cast<std::uintptr_t>(raw) + bytes) & ~std::uintptr_t(4095);
+        if (e > a) ::madvise(reinterpret_cast<void*>(a), e - a, MADV_HUGEPAGE);
+        const std::size_t parts = pp.parts.size();
+        run_parts(parts, [&](std::size_t k) {
             const std::size_t lo = bytes * k / parts, hi = bytes * (k + 1) / parts;
             std::memset(raw + lo, 0, hi - lo);
-        };
-        std::vector<std::thread> tp;
-        for (std::size_t k = 1; k < parts; ++k) tp.emplace_back(touch, k);
-        touch(0);
-        for (auto& t : tp) t.join();
+        });
     }
-    for (const Part& part : out)
-        for (const Seed& sd : part.particles)
+    for (const auto& seeds : pp.parts)
+        for (const Seed& sd : seeds)
         {
             all.push_back(*sd.proto);
             Particle& q = all.back();
@@ -492,12 +527,13 @@ extern "C" int64_t snow_io_import(const char* groups_csv, const char* particles_
     try
     {
         if (!groups_csv || !particles_csv) throw std::runtime_error("snow_io_import: NULL file name");
-        const std::vector<Particle> v = import_particles(groups_csv, particles_csv);
-        const auto n = static_cast<int64_t>(v.size());
+        // parsed on all threads and written straight into the caller's records
+        const ParsedParticles pp = parse_particles(groups_csv, particles_csv);
+        const auto n = static_cast<int64_t>(pp.total);
         if (records)
         {
             if (n > capacity) return -2;
-            if (n) std::memcpy(records, v.data(), v.size() * sizeof(Particle));
+            fill_records(pp, records);
         }
         return n;
     }
